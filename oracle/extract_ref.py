@@ -1,0 +1,44 @@
+"""Build step for the reference harness (oracle/_ref): writes a translation unit
+that #includes line ranges of the reference's gkc_cuda.cu, so its device
+kernels compile as host C++ behind oracle/ref_shim.h.
+
+The reference file cannot be compiled whole by a host compiler because its
+host driver uses the <<<...>>> launch syntax, so only the ranges holding the
+constant tables and the kernels are taken.  Each range is anchored on a line
+whose text is checked, so a different reference revision fails loudly rather
+than compiling something else.  Output goes to oracle/_ref/ only.
+
+Usage: python extract_ref.py <reference_root> <out_file>
+"""
+import sys
+
+# (first line, last line, anchor text expected on the first line)
+RANGES = [
+    (1, 8, "#define _in_"),                     # FILTER_KERNEL selection (:6)
+    (25, 93, "d_basemap[256]"),                 # code tables
+    (146, 339, "struct T_d_data"),              # HPC, filters, minimizer, GenSKM, MoveOffset
+]
+ANCHORS = {
+    164: "GPU_HPCEncoding",
+    234: "GPU_GenMinimizer",
+    298: "GPU_GenSKM",
+    331: "MoveOffset",
+}
+
+
+def main():
+    ref_root, out = sys.argv[1], sys.argv[2]
+    path = f"{ref_root}/gkc_cuda.cu"
+    lines = open(path, encoding="utf-8", errors="replace").read().split("\n")
+    for ln, text in list(ANCHORS.items()) + [(a, t) for a, _, t in RANGES]:
+        if text not in lines[ln - 1]:
+            raise SystemExit(f"{path}:{ln}: expected '{text}', found '{lines[ln - 1]}'")
+    with open(out, "w") as f:
+        f.write("// generated by oracle/extract_ref.py -- not source\n")
+        for a, b, _ in RANGES:
+            f.write(f'#line {a} "{path}"\n')
+            f.write("\n".join(lines[a - 1:b]) + "\n")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,262 @@
+"""ctypes bindings to the checkers under oracle/ (test infrastructure only).
+
+liboracle.so is the plain-C restatement; oracle/_ref/libgkcref.so is the
+reference's own code compiled from its sources (present only where it was
+built).  Results are returned as numpy arrays.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libgkcref.so")
+
+u64p = C.POINTER(C.c_uint64)
+u32p = C.POINTER(C.c_uint32)
+u8p = C.POINTER(C.c_uint8)
+
+
+class OrcSkms(C.Structure):
+    _fields_ = [("n_skm", C.c_uint64), ("n_bytes", C.c_uint64), ("bin", u32p), ("len", u32p),
+                ("byte_off", u64p), ("read_id", u64p), ("start", u32p), ("minimizer", u32p),
+                ("bytes", u8p)]
+
+
+class OrcCounts(C.Structure):
+    _fields_ = [("nbins", C.c_uint32), ("n_distinct", C.c_uint64), ("bin_off", u64p),
+                ("keys_lo", u64p), ("keys_hi", u64p), ("counts", u32p)]
+
+
+class OrcPos(C.Structure):
+    _fields_ = [("n_distinct", C.c_uint64), ("n_pos", C.c_uint64), ("keys_lo", u64p),
+                ("keys_hi", u64p), ("pos_off", u64p), ("pos", u32p)]
+
+
+class RefSkms(C.Structure):
+    _fields_ = [("n_skm", C.c_uint64), ("n_bytes", C.c_uint64), ("bin", u32p), ("len", u32p),
+                ("byte_off", u64p), ("bytes", u8p)]
+
+
+class RefCounts(C.Structure):
+    _fields_ = [("nbins", C.c_uint32), ("n_distinct", C.c_uint64), ("bin_off", u64p),
+                ("keys", u64p), ("counts", u32p), ("returned", u64p)]
+
+
+def _arr(ptr, n, dtype):
+    if n == 0 or not ptr:
+        return np.zeros(0, dtype=dtype)
+    return np.ctypeslib.as_array(ptr, shape=(int(n),)).astype(dtype, copy=True)
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+_orc = None
+_ref = None
+
+
+def oracle():
+    global _orc
+    if _orc is None:
+        lib = C.CDLL(ORACLE_SO)
+        lib.orc_partition.argtypes = [u8p, u64p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int,
+                                      C.POINTER(OrcSkms)]
+        lib.orc_count_bins.argtypes = [C.POINTER(OrcSkms), C.c_int, C.c_int, C.POINTER(OrcCounts)]
+        lib.orc_count_packed.argtypes = [u32p, u64p, u8p, C.c_uint64, C.c_int, C.POINTER(OrcCounts)]
+        lib.orc_window_minimizers.argtypes = [u8p, C.c_int32, C.c_int, C.c_int, u32p]
+        lib.orc_window_minimizer_pos.argtypes = [u8p, C.c_int32, C.c_int, C.c_int, u32p, u8p,
+                                                 C.POINTER(C.c_int8)]
+        lib.orc_hpc.argtypes = [u8p, u64p, C.c_int64, u8p, C.POINTER(C.c_int32),
+                                C.POINTER(C.c_int32)]
+        lib.orc_subsample_positions.argtypes = [u8p, u64p, C.c_int64, C.c_int, C.c_int, C.c_uint32,
+                                                C.POINTER(OrcPos)]
+        lib.orc_skms_free.argtypes = [C.POINTER(OrcSkms)]
+        lib.orc_counts_free.argtypes = [C.POINTER(OrcCounts)]
+        lib.orc_poslists_free.argtypes = [C.POINTER(OrcPos)]
+        _orc = lib
+    return _orc
+
+
+def ref_available():
+    return os.path.exists(REF_SO)
+
+
+def reference():
+    global _ref
+    if _ref is None:
+        lib = C.CDLL(REF_SO)
+        lib.ref_partition.argtypes = [C.c_char_p, u64p, C.c_int64, C.c_int, C.c_int, C.c_int,
+                                      C.c_int, C.c_int, C.c_int, C.POINTER(RefSkms)]
+        lib.ref_count_bins.argtypes = [C.POINTER(RefSkms), C.c_int, C.c_int, C.c_int,
+                                       C.POINTER(RefCounts)]
+        lib.ref_pipeline.argtypes = [C.c_char_p, u64p, C.c_int64, C.c_int, C.c_int, C.c_int,
+                                     C.c_int, C.c_int, C.c_int, u64p, u64p]
+        lib.ref_skms_free.argtypes = [C.POINTER(RefSkms)]
+        lib.ref_counts_free.argtypes = [C.POINTER(RefCounts)]
+        _ref = lib
+    return _ref
+
+
+class Skms:
+    """Superkmers as flat arrays: bin, len, byte_off into `bytes`."""
+
+    def __init__(self, bin, length, byte_off, data, minimizer=None, read_id=None, start=None):
+        self.bin = bin
+        self.len = length
+        self.byte_off = byte_off
+        self.bytes = data
+        self.minimizer = minimizer
+        self.read_id = read_id
+        self.start = start
+
+    def multisets(self, nbins):
+        """Per bin: sorted list of (len, packed bytes) -- the partition parity form."""
+        out = [[] for _ in range(nbins)]
+        for i in range(len(self.bin)):
+            nb = (int(self.len[i]) + 3) // 4
+            o = int(self.byte_off[i])
+            out[int(self.bin[i])].append((int(self.len[i]), self.bytes[o:o + nb].tobytes()))
+        for b in out:
+            b.sort()
+        return out
+
+
+def oracle_partition(reads, offs, k, p, hpc, nbins):
+    lib = oracle()
+    reads = np.ascontiguousarray(reads, dtype=np.uint8)
+    offs = np.ascontiguousarray(offs, dtype=np.uint64)
+    s = OrcSkms()
+    rc = lib.orc_partition(_ptr(reads, u8p), _ptr(offs, u64p), len(offs) - 1, k, p, int(hpc), nbins,
+                           C.byref(s))
+    assert rc == 0, rc
+    out = Skms(_arr(s.bin, s.n_skm, np.uint32), _arr(s.len, s.n_skm, np.uint32),
+               _arr(s.byte_off, s.n_skm, np.uint64), _arr(s.bytes, s.n_bytes, np.uint8),
+               _arr(s.minimizer, s.n_skm, np.uint32), _arr(s.read_id, s.n_skm, np.uint64),
+               _arr(s.start, s.n_skm, np.uint32))
+    lib.orc_skms_free(C.byref(s))
+    return out
+
+
+def _counts_from(c, wide):
+    nb = c.nbins
+    res = dict(bin_off=_arr(c.bin_off, nb + 1, np.uint64),
+               keys_lo=_arr(c.keys_lo, c.n_distinct, np.uint64),
+               counts=_arr(c.counts, c.n_distinct, np.uint32))
+    res["keys_hi"] = _arr(c.keys_hi, c.n_distinct, np.uint64) if wide else None
+    return res
+
+
+def oracle_count_bins(skms, k, nbins):
+    lib = oracle()
+    s = OrcSkms()
+    s.n_skm = len(skms.bin)
+    s.n_bytes = len(skms.bytes)
+    keep = [np.ascontiguousarray(skms.bin, np.uint32), np.ascontiguousarray(skms.len, np.uint32),
+            np.ascontiguousarray(skms.byte_off, np.uint64),
+            np.ascontiguousarray(skms.bytes if len(skms.bytes) else np.zeros(1, np.uint8), np.uint8)]
+    s.bin = _ptr(keep[0], u32p)
+    s.len = _ptr(keep[1], u32p)
+    s.byte_off = _ptr(keep[2], u64p)
+    s.bytes = _ptr(keep[3], u8p)
+    c = OrcCounts()
+    rc = lib.orc_count_bins(C.byref(s), k, nbins, C.byref(c))
+    assert rc == 0, rc
+    res = _counts_from(c, k > 32)
+    lib.orc_counts_free(C.byref(c))
+    return res
+
+
+def oracle_minimizers(read, k, p, with_pos=False):
+    lib = oracle()
+    read = np.ascontiguousarray(read, dtype=np.uint8)
+    W = max(0, len(read) - k + 1)
+    mm = np.zeros(max(W, 1), np.uint32)
+    if not with_pos:
+        lib.orc_window_minimizers(_ptr(read, u8p), len(read), k, p, _ptr(mm, u32p))
+        return mm[:W]
+    pos = np.zeros(max(W, 1), np.uint8)
+    st = np.zeros(max(W, 1), np.int8)
+    lib.orc_window_minimizer_pos(_ptr(read, u8p), len(read), k, p, _ptr(mm, u32p), _ptr(pos, u8p),
+                                 st.ctypes.data_as(C.POINTER(C.c_int8)))
+    return mm[:W], pos[:W], st[:W]
+
+
+def oracle_hpc(reads, offs):
+    lib = oracle()
+    reads = np.ascontiguousarray(reads, dtype=np.uint8)
+    offs = np.ascontiguousarray(offs, dtype=np.uint64)
+    n = len(offs) - 1
+    out = np.zeros(max(len(reads), 1), np.uint8)
+    ln = np.zeros(max(n, 1), np.int32)
+    orig = np.zeros(max(len(reads), 1), np.int32)
+    lib.orc_hpc(_ptr(reads, u8p), _ptr(offs, u64p), n, _ptr(out, u8p),
+                ln.ctypes.data_as(C.POINTER(C.c_int32)), orig.ctypes.data_as(C.POINTER(C.c_int32)))
+    return out[:len(reads)], ln[:n], orig[:len(reads)]
+
+
+def oracle_subsample(reads, offs, k, p, mod):
+    lib = oracle()
+    reads = np.ascontiguousarray(reads, dtype=np.uint8)
+    offs = np.ascontiguousarray(offs, dtype=np.uint64)
+    r = OrcPos()
+    rc = lib.orc_subsample_positions(_ptr(reads, u8p), _ptr(offs, u64p), len(offs) - 1, k, p, mod,
+                                     C.byref(r))
+    assert rc == 0
+    res = dict(keys_lo=_arr(r.keys_lo, r.n_distinct, np.uint64),
+               keys_hi=_arr(r.keys_hi, r.n_distinct, np.uint64),
+               pos_off=_arr(r.pos_off, r.n_distinct + 1, np.uint64),
+               pos=_arr(r.pos, r.n_pos, np.uint32))
+    lib.orc_poslists_free(C.byref(r))
+    return res
+
+
+def ref_partition(reads, offs, k, p, hpc, nbins, batch_reads=2048, n_threads=4):
+    lib = reference()
+    reads = np.ascontiguousarray(reads, dtype=np.uint8)
+    offs = np.ascontiguousarray(offs, dtype=np.uint64)
+    s = RefSkms()
+    rc = lib.ref_partition(reads.ctypes.data_as(C.c_char_p), _ptr(offs, u64p), len(offs) - 1, k, p,
+                           int(hpc), nbins, batch_reads, n_threads, C.byref(s))
+    assert rc == 0
+    out = Skms(_arr(s.bin, s.n_skm, np.uint32), _arr(s.len, s.n_skm, np.uint32),
+               _arr(s.byte_off, s.n_skm, np.uint64), _arr(s.bytes, s.n_bytes, np.uint8))
+    lib.ref_skms_free(C.byref(s))
+    return out
+
+
+def ref_count_bins(skms, k, nbins, n_threads=4):
+    lib = reference()
+    s = RefSkms()
+    keep = [np.ascontiguousarray(skms.bin, np.uint32), np.ascontiguousarray(skms.len, np.uint32),
+            np.ascontiguousarray(skms.byte_off, np.uint64),
+            np.ascontiguousarray(skms.bytes if len(skms.bytes) else np.zeros(1, np.uint8), np.uint8)]
+    s.n_skm = len(skms.bin)
+    s.n_bytes = len(skms.bytes)
+    s.bin = _ptr(keep[0], u32p)
+    s.len = _ptr(keep[1], u32p)
+    s.byte_off = _ptr(keep[2], u64p)
+    s.bytes = _ptr(keep[3], u8p)
+    c = RefCounts()
+    rc = lib.ref_count_bins(C.byref(s), k, nbins, n_threads, C.byref(c))
+    assert rc == 0
+    res = dict(bin_off=_arr(c.bin_off, nbins + 1, np.uint64),
+               keys_lo=_arr(c.keys, c.n_distinct, np.uint64),
+               counts=_arr(c.counts, c.n_distinct, np.uint32),
+               returned=_arr(c.returned, nbins, np.uint64), keys_hi=None)
+    lib.ref_counts_free(C.byref(c))
+    return res
+
+
+def ref_pipeline(reads, offs, k, p, hpc, nbins, batch_reads=2048, n_threads=1):
+    lib = reference()
+    reads = np.ascontiguousarray(reads, dtype=np.uint8)
+    offs = np.ascontiguousarray(offs, dtype=np.uint64)
+    d = np.zeros(1, np.uint64)
+    km = np.zeros(1, np.uint64)
+    rc = lib.ref_pipeline(reads.ctypes.data_as(C.c_char_p), _ptr(offs, u64p), len(offs) - 1, k, p,
+                          int(hpc), nbins, batch_reads, n_threads, _ptr(d, u64p), _ptr(km, u64p))
+    assert rc == 0
+    return int(d[0]), int(km[0])
