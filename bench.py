@@ -1,0 +1,442 @@
+"""Benchmark: canonical k-mers counted per second on one B200 (or N, weak).
+
+Default workload (the north-star shape): a 100 Mbp synthetic genome with 5%
+of its length as 1-5 kbp segment copies (1% divergence), sampled as 150 bp
+reads on both strands to 30x coverage (20 M reads, 3.0 G bases) with 0.5%
+substitution errors; k=31, p=11, 256 bins.  Reads are generated on the device
+from a seed.  One step = the batched, graph-captured pipeline
+(partition -> expand -> sort -> count) over all reads, inputs resident in HBM.
+
+Printed: one JSON line (rank 0).  `--impl reference` times the reference's own
+CPU implementation (oracle/_ref, compiled from the reference sources) on a
+bounded sample of the same workload instead.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+WORKLOADS = {
+    # name: generator, sizes, k, p, nbins
+    "ns": dict(gen="genome", genome_len=100_000_000, coverage=30, read_len=150, err=0.005,
+               k=31, p=11, nbins=256, hpc=0),
+    "config2": dict(gen="genome", genome_len=10_000_000, coverage=30, read_len=150, err=0.005,
+                    k=31, p=11, nbins=256, hpc=0),
+    "config1": dict(gen="iid", n_reads=20000, read_len=150, n_rate=0.001, k=31, p=11, nbins=256,
+                    hpc=0),
+    "config4": dict(gen="genome", genome_len=100_000_000, coverage=30, read_len=250, err=0.005,
+                    k=63, p=13, nbins=256, hpc=0),
+}
+METRIC = "canonical k-mers counted/s"
+SEED = 2026
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ns", choices=sorted(WORKLOADS))
+    ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-sample-reads", type=int, default=200_000)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--seed", type=int, default=SEED)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- helpers
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), \
+        int(os.environ.get("LOCAL_RANK", 0))
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes(B, R, S, N, D, k):
+    """Fixed byte model per stage (bytes that each stage must move at least
+    once in the reference's dataflow): B bases, R reads, S superkmers,
+    L superkmer bases, N k-mers, D distinct (k-mer, bin) pairs, w key bytes,
+    P 8-bit LSD passes."""
+    w = 8 if k <= 32 else 16
+    P = math.ceil(2 * k / 8)
+    L = N + S * (k - 1)
+    part = B + 8 * (R + 1) + L / 4 + 8 * S
+    expand = L / 4 + 8 * S + w * N
+    sort = w * N + P * 2 * w * N
+    count = w * N + (w + 4) * D
+    return dict(partition=part, expand=expand, sort=sort, count=count,
+                total=part + expand + sort + count, w=w, P=P, L=L)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        rows = []
+        for line in (getattr(self, "out", "") or "").strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), parts[3:7]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------- workload (GPU)
+
+def make_workload_device(wl, seed, rank, torch, G):
+    """Reads (uint8) and offsets (int64 view of uint64) on the current device."""
+    L = G.lib()
+    dev = torch.cuda.current_device()
+    if wl["gen"] == "iid":
+        n = wl["n_reads"]
+        reads = torch.empty(n * wl["read_len"] + 64, dtype=torch.uint8, device=dev)
+        offs = torch.empty(n + 1, dtype=torch.int64, device=dev)
+        st = L.gkc_synth_iid_reads(1, seed + rank, n, wl["read_len"], wl["n_rate"], reads.data_ptr(),
+                                   offs.data_ptr())
+        assert st == 0
+        return reads, offs, n, n * wl["read_len"], None
+    Gl = wl["genome_len"]
+    genome = torch.empty(Gl, dtype=torch.uint8, device=dev)
+    assert L.gkc_synth_genome(1, seed, Gl, 0.05, 0.01, genome.data_ptr()) == 0
+    n = wl["coverage"] * Gl // wl["read_len"]
+    reads = torch.empty(n * wl["read_len"] + 64, dtype=torch.uint8, device=dev)
+    offs = torch.empty(n + 1, dtype=torch.int64, device=dev)
+    # each rank samples its own reads of the same genome (weak scaling)
+    assert L.gkc_synth_short_reads(1, seed, genome.data_ptr(), Gl, rank * n, n, wl["read_len"],
+                                   wl["err"], reads.data_ptr(), offs.data_ptr()) == 0
+    return reads, offs, n, n * wl["read_len"], genome
+
+
+def host_sample(wl, seed, n_reads, genome_host=None):
+    """The first n_reads reads of the workload, generated on the host."""
+    from gkc_b200 import synth
+    if wl["gen"] == "iid":
+        return synth.iid_reads(seed, min(n_reads, wl["n_reads"]), wl["read_len"], wl["n_rate"])
+    g = genome_host if genome_host is not None else synth.genome(seed, wl["genome_len"])
+    return synth.short_reads(seed, g, n_reads, wl["read_len"], wl["err"])
+
+
+def cpu_reference_rate(reads, offs, wl, threads):
+    """The reference's CPU path (partition kernels + SKMStore + Thrust-host
+    counting, compiled from its sources) on a sample; returns k-mers/s."""
+    import oracle_ffi as F
+    t0 = time.perf_counter()
+    distinct, kmers = F.ref_pipeline(reads, offs, wl["k"], wl["p"], wl["hpc"], wl["nbins"],
+                                     batch_reads=2048, n_threads=threads)
+    dt = time.perf_counter() - t0
+    return kmers / dt, dt, kmers, distinct
+
+
+# ------------------------------------------------------------ reference arm
+
+def run_reference(args, wl):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle_ffi as F
+    if not F.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference tree absent at build time)"}))
+        return
+    threads = os.cpu_count() or 1
+    n = args.cpu_sample_reads if wl["gen"] != "iid" else wl["n_reads"]
+    reads, offs = host_sample(wl, args.seed, n)
+    for _ in range(args.warmup):
+        cpu_reference_rate(reads, offs, wl, threads)
+    rates, secs, km = [], [], 0
+    for _ in range(args.steps):
+        r, dt, kmers, _ = cpu_reference_rate(reads, offs, wl, threads)
+        rates.append(r)
+        secs.append(dt)
+        km = kmers
+    value = float(np.median(rates))
+    sample = f"first {len(offs) - 1} reads ({int(offs[-1])} bases, {km} k-mers) of workload {wl_name(args)}"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "kmers/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * float(np.median(secs)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": config_dict(args, wl, len(offs) - 1, int(offs[-1])),
+        "cpu_baseline": {"value": value, "unit": "kmers/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "kmers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def wl_name(args):
+    return {"ns": "ns-100Mbp-30x-150bp-k31", "config2": "config2-10Mbp-30x-150bp-k31",
+            "config1": "config1-iid-20000x150bp-k31", "config4": "config4-100Mbp-30x-250bp-k63"}[args.workload]
+
+
+def config_dict(args, wl, n_reads, n_bases):
+    d = {"workload": wl_name(args), "reads": n_reads, "bases": n_bases, "k": wl["k"], "p": wl["p"],
+         "nbins": wl["nbins"], "hpc": bool(wl["hpc"]), "seed": args.seed,
+         "l2": "inputs larger than L2 (reads + superkmers + keys >> 126 MB)",
+         "mode": "batched, graph-captured", "parallelism": f"weak-replicas{args.gpus}"}
+    if wl["gen"] == "genome":
+        d.update(genome_bp=wl["genome_len"], coverage=wl["coverage"], read_len=wl["read_len"],
+                 error_rate=wl["err"])
+    return d
+
+
+# ------------------------------------------------------------------ our arm
+
+def run_ours(args, wl):
+    import torch
+    import gkc_b200 as G
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    reads, offs, n_reads, n_bases, genome = make_workload_device(wl, args.seed, rank, torch, G)
+    torch.cuda.synchronize()
+    prm = G.params(wl["k"], wl["p"], wl["nbins"], wl["hpc"])
+    ctx = G.Context(local)
+    stream = torch.cuda.Stream()  # graphs cannot be captured on the legacy default stream
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+
+    def step():
+        return ctx.pipeline_device(reads, n_bases, offs, n_reads, prm, G.MODE_BATCHED)
+
+    for _ in range(max(args.warmup, 3)):
+        pv, cv = step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    stage_acc = {}
+    launches = 0
+    barrier()
+    with ClockSampler(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            pv, cv = step()
+            t = ctx.timings()
+            launches += int(t.launches)
+            for name, ms in t.stages().items():
+                stage_acc.setdefault(name, []).append(ms)
+        e1.record(stream)
+        barrier()
+    ms_total = e0.elapsed_time(e1)
+    if dist:
+        tt = torch.tensor([ms_total], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_total = float(tt.item())
+    clocks = clk.summary()
+
+    N, D, S = int(cv.n_kmers), int(cv.n_distinct), int(pv.n_superkmers)
+    B, R = int(pv.n_bases), int(pv.n_reads)
+    ms_step = ms_total / args.steps
+    value = N * world * args.steps / (ms_total / 1000.0)
+    stages = {k: float(np.mean(v)) for k, v in stage_acc.items()}
+    model = algorithmic_bytes(B, R, S, N, D, wl["k"])
+    peak, peak_kind = peaks()
+
+    # dominant kernel and its model bytes per launch
+    kernel_bytes = {"partition": model["partition"], "bucket_scatter": model["expand"],
+                    "sort_count": model["sort"] + model["count"]}
+    dom = max(kernel_bytes, key=lambda s: stages.get(s, 0.0))
+    dom_ms = stages[dom]
+    achieved = kernel_bytes[dom] / (dom_ms / 1000.0) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            with open(tfile) as f:
+                td = json.load(f)
+            per_unit = td.get(wl_name(args), {}).get(dom)
+            if per_unit is not None:
+                traffic = per_unit["dram_bytes_per_kmer"] * N
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                "model": "fixed algorithmic-bytes model (see DESIGN.md)",
+                "model_bytes_per_launch": kernel_bytes[dom], "ms_per_launch": dom_ms}
+    if traffic:
+        roofline["frac_dram_traffic"] = traffic / (dom_ms / 1000.0) / 1e9 / peak
+    pipeline = {"model_bytes": model["total"], "ms": ms_step,
+                "achieved_gbs": model["total"] / (ms_step / 1000.0) / 1e9,
+                "frac_of_hbm_roofline": model["total"] / (ms_step / 1000.0) / 1e9 / peak,
+                "bases_per_s": B * world / (ms_step / 1000.0), "superkmers": S, "kmers": N,
+                "distinct": D}
+
+    result = {
+        "metric": METRIC, "value": value, "unit": "kmers/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64" if wl["k"] <= 32 else "u128", "data": "synthetic",
+        "config": config_dict(args, wl, n_reads, n_bases), "roofline": roofline,
+        "pipeline": pipeline, "stages_ms": stages, "gpu_launches": launches, "clocks": clocks,
+    }
+
+    # plain per-stage form on the same input (bit-exact check against batched)
+    if not args.no_plain and rank == 0:
+        bin_off_b, keys_b, counts_b = None, None, None
+        h_bo = np.zeros(wl["nbins"] + 1, np.uint64)
+        G.lib().gkc_count_copy_out(ctx.h, h_bo.ctypes.data, None, None)
+        ref_digest = (int(cv.n_distinct), h_bo.tobytes())
+        pe0 = torch.cuda.Event(enable_timing=True)
+        pe1 = torch.cuda.Event(enable_timing=True)
+        ctx.pipeline_device(reads, n_bases, offs, n_reads, prm, G.MODE_PLAIN)  # warm-up
+        torch.cuda.synchronize()
+        pe0.record(stream)
+        for _ in range(args.plain_steps):
+            ppv, pcv = ctx.pipeline_device(reads, n_bases, offs, n_reads, prm, G.MODE_PLAIN)
+        pe1.record(stream)
+        torch.cuda.synchronize()
+        p_ms = pe0.elapsed_time(pe1) / args.plain_steps
+        h_bo2 = np.zeros(wl["nbins"] + 1, np.uint64)
+        G.lib().gkc_count_copy_out(ctx.h, h_bo2.ctypes.data, None, None)
+        same = (int(pcv.n_distinct), h_bo2.tobytes()) == ref_digest
+        result["plain"] = {"value": N / (p_ms / 1000.0), "unit": "kmers/s", "ms_per_step": p_ms,
+                           "steps": args.plain_steps, "batched_over_plain": p_ms / ms_step,
+                           "same_counts_as_batched": bool(same),
+                           "launches_per_step": int(ctx.timings().launches)}
+        # restore the batched result in the context
+        step()
+
+    # end to end through the host API: pinned host reads in, full sorted list out
+    if not args.no_e2e:
+        h_reads = torch.empty(n_bases, dtype=torch.uint8, pin_memory=True)
+        h_offs = torch.empty(n_reads + 1, dtype=torch.int64, pin_memory=True)
+        h_reads.copy_(reads[:n_bases])
+        h_offs.copy_(offs)
+        kw = 1 if wl["k"] <= 32 else 2
+        h_binoff = torch.empty(wl["nbins"] + 1, dtype=torch.int64, pin_memory=True)
+        h_keys = torch.empty(max(D * kw, 1), dtype=torch.int64, pin_memory=True)
+        h_counts = torch.empty(max(D, 1), dtype=torch.int32, pin_memory=True)
+        nr = h_reads.numpy()
+        no = h_offs.numpy().view(np.uint64)
+        del reads  # the host path uploads its own copy
+        torch.cuda.empty_cache()
+
+        def e2e_step():
+            c = ctx.pipeline_host(nr, no, prm, G.MODE_BATCHED)
+            L = G.lib()
+            st = L.gkc_count_copy_out(ctx.h, h_binoff.data_ptr(), h_keys.data_ptr(), h_counts.data_ptr())
+            assert st == 0
+            return c
+
+        e2e_step()
+        barrier()
+        ee0 = torch.cuda.Event(enable_timing=True)
+        ee1 = torch.cuda.Event(enable_timing=True)
+        ee0.record(stream)
+        for _ in range(args.e2e_steps):
+            c = e2e_step()
+        ee1.record(stream)
+        barrier()
+        e_ms = ee0.elapsed_time(ee1)
+        if dist:
+            tt = torch.tensor([e_ms], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e_ms = float(tt.item())
+        nd = int(c.n_distinct)
+        result["e2e"] = {"value": N * world * args.e2e_steps / (e_ms / 1000.0), "unit": "kmers/s",
+                         "h2d_bytes_per_step": n_bases + (n_reads + 1) * 8,
+                         "d2h_bytes_per_step": (wl["nbins"] + 1) * 8 + nd * 8 * kw + nd * 4,
+                         "ms_per_step": e_ms / args.e2e_steps, "steps": args.e2e_steps,
+                         "api": "gkc_pipeline_host + gkc_count_copy_out"}
+
+    # CPU baseline: the reference's own CPU path on a bounded sample (rank 0, N=1)
+    if not args.no_cpu and rank == 0 and world == 1:
+        import oracle_ffi as F
+        if F.ref_available():
+            threads = os.cpu_count() or 1
+            n = args.cpu_sample_reads if wl["gen"] != "iid" else wl["n_reads"]
+            gh = genome.cpu().numpy() if genome is not None else None
+            sr, so = host_sample(wl, args.seed, n, gh)
+            rate, dt, km, _ = cpu_reference_rate(sr, so, wl, threads)
+            result["cpu_baseline"] = {
+                "value": rate, "unit": "kmers/s", "cores": threads, "kind": "reference",
+                "sample": f"first {len(so) - 1} reads ({int(so[-1])} bases, {km} k-mers) of the workload, {dt:.2f} s"}
+        else:
+            result["cpu_baseline"] = {"value": None, "unit": "kmers/s", "cores": 0, "kind": "reference",
+                                      "sample": "oracle/_ref not built"}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(result))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, wl)
+    else:
+        run_ours(args, wl)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,291 @@
+"""gkc_b200: B200-native k-mer partitioning and counting.
+
+Thin ctypes binding over the C ABI in include/gkc/gkc.h (libgkc_b200.so,
+built in-tree by gkc_b200.build).  There is no fallback: if the shared
+library is missing, loading fails with an error.
+
+Host-level calls take numpy arrays; device-level calls take torch CUDA
+tensors (torch is used only to hold device memory).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgkc_b200.so")
+
+MODE_BATCHED = 0
+MODE_PLAIN = 1
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no CUDA device",
+          4: "out of device memory", 5: "HBM budget exceeded", 6: "capacity exceeded",
+          7: "device-side wait timed out", 8: "not ready", 9: "cancelled", 10: "not found",
+          11: "internal error"}
+
+
+class GkcError(RuntimeError):
+    def __init__(self, status, msg=""):
+        super().__init__(f"gkc status {status} ({STATUS.get(status, '?')}): {msg}")
+        self.status = status
+
+
+class Params(C.Structure):
+    _fields_ = [("k", C.c_int), ("p", C.c_int), ("hpc", C.c_int), ("nbins", C.c_int)]
+
+
+class PartitionView(C.Structure):
+    _fields_ = [("n_reads", C.c_uint64), ("n_bases", C.c_uint64), ("n_superkmers", C.c_uint64),
+                ("n_packed_bytes", C.c_uint64), ("n_kmers", C.c_uint64), ("nbins", C.c_uint32),
+                ("bin_skm_off", C.c_void_p), ("bin_kmer_off", C.c_void_p), ("skm_desc", C.c_void_p),
+                ("skm_minimizer", C.c_void_p), ("packed", C.c_void_p), ("hpc_reads", C.c_void_p),
+                ("hpc_offs", C.c_void_p), ("hpc_orig_pos", C.c_void_p)]
+
+
+class CountView(C.Structure):
+    _fields_ = [("n_distinct", C.c_uint64), ("n_kmers", C.c_uint64), ("nbins", C.c_uint32),
+                ("key_words", C.c_int), ("bin_off", C.c_void_p), ("keys", C.c_void_p),
+                ("counts", C.c_void_p)]
+
+
+class PoslistView(C.Structure):
+    _fields_ = [("n_distinct", C.c_uint64), ("n_positions", C.c_uint64), ("key_words", C.c_int),
+                ("keys", C.c_void_p), ("pos_off", C.c_void_p), ("positions", C.c_void_p)]
+
+
+MAX_STAGES = 8
+
+
+class Timings(C.Structure):
+    _fields_ = [("partition_ms", C.c_float), ("count_ms", C.c_float), ("total_ms", C.c_float),
+                ("h2d_ms", C.c_float), ("d2h_ms", C.c_float), ("launches", C.c_uint32),
+                ("graph_replayed", C.c_uint32), ("n_stages", C.c_uint32),
+                ("stage_ms", C.c_float * MAX_STAGES)]
+
+    def stages(self):
+        L = lib()
+        return {L.gkc_stage_name(i).decode(): float(self.stage_ms[i]) for i in range(self.n_stages)}
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("status", C.c_int), ("n_bases", C.c_uint64),
+                ("n_kmers", C.c_uint64), ("n_distinct", C.c_uint64), ("nbins", C.c_uint32),
+                ("key_words", C.c_int), ("submit_s", C.c_double), ("start_s", C.c_double),
+                ("end_s", C.c_double), ("hbm_bytes", C.c_uint64)]
+
+
+# (name, restype, argtypes) for every exported symbol of include/gkc/gkc.h
+vp, u64, u32, i32, dbl = C.c_void_p, C.c_uint64, C.c_uint32, C.c_int, C.c_double
+P = C.POINTER
+SIGNATURES = [
+    ("gkc_abi_version", C.c_int, []),
+    ("gkc_stage_name", C.c_char_p, [C.c_int]),
+    ("gkc_status_string", C.c_char_p, [C.c_int]),
+    ("gkc_ctx_create", C.c_int, [C.c_int, u64, P(vp)]),
+    ("gkc_ctx_destroy", None, [vp]),
+    ("gkc_ctx_last_error", C.c_char_p, [vp]),
+    ("gkc_ctx_set_stream", C.c_int, [vp, vp]),
+    ("gkc_ctx_synchronize", C.c_int, [vp]),
+    ("gkc_ctx_device_bytes", u64, [vp]),
+    ("gkc_ctx_release_workspace", C.c_int, [vp]),
+    ("gkc_last_timings", C.c_int, [vp, P(Timings)]),
+    ("gkc_partition_device", C.c_int, [vp, P(Params), vp, u64, vp, u64, P(PartitionView)]),
+    ("gkc_partition_host", C.c_int, [vp, P(Params), vp, vp, u64, P(PartitionView)]),
+    ("gkc_partition_copy_out", C.c_int, [vp, vp, vp, vp, vp, vp]),
+    ("gkc_count_device", C.c_int, [vp, P(Params), C.c_int, P(CountView)]),
+    ("gkc_count_superkmers_host", C.c_int, [vp, C.c_int, vp, vp, u64, C.c_int, P(u64)]),
+    ("gkc_count_copy_out", C.c_int, [vp, vp, vp, vp]),
+    ("gkc_pipeline_device", C.c_int, [vp, P(Params), C.c_int, vp, u64, vp, u64, P(PartitionView),
+                                      P(CountView)]),
+    ("gkc_pipeline_host", C.c_int, [vp, P(Params), C.c_int, vp, vp, u64, P(CountView)]),
+    ("gkc_minimizers_device", C.c_int, [vp, P(Params), vp, u64, vp, u64, vp, vp, vp]),
+    ("gkc_subsample_positions_device", C.c_int, [vp, P(Params), u32, vp, u64, vp, u64,
+                                                 P(PoslistView)]),
+    ("gkc_hpc_device", C.c_int, [vp, vp, u64, vp, u64, vp, vp, vp]),
+    ("gkc_server_create", C.c_int, [C.c_int, u64, C.c_int, P(vp)]),
+    ("gkc_server_destroy", None, [vp]),
+    ("gkc_server_submit", C.c_int, [vp, P(Params), vp, vp, u64, P(u64)]),
+    ("gkc_server_submit_device_synth", C.c_int, [vp, P(Params), C.c_int, u64, u64, P(u64)]),
+    ("gkc_server_poll", C.c_int, [vp, u64, P(JobInfo)]),
+    ("gkc_server_wait", C.c_int, [vp, u64, dbl, P(JobInfo)]),
+    ("gkc_server_cancel", C.c_int, [vp, u64]),
+    ("gkc_server_copy_result", C.c_int, [vp, u64, vp, vp, vp]),
+    ("gkc_server_release", C.c_int, [vp, u64]),
+    ("gkc_job_hbm_estimate", u64, [P(Params), u64, u64]),
+    ("gkc_synth_iid_reads", C.c_int, [C.c_int, u64, u64, u32, dbl, vp, vp]),
+    ("gkc_synth_genome", C.c_int, [C.c_int, u64, u64, dbl, dbl, vp]),
+    ("gkc_synth_short_reads", C.c_int, [C.c_int, u64, vp, u64, u64, u64, u32, dbl, vp, vp]),
+    ("gkc_synth_long_read_offsets", u64, [u64, dbl, dbl, u32, u32, u64, u64, vp]),
+    ("gkc_synth_long_reads", C.c_int, [C.c_int, u64, vp, u64, u64, vp, vp]),
+]
+
+_lib = None
+
+
+def lib():
+    """Loads libgkc_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m gkc_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    """Address of a numpy array or a torch tensor."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def params(k, p, nbins, hpc=False):
+    return Params(int(k), int(p), int(bool(hpc)), int(nbins))
+
+
+class Context:
+    """One device context (reference: GPUReset + the per-call CUDA state of
+    GenSuperkmerGPU / kmc_counting_GPU)."""
+
+    def __init__(self, device=0, hbm_budget=0):
+        self._L = lib()
+        h = C.c_void_p()
+        st = self._L.gkc_ctx_create(int(device), int(hbm_budget), C.byref(h))
+        if st != 0:
+            raise GkcError(st, "gkc_ctx_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self._L.gkc_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st, what):
+        if st != 0:
+            msg = self._L.gkc_ctx_last_error(self.h)
+            raise GkcError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def timings(self):
+        t = Timings()
+        self._check(self._L.gkc_last_timings(self.h, C.byref(t)), "timings")
+        return t
+
+    def device_bytes(self):
+        return int(self._L.gkc_ctx_device_bytes(self.h))
+
+    def set_stream(self, stream_ptr):
+        self._check(self._L.gkc_ctx_set_stream(self.h, C.c_void_p(stream_ptr)), "set_stream")
+
+    # ---- partition ----
+    def partition_host(self, reads, offs, prm):
+        reads = np.ascontiguousarray(reads, np.uint8)
+        offs = np.ascontiguousarray(offs, np.uint64)
+        v = PartitionView()
+        self._check(self._L.gkc_partition_host(self.h, C.byref(prm), _ptr(reads), _ptr(offs),
+                                               len(offs) - 1, C.byref(v)), "partition_host")
+        return v
+
+    def partition_device(self, d_reads, n_bytes, d_offs, n_reads, prm):
+        v = PartitionView()
+        self._check(self._L.gkc_partition_device(self.h, C.byref(prm), _ptr(d_reads), int(n_bytes),
+                                                 _ptr(d_offs), int(n_reads), C.byref(v)),
+                    "partition_device")
+        return v
+
+    def partition_copy_out(self, view):
+        """-> (bin_off, lens, byte_off, packed, minimizer) numpy arrays."""
+        n, nb = int(view.n_superkmers), int(view.nbins)
+        bin_off = np.zeros(nb + 1, np.uint64)
+        lens = np.zeros(max(n, 1), np.uint32)
+        boff = np.zeros(max(n, 1), np.uint64)
+        packed = np.zeros(max(int(view.n_packed_bytes), 1), np.uint8)
+        mm = np.zeros(max(n, 1), np.uint32)
+        self._check(self._L.gkc_partition_copy_out(self.h, _ptr(bin_off), _ptr(lens), _ptr(boff),
+                                                   _ptr(packed), _ptr(mm)), "partition_copy_out")
+        return bin_off, lens[:n], boff[:n], packed[:int(view.n_packed_bytes)], mm[:n]
+
+    # ---- count ----
+    def count_device(self, prm, mode=MODE_BATCHED):
+        v = CountView()
+        self._check(self._L.gkc_count_device(self.h, C.byref(prm), int(mode), C.byref(v)),
+                    "count_device")
+        return v
+
+    def count_superkmers_host(self, k, lens, packed, mode=MODE_BATCHED):
+        lens = np.ascontiguousarray(lens, np.uint32)
+        packed = np.ascontiguousarray(packed, np.uint8)
+        nd = C.c_uint64()
+        self._check(self._L.gkc_count_superkmers_host(self.h, int(k), _ptr(lens), _ptr(packed),
+                                                      len(lens), int(mode), C.byref(nd)),
+                    "count_superkmers_host")
+        return int(nd.value)
+
+    def count_copy_out(self, view):
+        """-> (bin_off, keys (n, key_words) uint64, counts)."""
+        nd, nb, kw = int(view.n_distinct), int(view.nbins), int(view.key_words)
+        bin_off = np.zeros(nb + 1, np.uint64)
+        keys = np.zeros(max(nd * kw, 1), np.uint64)
+        counts = np.zeros(max(nd, 1), np.uint32)
+        self._check(self._L.gkc_count_copy_out(self.h, _ptr(bin_off), _ptr(keys), _ptr(counts)),
+                    "count_copy_out")
+        return bin_off, keys[:nd * kw].reshape(nd, kw), counts[:nd]
+
+    # ---- pipeline ----
+    def pipeline_device(self, d_reads, n_bytes, d_offs, n_reads, prm, mode=MODE_BATCHED):
+        pv, cv = PartitionView(), CountView()
+        self._check(self._L.gkc_pipeline_device(self.h, C.byref(prm), int(mode), _ptr(d_reads),
+                                                int(n_bytes), _ptr(d_offs), int(n_reads),
+                                                C.byref(pv), C.byref(cv)), "pipeline_device")
+        return pv, cv
+
+    def pipeline_host(self, reads, offs, prm, mode=MODE_BATCHED):
+        reads = np.ascontiguousarray(reads, np.uint8)
+        offs = np.ascontiguousarray(offs, np.uint64)
+        cv = CountView()
+        self._check(self._L.gkc_pipeline_host(self.h, C.byref(prm), int(mode), _ptr(reads),
+                                              _ptr(offs), len(offs) - 1, C.byref(cv)),
+                    "pipeline_host")
+        return cv
+
+    def minimizers_device(self, d_reads, n_bytes, d_offs, n_reads, prm, d_mm, d_pos, d_strand):
+        self._check(self._L.gkc_minimizers_device(self.h, C.byref(prm), _ptr(d_reads), int(n_bytes),
+                                                  _ptr(d_offs), int(n_reads), _ptr(d_mm),
+                                                  _ptr(d_pos), _ptr(d_strand)), "minimizers")
+
+    def subsample_positions_device(self, d_reads, n_bytes, d_offs, n_reads, prm, mod):
+        v = PoslistView()
+        self._check(self._L.gkc_subsample_positions_device(self.h, C.byref(prm), int(mod),
+                                                           _ptr(d_reads), int(n_bytes), _ptr(d_offs),
+                                                           int(n_reads), C.byref(v)), "subsample")
+        return v
+
+    def hpc_device(self, d_reads, n_bytes, d_offs, n_reads, d_out, d_out_offs, d_orig):
+        self._check(self._L.gkc_hpc_device(self.h, _ptr(d_reads), int(n_bytes), _ptr(d_offs),
+                                           int(n_reads), _ptr(d_out), _ptr(d_out_offs),
+                                           _ptr(d_orig)), "hpc")
+
+
+def skms_from_copy(bin_off, lens, boff, packed):
+    """Per-superkmer bin ids from the bin offsets (for parity checks)."""
+    nb = len(bin_off) - 1
+    bins = np.repeat(np.arange(nb, dtype=np.uint32), np.diff(bin_off).astype(np.int64))
+    return bins, lens, boff, packed

@@ -1,0 +1,913 @@
+// C ABI: contexts, device workspaces, and the partition / count pipelines.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/gkc/gkc.h"
+#include "common.cuh"
+#include "ctx.h"
+#include "kernels.h"
+
+using namespace gkc;
+
+// ------------------------------------------------------------------ helpers
+
+const char *gkc_status_string(gkc_status s) {
+  switch (s) {
+    case GKC_OK: return "ok";
+    case GKC_ERR_INVALID_ARG: return "invalid argument";
+    case GKC_ERR_CUDA: return "CUDA error";
+    case GKC_ERR_NO_DEVICE: return "no CUDA device";
+    case GKC_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case GKC_ERR_BUDGET: return "HBM budget exceeded";
+    case GKC_ERR_CAPACITY: return "capacity exceeded";
+    case GKC_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+    case GKC_ERR_NOT_READY: return "not ready";
+    case GKC_ERR_CANCELLED: return "cancelled";
+    case GKC_ERR_NOT_FOUND: return "not found";
+    default: return "internal error";
+  }
+}
+
+int gkc_abi_version(void) { return GKC_ABI_VERSION; }
+
+// Stages of the batched pipeline, bounded by events sev[i] .. sev[i+1].
+static const char *kStageNames[] = {"prepare", "partition", "bin_scatter", "bucket_hist",
+                                    "bucket_scatter", "sort_count", "finalize"};
+constexpr int kNumStages = 7;
+const char *gkc_stage_name(int i) { return (i >= 0 && i < kNumStages) ? kStageNames[i] : ""; }
+
+// Records stage boundary i on the context stream (as a graph node while capturing).
+static void stage_mark(gkc_ctx *c, int i) {
+  if (c->capturing) cudaEventRecordWithFlags(c->sev[i], c->st, cudaEventRecordExternal);
+  else cudaEventRecord(c->sev[i], c->st);
+}
+
+static void read_stage_times(gkc_ctx *c) {
+  c->tm.n_stages = kNumStages;
+  for (int i = 0; i < kNumStages; i++) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, c->sev[i], c->sev[i + 1]) != cudaSuccess) {
+      cudaGetLastError();
+      ms = -1;
+    }
+    c->tm.stage_ms[i] = ms;
+  }
+}
+
+gkc_status ctx_fail(gkc_ctx *c, gkc_status s, const std::string &msg) {
+  if (c) c->err = msg;
+  return s;
+}
+
+gkc_status ctx_cuda(gkc_ctx *c, cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return GKC_OK;
+  cudaGetLastError();
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  return ctx_fail(c, e == cudaErrorMemoryAllocation ? GKC_ERR_OUT_OF_MEMORY : GKC_ERR_CUDA, m);
+}
+
+#define CK(call)                                                  \
+  do {                                                            \
+    gkc_status _s = ctx_cuda(c, (call), #call);                   \
+    if (_s != GKC_OK) return _s;                                  \
+  } while (0)
+#define LAUNCHED(c)                                               \
+  do {                                                            \
+    (c)->launches++;                                              \
+    cudaError_t _e = cudaPeekAtLastError();                       \
+    if (_e != cudaSuccess) return ctx_cuda((c), _e, "kernel launch"); \
+  } while (0)
+
+void *ws_get(gkc_ctx *c, const char *name, size_t bytes, gkc_status *st) {
+  *st = GKC_OK;
+  if (bytes == 0) bytes = 16;
+  bytes = (bytes + 255) & ~(size_t)255;
+  auto it = c->bufs.find(name);
+  if (it != c->bufs.end() && it->second.bytes >= bytes) return it->second.p;
+  size_t old = 0;
+  if (it != c->bufs.end()) {
+    old = it->second.bytes;
+    cudaFree(it->second.p);
+    c->used -= old;
+    c->bufs.erase(it);
+    c->graph_valid = false;
+  }
+  size_t want = std::max(bytes, old + old / 4);
+  if (c->budget && c->used + want > c->budget) want = bytes;
+  if (c->budget && c->used + want > c->budget) {
+    *st = ctx_fail(c, GKC_ERR_BUDGET, std::string("workspace '") + name + "' needs " +
+                                          std::to_string(bytes) + " bytes beyond the HBM budget");
+    return nullptr;
+  }
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, want);
+  if (e != cudaSuccess) {
+    *st = ctx_cuda(c, e, (std::string("cudaMalloc ") + name).c_str());
+    return nullptr;
+  }
+  c->used += want;
+  c->bufs[name] = DevBuf{p, want};
+  c->graph_valid = false;
+  return p;
+}
+
+#define WS(ptr, type, name, count)                                      \
+  type *ptr;                                                            \
+  do {                                                                  \
+    gkc_status _s;                                                      \
+    ptr = (type *)ws_get(c, name, sizeof(type) * (size_t)(count), &_s); \
+    if (_s != GKC_OK) return _s;                                        \
+  } while (0)
+
+// ------------------------------------------------------------------ context
+
+gkc_status gkc_ctx_create(int device_id, uint64_t hbm_budget_bytes, gkc_ctx **out) {
+  if (!out) return GKC_ERR_INVALID_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return GKC_ERR_NO_DEVICE;
+  }
+  if (device_id < 0 || device_id >= n) return GKC_ERR_INVALID_ARG;
+  gkc_ctx *c = new gkc_ctx();
+  c->dev = device_id;
+  c->budget = hbm_budget_bytes;
+  if (cudaSetDevice(device_id) != cudaSuccess) {
+    delete c;
+    return GKC_ERR_CUDA;
+  }
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, device_id);
+  c->n_sms = prop.multiProcessorCount;
+  c->max_smem_optin = (int)prop.sharedMemPerBlockOptin;
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMallocHost(&c->h_tot, sizeof(DevTotals)) != cudaSuccess) {
+    delete c;
+    return GKC_ERR_CUDA;
+  }
+  c->own_stream = true;
+  for (int i = 0; i < 4; i++) cudaEventCreate(&c->ev[i]);
+  for (int i = 0; i <= GKC_MAX_STAGES; i++) cudaEventCreate(&c->sev[i]);
+  *out = c;
+  return GKC_OK;
+}
+
+void gkc_ctx_destroy(gkc_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->dev);
+  if (c->st) cudaStreamSynchronize(c->st);
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  for (auto &kv : c->bufs) cudaFree(kv.second.p);
+  for (int i = 0; i < 4; i++)
+    if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  for (int i = 0; i <= GKC_MAX_STAGES; i++)
+    if (c->sev[i]) cudaEventDestroy(c->sev[i]);
+  if (c->h_tot) cudaFreeHost(c->h_tot);
+  if (c->own_stream && c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+const char *gkc_ctx_last_error(const gkc_ctx *c) { return c ? c->err.c_str() : "no context"; }
+
+gkc_status gkc_ctx_set_stream(gkc_ctx *c, void *stream) {
+  if (!c) return GKC_ERR_INVALID_ARG;
+  cudaSetDevice(c->dev);
+  cudaStreamSynchronize(c->st);
+  if (c->own_stream) cudaStreamDestroy(c->st);
+  c->st = (cudaStream_t)stream;
+  c->own_stream = false;
+  c->graph_valid = false;
+  return GKC_OK;
+}
+
+gkc_status gkc_ctx_synchronize(gkc_ctx *c) {
+  if (!c) return GKC_ERR_INVALID_ARG;
+  CK(cudaStreamSynchronize(c->st));
+  return GKC_OK;
+}
+
+uint64_t gkc_ctx_device_bytes(const gkc_ctx *c) { return c ? c->used : 0; }
+
+gkc_status gkc_ctx_release_workspace(gkc_ctx *c) {
+  if (!c) return GKC_ERR_INVALID_ARG;
+  cudaSetDevice(c->dev);
+  cudaStreamSynchronize(c->st);
+  if (c->gexec) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  for (auto &kv : c->bufs) cudaFree(kv.second.p);
+  c->bufs.clear();
+  c->used = 0;
+  c->graph_valid = false;
+  c->have_part = c->have_count = false;
+  return GKC_OK;
+}
+
+gkc_status gkc_last_timings(const gkc_ctx *c, gkc_timings *out) {
+  if (!c || !out) return GKC_ERR_INVALID_ARG;
+  *out = c->tm;
+  return GKC_OK;
+}
+
+// ------------------------------------------------------------- validation
+
+static gkc_status check_params(gkc_ctx *c, const gkc_params *prm) {
+  if (!prm) return ctx_fail(c, GKC_ERR_INVALID_ARG, "params is NULL");
+  if (prm->k < 1 || prm->k > 64) return ctx_fail(c, GKC_ERR_INVALID_ARG, "k must be in [1, 64]");
+  if (prm->p < 3 || prm->p > 16 || prm->p > prm->k)
+    return ctx_fail(c, GKC_ERR_INVALID_ARG, "p must be in [3, 16] and <= k");
+  if (prm->nbins < 1 || prm->nbins > (1 << 20))
+    return ctx_fail(c, GKC_ERR_INVALID_ARG, "nbins must be in [1, 2^20]");
+  return GKC_OK;
+}
+
+// --------------------------------------------------------------- totals
+
+__global__ void k_finalize(DevTotals *t, const unsigned long long *cursors, const uint32_t *err,
+                           const uint64_t *bin_kstart, uint32_t nbins, const uint64_t *n_bytes_dev,
+                           const uint64_t *bin_out) {
+  t->n_skm = cursors[0];
+  t->n_packed = cursors[1];
+  t->err = *err;
+  t->n_kmers = bin_kstart ? bin_kstart[nbins] : 0;
+  t->n_bytes = n_bytes_dev ? *n_bytes_dev : 0;
+  t->n_distinct = bin_out ? bin_out[nbins] : 0;
+}
+
+// ------------------------------------------------------------- partition
+
+// Capacity estimates for the superkmer outputs (exact sizes are re-derived
+// from the device cursors when a run overflows them).
+static void partition_caps(const gkc_params *prm, uint64_t n_bytes, uint64_t n_reads,
+                           uint64_t *cap_skm, uint64_t *cap_bytes) {
+  const double omega = prm->k - prm->p + 1;
+  uint64_t w = n_bytes;
+  uint64_t s = (uint64_t)((double)w * 3.0 / (omega + 1.0)) + n_reads + 4096;
+  if (s > w + 16) s = w + 16;
+  uint64_t tiles = n_bytes / kPartTile + 2;
+  *cap_skm = s;
+  *cap_bytes = (w + s * (uint64_t)(prm->k - 1)) / 4 + s + tiles * 16 + 64;
+}
+
+// Enqueues HPC (optional), partition and bin scatter on c->st.
+static gkc_status enqueue_partition(gkc_ctx *c, const gkc_params *prm, const char *d_reads,
+                                    uint64_t n_bytes, const uint64_t *d_offs, uint64_t n_reads,
+                                    uint64_t cap_skm, uint64_t cap_bytes) {
+  const uint32_t nbins = (uint32_t)prm->nbins;
+  const uint8_t *src = reinterpret_cast<const uint8_t *>(d_reads);
+  const uint64_t *offs = d_offs;
+  const uint64_t *nbytes_dev = nullptr;
+  WS(tot, unsigned long long, "cursors", 4);
+  WS(err, uint32_t, "err", 4);
+  stage_mark(c, 0);
+  CK(cudaMemsetAsync(tot, 0, 4 * sizeof(unsigned long long), c->st));
+  CK(cudaMemsetAsync(err, 0, 4 * sizeof(uint32_t), c->st));
+  c->part_hpc_reads = nullptr;
+  c->part_hpc_offs = nullptr;
+  c->part_hpc_orig = nullptr;
+  if (prm->hpc) {
+    WS(runlen, unsigned long long, "hpc_runlen", n_reads + 1);
+    WS(hoffs, uint64_t, "hpc_offs", n_reads + 2);
+    WS(hreads, uint8_t, "hpc_reads", n_bytes + 64);
+    WS(horig, int32_t, "hpc_orig", n_bytes + 16);
+    WS(stmp, uint64_t, "scan_tmp", scan_u64_tmp_words(n_reads + 1) + 8);
+    k_hpc_count<<<c->n_sms * 8, 256, 0, c->st>>>(src, offs, n_reads, runlen);
+    LAUNCHED(c);
+    scan_u64(runlen, hoffs, n_reads, stmp, c->st);
+    c->launches += 4;
+    k_hpc_write<<<c->n_sms * 8, 256, 0, c->st>>>(src, offs, n_reads, hoffs, hreads, horig);
+    LAUNCHED(c);
+    src = hreads;
+    offs = hoffs;
+    nbytes_dev = hoffs + n_reads;
+    c->part_hpc_reads = (const char *)hreads;
+    c->part_hpc_offs = hoffs;
+    c->part_hpc_orig = horig;
+  }
+  const uint64_t rs_words = (n_bytes + 1 + 31) / 32 + 2;
+  WS(rs, uint32_t, "rs_bits", rs_words);
+  CK(cudaMemsetAsync(rs, 0, rs_words * 4, c->st));
+  k_read_start_bits<<<(unsigned)std::min<uint64_t>((n_reads + 256) / 256, 65535), 256, 0, c->st>>>(
+      offs, n_reads, rs);
+  LAUNCHED(c);
+
+  WS(desc, uint64_t, "skm_desc_tile", cap_skm);
+  WS(mm, uint32_t, "skm_mm_tile", cap_skm);
+  WS(packed, uint8_t, "packed", cap_bytes);
+  WS(bin_nskm, unsigned long long, "bin_nskm", nbins + 1);
+  WS(bin_nkm, unsigned long long, "bin_nkmers", nbins + 1);
+  CK(cudaMemsetAsync(bin_nskm, 0, (nbins + 1) * 8, c->st));
+  CK(cudaMemsetAsync(bin_nkm, 0, (nbins + 1) * 8, c->st));
+
+  PartArgs a;
+  memset(&a, 0, sizeof(a));
+  a.reads = src;
+  a.nbytes = n_bytes;
+  a.nbytes_dev = nbytes_dev;
+  a.aligned16 = ((uintptr_t)src % 16) == 0;
+  a.rs_bits = rs;
+  a.rs_words = rs_words;
+  a.k = prm->k;
+  a.p = prm->p;
+  a.nbins = (int)nbins;
+  a.nbins_smem = nbins <= 1024 ? (int)((nbins + 1) & ~1u) : 0;
+  a.skm_desc = desc;
+  a.skm_mm = mm;
+  a.skm_gpos = nullptr;
+  a.packed = packed;
+  a.cursors = tot;
+  a.cap_skm = cap_skm;
+  a.cap_bytes = cap_bytes;
+  a.bin_nskm = bin_nskm;
+  a.bin_nkmers = bin_nkm;
+  a.err = err;
+  size_t smem = partition_smem_bytes(a.nbins_smem);
+  CK(cudaFuncSetAttribute(k_partition, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_partition, kPartThreads, smem));
+  uint64_t tiles = (n_bytes + kPartTile - 1) / kPartTile;
+  unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)c->n_sms * std::max(occ, 1)));
+  stage_mark(c, 1);
+  k_partition<<<grid, kPartThreads, smem, c->st>>>(a);
+  LAUNCHED(c);
+  stage_mark(c, 2);
+
+  WS(bin_start, uint64_t, "bin_start", nbins + 1);
+  WS(bin_kstart, uint64_t, "bin_kstart", nbins + 1);
+  k_bin_prefix<<<1, 32, 0, c->st>>>(bin_nskm, bin_nkm, nbins, bin_start, bin_kstart);
+  LAUNCHED(c);
+  WS(bfill, unsigned long long, "bin_fill", nbins + 1);
+  CK(cudaMemsetAsync(bfill, 0, (nbins + 1) * 8, c->st));
+  WS(bdesc, uint64_t, "skm_desc_bin", cap_skm);
+  WS(bmm, uint32_t, "skm_mm_bin", cap_skm);
+  k_bin_scatter<<<c->n_sms * 8, 256, 0, c->st>>>(tot, desc, mm, nbins, bin_start, bfill, bdesc,
+                                                 bmm, nullptr, nullptr, err);
+  LAUNCHED(c);
+
+  c->part_cap_skm = cap_skm;
+  c->part_cap_bytes = cap_bytes;
+  c->part_nbytes_dev = nbytes_dev;
+  return GKC_OK;
+}
+
+static gkc_status fill_partition_view(gkc_ctx *c, const gkc_params *prm, uint64_t n_reads,
+                                      uint64_t n_bytes) {
+  gkc_partition_view &v = c->pv;
+  memset(&v, 0, sizeof(v));
+  v.n_reads = n_reads;
+  v.n_bases = prm->hpc ? c->h_tot->n_bytes : n_bytes;
+  v.n_superkmers = c->h_tot->n_skm;
+  v.n_packed_bytes = c->h_tot->n_packed;
+  v.n_kmers = c->h_tot->n_kmers;
+  v.nbins = (uint32_t)prm->nbins;
+  v.bin_skm_off = (const uint64_t *)c->bufs["bin_start"].p;
+  v.bin_kmer_off = (const uint64_t *)c->bufs["bin_kstart"].p;
+  v.skm_desc = (const uint64_t *)c->bufs["skm_desc_bin"].p;
+  v.skm_minimizer = (const uint32_t *)c->bufs["skm_mm_bin"].p;
+  v.packed = (const uint8_t *)c->bufs["packed"].p;
+  v.hpc_reads = c->part_hpc_reads;
+  v.hpc_offs = c->part_hpc_offs;
+  v.hpc_orig_pos = c->part_hpc_orig;
+  c->pp = *prm;
+  c->have_part = true;
+  return GKC_OK;
+}
+
+static gkc_status read_totals(gkc_ctx *c, bool with_count, uint32_t nbins) {
+  const uint64_t *bk = (const uint64_t *)c->bufs["bin_kstart"].p;
+  const uint64_t *bo = with_count ? (const uint64_t *)c->bufs["bin_out"].p : nullptr;
+  WS(dt, DevTotals, "totals", 1);
+  k_finalize<<<1, 1, 0, c->st>>>(dt, (const unsigned long long *)c->bufs["cursors"].p,
+                                 (const uint32_t *)c->bufs["err"].p, bk, nbins, c->part_nbytes_dev, bo);
+  LAUNCHED(c);
+  CK(cudaMemcpyAsync(c->h_tot, dt, sizeof(DevTotals), cudaMemcpyDeviceToHost, c->st));
+  stage_mark(c, 7);
+  return GKC_OK;
+}
+
+static gkc_status check_device_err(gkc_ctx *c) {
+  uint32_t e = c->h_tot->err;
+  if (e & ERR_SPIN_TIMEOUT) return ctx_fail(c, GKC_ERR_DEVICE_TIMEOUT, "device look-back wait timed out");
+  if (e & ERR_BAD_READ) return ctx_fail(c, GKC_ERR_INVALID_ARG, "read longer than supported");
+  return GKC_OK;
+}
+
+gkc_status partition_device_impl(gkc_ctx *c, const gkc_params *prm, const char *d_reads,
+                                 uint64_t n_bytes, const uint64_t *d_offs, uint64_t n_reads) {
+  uint64_t cap_skm, cap_bytes;
+  partition_caps(prm, n_bytes, n_reads, &cap_skm, &cap_bytes);
+  for (int attempt = 0; attempt < 2; attempt++) {
+    c->graph_valid = false;
+    gkc_status s = enqueue_partition(c, prm, d_reads, n_bytes, d_offs, n_reads, cap_skm, cap_bytes);
+    if (s != GKC_OK) return s;
+    s = read_totals(c, false, (uint32_t)prm->nbins);
+    if (s != GKC_OK) return s;
+    CK(cudaStreamSynchronize(c->st));
+    if (!(c->h_tot->err & ERR_CAPACITY)) break;
+    cap_skm = c->h_tot->n_skm + 16;
+    cap_bytes = c->h_tot->n_packed + 64;
+    if (attempt == 1) return ctx_fail(c, GKC_ERR_CAPACITY, "partition capacity");
+  }
+  gkc_status s = check_device_err(c);
+  if (s != GKC_OK) return s;
+  return fill_partition_view(c, prm, n_reads, n_bytes);
+}
+
+gkc_status gkc_partition_device(gkc_ctx *c, const gkc_params *prm, const char *d_reads,
+                                uint64_t n_bytes, const uint64_t *d_offs, uint64_t n_reads,
+                                gkc_partition_view *out) {
+  if (!c) return GKC_ERR_INVALID_ARG;
+  gkc_status s = check_params(c, prm);
+  if (s != GKC_OK) return s;
+  if (n_bytes > 0 && (!d_reads || !d_offs)) return ctx_fail(c, GKC_ERR_INVALID_ARG, "null input");
+  cudaSetDevice(c->dev);
+  c->launches = 0;
+  CK(cudaEventRecord(c->ev[0], c->st));
+  s = partition_device_impl(c, prm, d_reads, n_bytes, d_offs, n_reads);
+  if (s != GKC_OK) return s;
+  CK(cudaEventRecord(c->ev[1], c->st));
+  CK(cudaEventSynchronize(c->ev[1]));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+  c->tm = gkc_timings{};
+  c->tm.partition_ms = ms;
+  c->tm.total_ms = ms;
+  c->tm.launches = c->launches;
+  if (out) *out = c->pv;
+  return GKC_OK;
+}
+
+// ------------------------------------------------------------------ count
+
+template <typename K>
+static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint64_t keys_cap,
+                                        uint64_t scratch_keys) {
+  const uint32_t nbins = (uint32_t)prm->nbins;
+  uint32_t max_bits = 12;
+  while (max_bits > 0 && ((uint64_t)nbins << max_bits) > (1ull << 22)) max_bits--;
+  const uint64_t max_buckets = (uint64_t)nbins << max_bits;
+  const int cap = sort_count_cap<K>();
+  WS(bin_bits, uint32_t, "bin_bits", nbins + 1);
+  WS(bucket_base, uint64_t, "bucket_base", nbins + 1);
+  WS(chunk_base, uint64_t, "chunk_base", nbins + 1);
+  CountPlan pl;
+  pl.nbins = nbins;
+  pl.bin_start = (const uint64_t *)c->bufs["bin_start"].p;
+  pl.bin_kstart = (const uint64_t *)c->bufs["bin_kstart"].p;
+  pl.target_bucket = (uint32_t)(cap * 2 / 5);
+  if (getenv("GKC_TARGET_BUCKET")) pl.target_bucket = (uint32_t)atoi(getenv("GKC_TARGET_BUCKET"));
+  pl.max_bits = max_bits;
+  pl.chunk_skm = 1024;
+  pl.k = prm->k;
+  pl.err = (const uint32_t *)c->bufs["err"].p;
+  pl.bin_bits = bin_bits;
+  pl.bucket_base = bucket_base;
+  pl.chunk_base = chunk_base;
+  stage_mark(c, 3);
+  k_count_plan<<<1, 32, 0, c->st>>>(pl);
+  LAUNCHED(c);
+
+  WS(bcount, unsigned long long, "bucket_count", max_buckets + 1);
+  WS(bstart, uint64_t, "bucket_start", max_buckets + 2);
+  WS(bcursor, unsigned long long, "bucket_cursor", max_buckets + 1);
+  WS(stmp, uint64_t, "scan_tmp2", scan_u64_tmp_words(max_buckets) + 8);
+  WS(keys, K, "keys", keys_cap);
+  WS(counts, uint32_t, "counts", keys_cap);
+  WS(err, uint32_t, "err", 4);
+  CK(cudaMemsetAsync(bcount, 0, (max_buckets + 1) * 8, c->st));
+
+  ExpandArgs ea;
+  memset(&ea, 0, sizeof(ea));
+  ea.desc = (const uint64_t *)c->bufs["skm_desc_bin"].p;
+  ea.packed = (const uint8_t *)c->bufs["packed"].p;
+  ea.nbins = nbins;
+  ea.bin_start = pl.bin_start;
+  ea.chunk_base = chunk_base;
+  ea.bin_bits = bin_bits;
+  ea.bucket_base = bucket_base;
+  ea.chunk_skm = pl.chunk_skm;
+  ea.k = prm->k;
+  ea.bucket_count = bcount;
+  ea.bucket_cursor = bcursor;
+  ea.keys = keys;
+  ea.keys_cap = keys_cap;
+  ea.err = err;
+  const unsigned ex_grid = c->n_sms * 8;
+  k_bucket_hist<K><<<ex_grid, 256, (1u << max_bits) * 4, c->st>>>(ea);
+  LAUNCHED(c);
+  scan_u64(bcount, bstart, max_buckets, stmp, c->st);
+  c->launches += 4;
+  CK(cudaMemcpyAsync(bcursor, bstart, max_buckets * 8, cudaMemcpyDeviceToDevice, c->st));
+  const size_t sc_smem = 4096 * 8 + 4096 * 4;
+  CK(cudaFuncSetAttribute(k_bucket_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc_smem));
+  stage_mark(c, 4);
+  k_bucket_scatter<K><<<ex_grid, 256, sc_smem, c->st>>>(ea);
+  LAUNCHED(c);
+
+  WS(status, unsigned long long, "lb_status", max_buckets + 1);
+  WS(ticket, unsigned long long, "lb_ticket", 2);
+  WS(bout, uint64_t, "bucket_out", max_buckets + 2);
+  scratch_keys = std::max<uint64_t>(scratch_keys, 4ull * cap);
+  WS(scratch, K, "sort_scratch", 2 * scratch_keys);
+  WS(scnt, uint32_t, "sort_scratch_cnt", 24 * 4096);
+  CK(cudaMemsetAsync(status, 0, (max_buckets + 1) * 8, c->st));
+  CK(cudaMemsetAsync(ticket, 0, 16, c->st));
+  SortCountArgs sa;
+  sa.bucket_start = bstart;
+  sa.n_buckets_dev = bucket_base + nbins;
+  sa.bucket_base = bucket_base;
+  sa.bin_bits = bin_bits;
+  sa.nbins = nbins;
+  sa.k = prm->k;
+  sa.keys = keys;
+  sa.out_keys = keys;  // in place: bucket i writes only below its own end (see count.cu)
+  sa.out_counts = counts;
+  sa.bucket_out = bout;
+  sa.status = status;
+  sa.ticket = ticket;
+  sa.scratch = scratch;
+  sa.scratch_keys = scratch_keys;
+  sa.scratch_cnt = scnt;
+  sa.err = err;
+  sa.prof = nullptr;
+  if (getenv("GKC_PROFILE_SORT")) {
+    WS(prof, unsigned long long, "sort_prof", 16);
+    CK(cudaMemsetAsync(prof, 0, 16 * 8, c->st));
+    sa.prof = prof;
+  }
+  const size_t smem = sort_count_smem_bytes<K>();
+  CK(cudaFuncSetAttribute(k_sort_count<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sort_count<K>, kSortThreads, smem));
+  stage_mark(c, 5);
+  unsigned sgrid = c->n_sms * std::max(occ, 1);
+  if (getenv("GKC_SORT_GRID")) sgrid = (unsigned)atoi(getenv("GKC_SORT_GRID"));
+  k_sort_count<K><<<sgrid, kSortThreads, smem, c->st>>>(sa);
+  LAUNCHED(c);
+  stage_mark(c, 6);
+  if (sa.prof && !c->capturing) {
+    unsigned long long h[16];
+    cudaMemcpyAsync(h, sa.prof, sizeof(h), cudaMemcpyDeviceToHost, c->st);
+    cudaStreamSynchronize(c->st);
+    fprintf(stderr,
+            "sort_count profile: grid=%u occ=%d smem=%zu buckets=%llu oversize=%llu keys=%llu big=%llu "
+            "cyc load=%llu sort=%llu runs=%llu lookback=%llu write=%llu\n",
+            sgrid, occ, smem, h[6], h[5], h[8], h[7], h[0], h[1], h[2], h[3], h[4]);
+  }
+  WS(bin_out, uint64_t, "bin_out", nbins + 1);
+  k_bin_out_offsets<<<(nbins + 256) / 256, 256, 0, c->st>>>(bout, bucket_base, nbins, bin_out);
+  LAUNCHED(c);
+  c->count_keys_cap = keys_cap;
+  return GKC_OK;
+}
+
+// Oversized buckets are sorted through a scratch area; it starts at 1/16 of
+// the keys and grows to the full key count if a bucket does not fit.
+static gkc_status enqueue_count(gkc_ctx *c, const gkc_params *prm, uint64_t keys_cap) {
+  uint64_t scratch = c->scratch_full ? keys_cap : keys_cap / 16;
+  if (prm->k <= 32) return enqueue_count_batched<uint64_t>(c, prm, keys_cap, scratch);
+  return enqueue_count_batched<u128>(c, prm, keys_cap, scratch);
+}
+
+static void fill_count_view(gkc_ctx *c, const gkc_params *prm) {
+  gkc_count_view &v = c->cv;
+  memset(&v, 0, sizeof(v));
+  v.n_distinct = c->h_tot->n_distinct;
+  v.n_kmers = c->h_tot->n_kmers;
+  v.nbins = (uint32_t)prm->nbins;
+  v.key_words = prm->k <= 32 ? 1 : 2;
+  v.bin_off = (const uint64_t *)c->bufs["bin_out"].p;
+  v.keys = (const uint64_t *)c->bufs["keys"].p;
+  v.counts = (const uint32_t *)c->bufs["counts"].p;
+  c->ck = prm->k;
+  c->have_count = true;
+}
+
+gkc_status count_device_impl(gkc_ctx *c, const gkc_params *prm, gkc_mode mode) {
+  if (!c->have_part) return ctx_fail(c, GKC_ERR_INVALID_ARG, "no partition in the context");
+  if (mode == GKC_MODE_PLAIN) return count_plain_impl(c, prm);
+  uint64_t n_kmers = c->pv.n_kmers;
+  uint64_t keys_cap = n_kmers + 16;
+  gkc_status s = GKC_OK;
+  for (int attempt = 0; attempt < 2; attempt++) {
+    CK(cudaMemsetAsync(c->bufs["err"].p, 0, 16, c->st));
+    s = enqueue_count(c, prm, keys_cap);
+    if (s != GKC_OK) return s;
+    s = read_totals(c, true, (uint32_t)prm->nbins);
+    if (s != GKC_OK) return s;
+    CK(cudaStreamSynchronize(c->st));
+    if (!(c->h_tot->err & ERR_OVERSIZE_SCRATCH)) break;
+    c->scratch_full = true;
+  }
+  if (c->h_tot->err & ERR_OVERSIZE_SCRATCH)
+    return ctx_fail(c, GKC_ERR_CAPACITY, "oversized bucket beyond sort scratch");
+  if (c->h_tot->err & ERR_CAPACITY) return ctx_fail(c, GKC_ERR_CAPACITY, "key capacity");
+  s = check_device_err(c);
+  if (s != GKC_OK) return s;
+  fill_count_view(c, prm);
+  return GKC_OK;
+}
+
+gkc_status gkc_count_device(gkc_ctx *c, const gkc_params *prm, gkc_mode mode, gkc_count_view *out) {
+  if (!c) return GKC_ERR_INVALID_ARG;
+  gkc_status s = check_params(c, prm);
+  if (s != GKC_OK) return s;
+  if (c->have_part && (prm->k != c->pp.k || prm->nbins != c->pp.nbins))
+    return ctx_fail(c, GKC_ERR_INVALID_ARG, "params differ from the partition's");
+  cudaSetDevice(c->dev);
+  c->launches = 0;
+  CK(cudaEventRecord(c->ev[0], c->st));
+  s = count_device_impl(c, prm, mode);
+  if (s != GKC_OK) return s;
+  CK(cudaEventRecord(c->ev[1], c->st));
+  CK(cudaEventSynchronize(c->ev[1]));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+  c->tm = gkc_timings{};
+  c->tm.count_ms = ms;
+  c->tm.total_ms = ms;
+  c->tm.launches = c->launches;
+  if (out) *out = c->cv;
+  return GKC_OK;
+}
+
+// -------------------------------------------------------------- pipeline
+
+// Batched: the whole partition -> count pipeline is enqueued once under
+// stream capture and replayed as a CUDA graph while inputs and parameters are
+// unchanged.  All sizes the kernels need are read on the device.
+static gkc_status pipeline_batched(gkc_ctx *c, const gkc_params *prm, const char *d_reads,
+                                   uint64_t n_bytes, const uint64_t *d_offs, uint64_t n_reads) {
+  GraphKey key{d_reads, d_offs, n_bytes, n_reads, prm->k, prm->p, prm->hpc, prm->nbins};
+  uint64_t cap_skm, cap_bytes;
+  partition_caps(prm, n_bytes, n_reads, &cap_skm, &cap_bytes);
+  if (c->graph_valid && c->gkey == key && c->gexec) {
+    cap_skm = c->part_cap_skm;
+    cap_bytes = c->part_cap_bytes;
+  }
+  uint64_t keys_cap = std::max<uint64_t>(n_bytes, 16);
+  if (c->graph_valid && c->gkey == key) keys_cap = c->count_keys_cap;
+  for (int attempt = 0; attempt < 3; attempt++) {
+    if (c->graph_valid && c->gkey == key && c->gexec) {
+      CK(cudaGraphLaunch(c->gexec, c->st));
+      c->tm.graph_replayed = 1;
+      c->launches = c->graph_launches;
+    } else {
+      // allocate every workspace outside capture: one dry enqueue sizes them
+      c->launches = 0;
+      CK(cudaStreamSynchronize(c->st));
+      if (c->gexec) {
+        cudaGraphExecDestroy(c->gexec);
+        c->gexec = nullptr;
+      }
+      cudaStreamCaptureStatus cs;
+      CK(cudaStreamIsCapturing(c->st, &cs));
+      if (cs != cudaStreamCaptureStatusNone) return ctx_fail(c, GKC_ERR_INVALID_ARG, "stream already capturing");
+      // size pass: plain enqueue (not captured) so that allocation happens now
+      gkc_status s = enqueue_partition(c, prm, d_reads, n_bytes, d_offs, n_reads, cap_skm, cap_bytes);
+      if (s == GKC_OK) s = enqueue_count(c, prm, keys_cap);
+      if (s == GKC_OK) s = read_totals(c, true, (uint32_t)prm->nbins);
+      if (s != GKC_OK) return s;
+      CK(cudaStreamSynchronize(c->st));
+      if (!(c->h_tot->err & (ERR_CAPACITY | ERR_OVERSIZE_SCRATCH))) {
+        // capture the same sequence into a graph for later replays
+        c->graph_valid = true;
+        uint32_t launches = c->launches;
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+        c->capturing = true;
+        c->launches = 0;
+        s = enqueue_partition(c, prm, d_reads, n_bytes, d_offs, n_reads, cap_skm, cap_bytes);
+        if (s == GKC_OK) s = enqueue_count(c, prm, keys_cap);
+        if (s == GKC_OK) s = read_totals(c, true, (uint32_t)prm->nbins);
+        cudaError_t e = cudaStreamEndCapture(c->st, &g);
+        c->capturing = false;
+        if (s != GKC_OK) return s;
+        CK(e);
+        if (!c->graph_valid) {  // a workspace moved during capture: do not keep it
+          cudaGraphDestroy(g);
+        } else {
+          CK(cudaGraphInstantiate(&c->gexec, g, 0));
+          cudaGraphDestroy(g);
+          c->gkey = key;
+          c->graph_launches = c->launches;
+        }
+        c->launches = launches;
+        c->tm.graph_replayed = 0;
+        break;
+      }
+    }
+    CK(cudaStreamSynchronize(c->st));
+    if (!(c->h_tot->err & (ERR_CAPACITY | ERR_OVERSIZE_SCRATCH))) break;
+    // grow to the sizes the device reported and retry
+    c->graph_valid = false;
+    if (c->h_tot->err & ERR_OVERSIZE_SCRATCH) c->scratch_full = true;
+    cap_skm = std::max<uint64_t>(cap_skm, c->h_tot->n_skm + 16);
+    cap_bytes = std::max<uint64_t>(cap_bytes, c->h_tot->n_packed + 64);
+    keys_cap = std::max<uint64_t>(keys_cap, c->h_tot->n_kmers + 16);
+    if (attempt == 2) return ctx_fail(c, GKC_ERR_CAPACITY, "pipeline capacity");
+  }
+  CK(cudaStreamSynchronize(c->st));
+  if (c->h_tot->err & (ERR_CAPACITY | ERR_OVERSIZE_SCRATCH)) {
+    c->graph_valid = false;
+    return ctx_fail(c, GKC_ERR_CAPACITY, "pipeline capacity");
+  }
+  gkc_status s = check_device_err(c);
+  if (s != GKC_OK) return s;
+  read_stage_times(c);
+  fill_partition_view(c, prm, n_reads, n_bytes);
+  fill_count_view(c, prm);
+  return GKC_OK;
+}
+
+gkc_status gkc_pipeline_device(gkc_ctx *c, const gkc_params *prm, gkc_mode mode,
+                               const char *d_reads, uint64_t n_bytes, const uint64_t *d_offs,
+                               uint64_t n_reads, gkc_partition_view *part, gkc_count_view *cnt) {
+  if (!c) return GKC_ERR_INVALID_ARG;
+  gkc_status s = check_params(c, prm);
+  if (s != GKC_OK) return s;
+  if (n_bytes > 0 && (!d_reads || !d_offs)) return ctx_fail(c, GKC_ERR_INVALID_ARG, "null input");
+  cudaSetDevice(c->dev);
+  c->tm = gkc_timings{};
+  CK(cudaEventRecord(c->ev[0], c->st));
+  if (mode == GKC_MODE_BATCHED) {
+    s = pipeline_batched(c, prm, d_reads, n_bytes, d_offs, n_reads);
+  } else {
+    c->launches = 0;
+    s = partition_plain_impl(c, prm, d_reads, n_bytes, d_offs, n_reads);
+    if (s == GKC_OK) {
+      CK(cudaEventRecord(c->ev[2], c->st));
+      s = count_plain_impl(c, prm);
+    }
+  }
+  if (s != GKC_OK) return s;
+  CK(cudaEventRecord(c->ev[1], c->st));
+  CK(cudaEventSynchronize(c->ev[1]));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+  c->tm.total_ms = ms;
+  c->tm.launches = c->launches;
+  if (part) *part = c->pv;
+  if (cnt) *cnt = c->cv;
+  return GKC_OK;
+}
+
+// Host entry: H2D of reads and rebased offsets, then the device pipeline.
+gkc_status upload_reads(gkc_ctx *c, const char *reads, const uint64_t *offs, uint64_t n_reads,
+                        char **d_reads, uint64_t **d_offs, uint64_t *n_bytes) {
+  const uint64_t base = n_reads ? offs[0] : 0;
+  const uint64_t nb = n_reads ? offs[n_reads] - base : 0;
+  WS(dr, char, "in_reads", nb + 64);
+  WS(doffs, uint64_t, "in_offs", n_reads + 1);
+  if (nb) CK(cudaMemcpyAsync(dr, reads + base, nb, cudaMemcpyHostToDevice, c->st));
+  if (base == 0) {
+    CK(cudaMemcpyAsync(doffs, offs, (n_reads + 1) * 8, cudaMemcpyHostToDevice, c->st));
+  } else {
+    c->offs_tmp.resize(n_reads + 1);
+    for (uint64_t r = 0; r <= n_reads; r++) c->offs_tmp[r] = offs[r] - base;
+    CK(cudaMemcpyAsync(doffs, c->offs_tmp.data(), (n_reads + 1) * 8, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  *d_reads = dr;
+  *d_offs = doffs;
+  *n_bytes = nb;
+  return GKC_OK;
+}
+
+gkc_status gkc_partition_host(gkc_ctx *c, const gkc_params *prm, const char *reads,
+                              const uint64_t *offs, uint64_t n_reads, gkc_partition_view *out) {
+  if (!c || (n_reads && (!reads || !offs))) return GKC_ERR_INVALID_ARG;
+  gkc_status s = check_params(c, prm);
+  if (s != GKC_OK) return s;
+  cudaSetDevice(c->dev);
+  char *dr;
+  uint64_t *doffs, nb;
+  s = upload_reads(c, reads, offs, n_reads, &dr, &doffs, &nb);
+  if (s != GKC_OK) return s;
+  return gkc_partition_device(c, prm, dr, nb, doffs, n_reads, out);
+}
+
+gkc_status gkc_pipeline_host(gkc_ctx *c, const gkc_params *prm, gkc_mode mode, const char *reads,
+                             const uint64_t *offs, uint64_t n_reads, gkc_count_view *cnt) {
+  if (!c || (n_reads && (!reads || !offs))) return GKC_ERR_INVALID_ARG;
+  gkc_status s = check_params(c, prm);
+  if (s != GKC_OK) return s;
+  cudaSetDevice(c->dev);
+  CK(cudaEventRecord(c->ev[3], c->st));
+  char *dr;
+  uint64_t *doffs, nb;
+  s = upload_reads(c, reads, offs, n_reads, &dr, &doffs, &nb);
+  if (s != GKC_OK) return s;
+  s = gkc_pipeline_device(c, prm, mode, dr, nb, doffs, n_reads, nullptr, cnt);
+  if (s != GKC_OK) return s;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[3], c->ev[0]);
+  c->tm.h2d_ms = ms;
+  return GKC_OK;
+}
+
+// --------------------------------------------------------------- copy out
+
+gkc_status gkc_partition_copy_out(gkc_ctx *c, uint64_t *bin_skm_off, uint32_t *skm_len,
+                                  uint64_t *skm_byte_off, uint8_t *packed, uint32_t *minimizer) {
+  if (!c || !c->have_part) return GKC_ERR_INVALID_ARG;
+  cudaSetDevice(c->dev);
+  const gkc_partition_view &v = c->pv;
+  if (bin_skm_off)
+    CK(cudaMemcpyAsync(bin_skm_off, v.bin_skm_off, (v.nbins + 1) * 8, cudaMemcpyDeviceToHost, c->st));
+  if (minimizer && v.n_superkmers)
+    CK(cudaMemcpyAsync(minimizer, v.skm_minimizer, v.n_superkmers * 4, cudaMemcpyDeviceToHost, c->st));
+  if (packed && v.n_packed_bytes)
+    CK(cudaMemcpyAsync(packed, v.packed, v.n_packed_bytes, cudaMemcpyDeviceToHost, c->st));
+  if ((skm_len || skm_byte_off) && v.n_superkmers) {
+    c->desc_tmp.resize(v.n_superkmers);
+    CK(cudaMemcpyAsync(c->desc_tmp.data(), v.skm_desc, v.n_superkmers * 8, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (uint64_t i = 0; i < v.n_superkmers; i++) {
+      if (skm_len) skm_len[i] = (uint32_t)(c->desc_tmp[i] & 0xFFFFFFu);
+      if (skm_byte_off) skm_byte_off[i] = c->desc_tmp[i] >> 24;
+    }
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return GKC_OK;
+}
+
+gkc_status gkc_count_copy_out(gkc_ctx *c, uint64_t *bin_off, uint64_t *keys, uint32_t *counts) {
+  if (!c || !c->have_count) return GKC_ERR_INVALID_ARG;
+  cudaSetDevice(c->dev);
+  const gkc_count_view &v = c->cv;
+  CK(cudaEventRecord(c->ev[2], c->st));
+  if (bin_off)
+    CK(cudaMemcpyAsync(bin_off, v.bin_off, (v.nbins + 1) * 8, cudaMemcpyDeviceToHost, c->st));
+  if (keys && v.n_distinct)
+    CK(cudaMemcpyAsync(keys, v.keys, v.n_distinct * 8 * v.key_words, cudaMemcpyDeviceToHost, c->st));
+  if (counts && v.n_distinct)
+    CK(cudaMemcpyAsync(counts, v.counts, v.n_distinct * 4, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaEventRecord(c->ev[3], c->st));
+  CK(cudaStreamSynchronize(c->st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
+  c->tm.d2h_ms = ms;
+  return GKC_OK;
+}
+
+// One bin of packed superkmers from the host (kmc_counting_GPU drop-in).
+gkc_status gkc_count_superkmers_host(gkc_ctx *c, int k, const uint32_t *skm_len,
+                                     const uint8_t *packed, uint64_t n_skm, gkc_mode mode,
+                                     uint64_t *n_distinct) {
+  if (!c || k < 1 || k > 64 || (n_skm && (!skm_len || !packed))) return GKC_ERR_INVALID_ARG;
+  cudaSetDevice(c->dev);
+  std::vector<uint64_t> desc(n_skm);
+  uint64_t off = 0, nk = 0;
+  for (uint64_t i = 0; i < n_skm; i++) {
+    if (skm_len[i] > 0xFFFFFFu) return ctx_fail(c, GKC_ERR_INVALID_ARG, "superkmer too long");
+    desc[i] = (off << 24) | skm_len[i];
+    off += (skm_len[i] + 3) / 4;
+    if (skm_len[i] >= (uint32_t)k) nk += skm_len[i] - k + 1;
+  }
+  WS(dd, uint64_t, "skm_desc_bin", n_skm + 1);
+  WS(dp, uint8_t, "packed", off + 16);
+  WS(dmm, uint32_t, "skm_mm_bin", n_skm + 1);
+  WS(bs, uint64_t, "bin_start", 2);
+  WS(bk, uint64_t, "bin_kstart", 2);
+  WS(cur, unsigned long long, "cursors", 4);
+  WS(err, uint32_t, "err", 4);
+  if (n_skm) CK(cudaMemcpyAsync(dd, desc.data(), n_skm * 8, cudaMemcpyHostToDevice, c->st));
+  if (off) CK(cudaMemcpyAsync(dp, packed, off, cudaMemcpyHostToDevice, c->st));
+  uint64_t hb[4] = {0, n_skm, 0, nk};
+  CK(cudaMemcpyAsync(bs, hb, 16, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(bk, hb + 2, 16, cudaMemcpyHostToDevice, c->st));
+  unsigned long long hc[4] = {n_skm, off, 0, 0};
+  CK(cudaMemcpyAsync(cur, hc, 32, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemsetAsync(err, 0, 16, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->pv = gkc_partition_view{};
+  c->pv.n_superkmers = n_skm;
+  c->pv.n_packed_bytes = off;
+  c->pv.n_kmers = nk;
+  c->pv.nbins = 1;
+  c->pv.bin_skm_off = bs;
+  c->pv.bin_kmer_off = bk;
+  c->pv.skm_desc = dd;
+  c->pv.skm_minimizer = dmm;
+  c->pv.packed = dp;
+  c->part_nbytes_dev = nullptr;
+  c->have_part = true;
+  gkc_params prm{k, 3, 0, 1};
+  c->pp = prm;
+  c->graph_valid = false;
+  gkc_status s = gkc_count_device(c, &prm, mode, nullptr);
+  if (s != GKC_OK) return s;
+  if (n_distinct) *n_distinct = c->cv.n_distinct;
+  return GKC_OK;
+}

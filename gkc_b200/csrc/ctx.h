@@ -1,0 +1,82 @@
+// Context state shared by the host-side translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/gkc/gkc.h"
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+// Small summary of a run, written on the device and read back once.
+struct DevTotals {
+  unsigned long long n_skm, n_packed;
+  uint32_t err, pad;
+  uint64_t n_kmers, n_bytes, n_distinct;
+};
+
+struct GraphKey {
+  const void *reads, *offs;
+  uint64_t n_bytes, n_reads;
+  int k, p, hpc, nbins;
+  bool operator==(const GraphKey &o) const {
+    return reads == o.reads && offs == o.offs && n_bytes == o.n_bytes && n_reads == o.n_reads &&
+           k == o.k && p == o.p && hpc == o.hpc && nbins == o.nbins;
+  }
+};
+
+struct gkc_ctx {
+  int dev = 0;
+  int n_sms = 148;
+  int max_smem_optin = 0;
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  uint64_t budget = 0, used = 0;
+  std::string err;
+  std::unordered_map<std::string, DevBuf> bufs;
+  DevTotals *h_tot = nullptr;  // pinned
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t sev[GKC_MAX_STAGES + 1] = {};  // stage boundaries of the batched pipeline
+  bool capturing = false;
+  uint32_t launches = 0;
+  gkc_timings tm{};
+  // partition state
+  gkc_params pp{};
+  bool have_part = false;
+  gkc_partition_view pv{};
+  uint64_t part_cap_skm = 0, part_cap_bytes = 0;
+  const uint64_t *part_nbytes_dev = nullptr;
+  const char *part_hpc_reads = nullptr;
+  const uint64_t *part_hpc_offs = nullptr;
+  const int32_t *part_hpc_orig = nullptr;
+  // count state
+  bool have_count = false;
+  int ck = 0;
+  gkc_count_view cv{};
+  uint64_t count_keys_cap = 0;
+  bool scratch_full = false;  // oversized buckets needed a full-size sort scratch
+  // graph of the batched pipeline
+  bool graph_valid = false;
+  GraphKey gkey{};
+  cudaGraphExec_t gexec = nullptr;
+  uint32_t graph_launches = 0;
+  // host scratch
+  std::vector<uint64_t> offs_tmp, desc_tmp;
+};
+
+gkc_status ctx_fail(gkc_ctx *c, gkc_status s, const std::string &msg);
+gkc_status ctx_cuda(gkc_ctx *c, cudaError_t e, const char *what);
+void *ws_get(gkc_ctx *c, const char *name, size_t bytes, gkc_status *st);
+gkc_status partition_plain_impl(gkc_ctx *c, const gkc_params *prm, const char *d_reads,
+                                uint64_t n_bytes, const uint64_t *d_offs, uint64_t n_reads);
+gkc_status count_plain_impl(gkc_ctx *c, const gkc_params *prm);
+gkc_status partition_device_impl(gkc_ctx *c, const gkc_params *prm, const char *d_reads,
+                                 uint64_t n_bytes, const uint64_t *d_offs, uint64_t n_reads);
+gkc_status count_device_impl(gkc_ctx *c, const gkc_params *prm, gkc_mode mode);
+gkc_status upload_reads(gkc_ctx *c, const char *reads, const uint64_t *offs, uint64_t n_reads,
+                        char **d_reads, uint64_t **d_offs, uint64_t *n_bytes);

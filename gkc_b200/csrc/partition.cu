@@ -1,0 +1,425 @@
+// Superkmer partitioning on the device.
+//
+// Semantics follow the reference's GPU_GenMinimizer / GPU_GenSKM /
+// SKMStore::add_skms (gkc_cuda.cu:234-324, superkmers.hpp:167-186):
+//   * every k-window of a read gets a canonical minimizer: the smallest
+//     forward or reverse-complement p-mer that passes the filter, else 4^p-1;
+//     windows touching a byte outside ACGTU follow the reference's exact
+//     per-window update rule (including its 255-code smear);
+//   * a superkmer is a maximal run of windows with equal minimizer value; its
+//     bases are packed 2 bits per base, MSB first, N as T, byte aligned;
+//   * its bin is minimizer % nbins.
+// Reads shorter than k produce nothing.
+//
+// The fused kernel is persistent and tiled over the concatenated read bytes:
+// each tile of PT_T window positions (+ halo) is loaded with 16-byte vector
+// loads into shared memory, minimizers are computed with a sliding-window
+// minimum over per-position filtered p-mer values, superkmer breaks are
+// compacted with a block scan, and the packed bytes are written as coalesced
+// 32-bit words.
+#include "common.cuh"
+#include "kernels.h"
+#include "minimizer.cuh"
+
+namespace gkc {
+
+constexpr int PT_NT = 512;
+constexpr int PT_T = 4096;                       // core windows per tile
+constexpr int PT_H = 512;                        // halo windows to find superkmer ends
+constexpr int PT_PRE = 64;                       // local index of the first core window
+constexpr int PT_NLOC = PT_PRE + PT_T + PT_H + 64;  // bytes held per tile (k <= 64)
+constexpr int PT_NW = PT_T + PT_H;               // windows with break flags
+constexpr int PT_WORDS = PT_NLOC / 32;
+constexpr int PT_PER_THREAD = PT_NW / PT_NT;     // 9 contiguous windows per thread
+static_assert(PT_NW % PT_NT == 0, "windows per thread");
+static_assert(PT_NLOC % 64 == 0, "tile alignment");
+
+struct PartSmem {
+  uint8_t cd[PT_NLOC];             // 2-bit code, or 255
+  uint32_t badw[PT_WORDS];         // bit i: byte i is not ACGTU
+  uint32_t rsw[PT_WORDS];          // bit i: a read starts at byte i
+  uint32_t validw[PT_WORDS];       // bit l: window l lies inside one read
+  union {
+    uint32_t g[PT_NLOC];           // filtered p-mer minimum per position, then suffix minima
+    uint32_t boff[PT_NLOC];        // per superkmer: byte offset in the tile
+  } a;
+  union {
+    uint32_t pre[PT_NLOC];         // prefix minima
+    uint32_t mm[PT_NLOC];          // window minimizer (after the window pass)
+  } b;
+  uint16_t brk[PT_NW + 1];         // local positions of breaks, ascending
+  uint16_t skm[PT_T + 1];          // break index of each core superkmer start
+  uint32_t scan_tmp[64];
+  uint64_t red_tmp[32];
+  int ext_end;                     // local end window of an extended last superkmer
+  uint32_t n_brk, n_skm, n_bytes;
+  unsigned long long base_skm, base_byte;
+};
+
+GKC_DEV bool bit_at(const uint32_t *w, int i) { return (w[i >> 5] >> (i & 31)) & 1u; }
+
+// Any bit set in [a, b] (inclusive), b - a < 96.
+GKC_DEV bool any_bits(const uint32_t *w, int a, int b) {
+  if (a > b) return false;
+  int wa = a >> 5, wb = b >> 5;
+  if (wa == wb) {
+    uint32_t m = (0xFFFFFFFFu >> (31 - (b & 31))) & (0xFFFFFFFFu << (a & 31));
+    return (w[wa] & m) != 0u;
+  }
+  if (w[wa] & (0xFFFFFFFFu << (a & 31))) return true;
+  for (int x = wa + 1; x < wb; x++)
+    if (w[x]) return true;
+  return (w[wb] & (0xFFFFFFFFu >> (31 - (b & 31)))) != 0u;
+}
+
+__global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  PartSmem &S = *reinterpret_cast<PartSmem *>(smem_raw);
+  const int tid = threadIdx.x;
+  const int k = a.k, p = a.p, omega = a.k - a.p + 1;
+  const uint32_t M = 0xFFFFFFFFu >> (32 - 2 * p);
+  if (a.nbytes_dev) a.nbytes = *a.nbytes_dev;
+  const uint64_t n_tiles = (a.nbytes + PT_T - 1) / PT_T;
+
+  // per-CTA bin histograms (small bin counts only)
+  unsigned long long *h_km = reinterpret_cast<unsigned long long *>(smem_raw + sizeof(PartSmem));
+  uint32_t *h_skm = reinterpret_cast<uint32_t *>(h_km + a.nbins_smem);
+  for (int i = tid; i < a.nbins_smem; i += PT_NT) {
+    h_skm[i] = 0;
+    h_km[i] = 0;
+  }
+
+  for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int64_t ts = (int64_t)tile * PT_T;
+    const int64_t G0 = ts - PT_PRE;  // global position of local 0 (64-aligned)
+
+    // ---- load bytes -> codes, bad-code bitmap, read-start bitmap ----
+    for (int q = tid * 16; q < PT_NLOC; q += PT_NT * 16) {
+      int64_t g = G0 + q;
+      uint8_t bytes[16];
+      if (g >= 0 && (uint64_t)(g + 16) <= a.nbytes && a.aligned16) {
+        uint4 v = __ldg(reinterpret_cast<const uint4 *>(a.reads + g));
+        *reinterpret_cast<uint4 *>(bytes) = v;
+#pragma unroll
+        for (int t = 0; t < 16; t++) S.cd[q + t] = (uint8_t)code_of_byte(bytes[t]);
+      } else {
+#pragma unroll
+        for (int t = 0; t < 16; t++) S.cd[q + t] = (uint8_t)global_code(a.reads, a.nbytes, g + t);
+      }
+    }
+    for (int w = tid; w < PT_WORDS; w += PT_NT) {
+      int64_t gw = (G0 >> 5) + w;  // G0 is a multiple of 64
+      S.rsw[w] = (gw >= 0 && (uint64_t)gw < a.rs_words) ? a.rs_bits[gw] : 0u;
+      S.validw[w] = 0u;
+    }
+    __syncthreads();
+    for (int w = tid; w < PT_WORDS; w += PT_NT) {
+      uint32_t m = 0;
+      const uint32_t *c4 = reinterpret_cast<const uint32_t *>(S.cd + w * 32);
+#pragma unroll
+      for (int t = 0; t < 8; t++) {
+        uint32_t x = c4[t];
+#pragma unroll
+        for (int u = 0; u < 4; u++) m |= (((x >> (8 * u)) & 0xFFu) == 255u ? 1u : 0u) << (t * 4 + u);
+      }
+      S.badw[w] = m;
+    }
+
+    // ---- filtered p-mer minimum per position (rolling, 16 positions a task) ----
+    {
+      const int npos = PT_NLOC - p + 1;
+      const int ntask = (npos + 15) / 16;
+      for (int task = tid; task < ntask; task += PT_NT) {
+        int a0 = task * 16;
+        uint32_t f = 0, r = 0;
+        for (int j = 0; j < p - 1; j++) {
+          uint32_t c = S.cd[a0 + j] & 3u;
+          f = (f << 2) | c;
+          r = (r >> 2) | ((3u - c) << (2 * p - 2));
+        }
+        int e = min(a0 + 16, npos);
+        for (int i = a0; i < e; i++) {
+          uint32_t c = S.cd[i + p - 1] & 3u;
+          f = ((f << 2) | c) & M;
+          r = (r >> 2) | ((3u - c) << (2 * p - 2));
+          uint32_t vf = mm_filter(f, p) ? f : M;
+          uint32_t vr = mm_filter(r, p) ? r : M;
+          S.a.g[i] = vf < vr ? vf : vr;
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- van Herk / Gil-Werman: prefix and suffix minima in blocks of omega ----
+    {
+      const int npos = PT_NLOC - p + 1;
+      const int nblk = (npos + omega - 1) / omega;
+      for (int blk = tid; blk < nblk; blk += PT_NT) {
+        int b0 = blk * omega, b1 = min(b0 + omega, npos);
+        uint32_t m = 0xFFFFFFFFu;
+        for (int i = b0; i < b1; i++) {
+          m = min(m, S.a.g[i]);
+          S.b.pre[i] = m;
+        }
+        m = 0xFFFFFFFFu;
+        for (int i = b1 - 1; i >= b0; i--) {
+          m = min(m, S.a.g[i]);
+          S.a.g[i] = m;  // suffix minima in place
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- window minimizers and validity for local windows [PRE-1, PRE+NW) ----
+    uint32_t mmv[PT_PER_THREAD + 1];
+    {
+      // strided ownership: window l = PRE-1 + tid + j*NT
+#pragma unroll
+      for (int j = 0; j <= PT_PER_THREAD; j++) {
+        int l = PT_PRE - 1 + tid + j * PT_NT;
+        mmv[j] = 0xFFFFFFFFu;
+        if (l < PT_PRE + PT_NW) {
+          int64_t s = G0 + l;
+          bool valid = s >= 0 && !any_bits(S.rsw, l + 1, l + k - 1) && (uint64_t)(s + k) <= a.nbytes;
+          if (valid) {
+            if (!any_bits(S.badw, l, l + k - 1)) {
+              mmv[j] = min(S.a.g[l], S.b.pre[l + omega - 1]);
+            } else {
+              const uint8_t *cw = S.cd + l;
+              mmv[j] = exact_window_minimizer([&](int i) { return (uint32_t)cw[i]; }, k, p);
+            }
+          }
+          // validity bit (atomicOr: several threads share a word)
+          if (valid) atomicOr(&S.validw[l >> 5], 1u << (l & 31));
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j <= PT_PER_THREAD; j++) {
+      int l = PT_PRE - 1 + tid + j * PT_NT;
+      if (l < PT_PRE + PT_NW) S.b.mm[l] = mmv[j];
+    }
+    __syncthreads();
+
+    // ---- breaks (window not valid, or a superkmer start) over [PRE, PRE+NW) ----
+    uint32_t nb_local = 0, ns_local = 0;
+    uint32_t brkbits = 0, startbits = 0;
+    const int lw0 = PT_PRE + tid * PT_PER_THREAD;
+#pragma unroll
+    for (int j = 0; j < PT_PER_THREAD; j++) {
+      int l = lw0 + j;
+      bool valid = bit_at(S.validw, l);
+      bool start = valid && (bit_at(S.rsw, l) || S.b.mm[l] != S.b.mm[l - 1] || !bit_at(S.validw, l - 1));
+      bool brk = !valid || start;
+      brkbits |= (brk ? 1u : 0u) << j;
+      bool core_start = start && l < PT_PRE + PT_T;
+      startbits |= (core_start ? 1u : 0u) << j;
+      nb_local += brk;
+      ns_local += core_start;
+    }
+    uint32_t tot;
+    uint32_t excl = block_exclusive_scan<PT_NT>(nb_local | (ns_local << 16), S.scan_tmp, &tot);
+    {
+      uint32_t bi = excl & 0xFFFFu, si = excl >> 16;
+#pragma unroll
+      for (int j = 0; j < PT_PER_THREAD; j++) {
+        if ((brkbits >> j) & 1u) {
+          if ((startbits >> j) & 1u) S.skm[si++] = (uint16_t)bi;
+          S.brk[bi++] = (uint16_t)(lw0 + j);
+        }
+      }
+    }
+    if (tid == 0) {
+      S.n_brk = tot & 0xFFFFu;
+      S.n_skm = tot >> 16;
+      S.ext_end = -1;
+    }
+    __syncthreads();
+    const uint32_t n_brk = S.n_brk, n_skm = S.n_skm;
+
+    // ---- the last core superkmer may run past the halo: extend it ----
+    if (n_skm > 0 && tid == 0) {
+      uint32_t jlast = S.skm[n_skm - 1];
+      if (jlast + 1 >= n_brk) {
+        int l = S.brk[jlast];
+        uint32_t mv = S.b.mm[l];
+        uint64_t w = (uint64_t)(G0 + PT_PRE + PT_NW);
+        // walk windows beyond the halo with the exact rule until a break
+        while (w < a.nbytes) {
+          if (global_rs(a.rs_bits, w) || !global_window_valid(a.rs_bits, a.nbytes, w, k)) break;
+          uint32_t v = exact_window_minimizer(
+              [&](int i) { return global_code(a.reads, a.nbytes, (int64_t)w + i); }, k, p);
+          if (v != mv) break;
+          w++;
+        }
+        S.ext_end = (int)((int64_t)w - G0);
+      }
+    }
+    __syncthreads();
+
+    // ---- superkmer sizes -> byte offsets (contiguous chunks of 8 per thread) ----
+    uint32_t my_bytes = 0;
+    const int sk0 = tid * 8;
+    for (int i = sk0; i < sk0 + 8 && i < (int)n_skm; i++) {
+      uint32_t j = S.skm[i];
+      int l = S.brk[j];
+      int e = (j + 1 < n_brk) ? S.brk[j + 1] : S.ext_end;
+      uint32_t len = (uint32_t)(e - l) + k - 1;
+      my_bytes += (len + 3) / 4;
+    }
+    uint32_t tile_bytes;
+    uint32_t boff = block_exclusive_scan<PT_NT>(my_bytes, S.scan_tmp, &tile_bytes);
+    // S.a.g is no longer needed: reuse it for per-superkmer byte offsets
+    for (int i = sk0; i < sk0 + 8 && i < (int)n_skm; i++) {
+      uint32_t j = S.skm[i];
+      int l = S.brk[j];
+      int e = (j + 1 < n_brk) ? S.brk[j + 1] : S.ext_end;
+      uint32_t len = (uint32_t)(e - l) + k - 1;
+      S.a.boff[i] = boff;
+      boff += (len + 3) / 4;
+    }
+    if (tid == 0) {
+      S.n_bytes = tile_bytes;
+      uint32_t rounded = (tile_bytes + 15u) & ~15u;
+      S.base_skm = n_skm ? atomicAdd(a.cursors + 0, (unsigned long long)n_skm) : 0ull;
+      S.base_byte = rounded ? atomicAdd(a.cursors + 1, (unsigned long long)rounded) : 0ull;
+      if (S.base_skm + n_skm > a.cap_skm || S.base_byte + rounded > a.cap_bytes)
+        atomicOr(a.err, ERR_CAPACITY);
+    }
+    __syncthreads();
+    const unsigned long long base_skm = S.base_skm, base_byte = S.base_byte;
+    const bool fits = base_skm + n_skm <= a.cap_skm && base_byte + ((tile_bytes + 15u) & ~15u) <= a.cap_bytes;
+
+    // ---- descriptors, bin histograms ----
+    for (int i = tid; i < (int)n_skm; i += PT_NT) {
+      uint32_t j = S.skm[i];
+      int l = S.brk[j];
+      int e = (j + 1 < n_brk) ? S.brk[j + 1] : S.ext_end;
+      uint32_t nk = (uint32_t)(e - l);
+      uint32_t len = nk + k - 1;
+      uint32_t mv = S.b.mm[l];
+      uint32_t bin = mv % (uint32_t)a.nbins;
+      if (len > 0xFFFFFFu) atomicOr(a.err, ERR_BAD_READ);
+      if (fits && len <= 0xFFFFFFu) {
+        uint64_t off = base_byte + S.a.boff[i];
+        a.skm_desc[base_skm + i] = (off << 24) | (uint64_t)len;
+        a.skm_mm[base_skm + i] = mv;
+        if (a.skm_gpos) a.skm_gpos[base_skm + i] = (uint64_t)(G0 + l);
+      }
+      if (bin < (uint32_t)a.nbins_smem) {
+        atomicAdd(&h_skm[bin], 1u);
+        atomicAdd(&h_km[bin], (unsigned long long)nk);
+      } else {
+        atomicAdd(&a.bin_nskm[bin], 1ull);
+        atomicAdd(&a.bin_nkmers[bin], (unsigned long long)nk);
+      }
+    }
+
+    // ---- packed bytes: one 32-bit word per thread step ----
+    if (fits) {
+      const uint32_t nwords = (tile_bytes + 3) / 4;
+      uint32_t *dst = reinterpret_cast<uint32_t *>(a.packed + base_byte);
+      for (uint32_t w = tid; w < nwords; w += PT_NT) {
+        uint32_t word = 0;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          uint32_t q = w * 4 + u;
+          if (q >= tile_bytes) break;
+          // superkmer holding byte q: last i with boff[i] <= q
+          int lo = 0, hi = (int)n_skm - 1;
+          while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (S.a.boff[mid] <= q) lo = mid; else hi = mid - 1;
+          }
+          uint32_t j = S.skm[lo];
+          int l = S.brk[j];
+          int e = (j + 1 < n_brk) ? S.brk[j + 1] : S.ext_end;
+          uint32_t len = (uint32_t)(e - l) + k - 1;
+          uint32_t bb = q - S.a.boff[lo];
+          uint32_t byte = 0;
+#pragma unroll
+          for (int t = 0; t < 4; t++) {
+            uint32_t bi = bb * 4 + t;
+            uint32_t c = 0;
+            if (bi < len) {
+              int lp = l + (int)bi;
+              c = (lp < PT_NLOC) ? (S.cd[lp] & 3u) : (global_code(a.reads, a.nbytes, G0 + lp) & 3u);
+            }
+            byte = (byte << 2) | c;
+          }
+          word |= byte << (8 * u);
+        }
+        dst[w] = word;
+      }
+    }
+    __syncthreads();
+  }
+
+  // flush bin histograms
+  for (int i = tid; i < a.nbins_smem; i += PT_NT) {
+    if (h_skm[i]) atomicAdd(&a.bin_nskm[i], (unsigned long long)h_skm[i]);
+    if (h_km[i]) atomicAdd(&a.bin_nkmers[i], h_km[i]);
+  }
+}
+
+size_t partition_smem_bytes(int nbins_smem) {
+  return sizeof(PartSmem) + (size_t)nbins_smem * (sizeof(uint32_t) + sizeof(unsigned long long)) + 16;
+}
+
+// Read-start bitmap: bit offs[r]-offs[0] for every read, plus bit nbytes as
+// the end-of-data sentinel.
+__global__ void k_read_start_bits(const uint64_t *offs, uint64_t n_reads, uint32_t *bits) {
+  uint64_t base = offs[0];
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r <= n_reads;
+       r += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t pos = offs[r] - base;
+    atomicOr(&bits[pos >> 5], 1u << (pos & 31));
+  }
+}
+
+// Counting sort of superkmer descriptors by bin, with warp-aggregated atomics
+// on the per-bin fill counters.
+__global__ void k_bin_scatter(const unsigned long long *n_skm_ptr, const uint64_t *desc,
+                              const uint32_t *mm, uint32_t nbins, const uint64_t *bin_start,
+                              unsigned long long *bin_fill, uint64_t *out_desc, uint32_t *out_mm,
+                              const uint64_t *gpos, uint64_t *out_gpos, const uint32_t *err) {
+  if (*err & (ERR_CAPACITY | ERR_BAD_READ)) return;  // outputs incomplete: the host re-runs
+  const uint64_t n = *n_skm_ptr;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i0 = blockIdx.x * (uint64_t)blockDim.x; i0 < n; i0 += stride) {
+    uint64_t i = i0 + threadIdx.x;
+    bool act = i < n;
+    uint32_t active = __ballot_sync(0xffffffffu, act);
+    if (!act) continue;
+    uint32_t m = mm[i];
+    uint32_t b = m % nbins;
+    uint32_t peers = __match_any_sync(active, b);
+    int leader = __ffs(peers) - 1;
+    uint32_t rank = __popc(peers & ((1u << lane_id()) - 1u));
+    unsigned long long base = 0;
+    if ((int)lane_id() == leader) base = atomicAdd(&bin_fill[b], (unsigned long long)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    uint64_t slot = bin_start[b] + base + rank;
+    out_desc[slot] = desc[i];
+    out_mm[slot] = m;
+    if (gpos) out_gpos[slot] = gpos[i];
+  }
+}
+
+// Exclusive scans of the per-bin counters (one thread; nbins is small).
+__global__ void k_bin_prefix(const unsigned long long *bin_nskm, const unsigned long long *bin_nkmers,
+                             uint32_t nbins, uint64_t *bin_start, uint64_t *bin_kstart) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint64_t cs = 0, ck = 0;
+  for (uint32_t b = 0; b < nbins; b++) {
+    bin_start[b] = cs;
+    bin_kstart[b] = ck;
+    cs += bin_nskm[b];
+    ck += bin_nkmers[b];
+  }
+  bin_start[nbins] = cs;
+  bin_kstart[nbins] = ck;
+}
+
+}  // namespace gkc

@@ -1,0 +1,232 @@
+/* gkc-b200: B200-native k-mer partitioning and counting (C ABI).
+ *
+ * Drop-in boundary for GKC's partition-and-count path.  Every entry point
+ * names the reference interface it replaces (paths relative to the GKC
+ * project root).  All entry points return a gkc_status; none exits the
+ * process (the reference's CUDA_CHECK calls exit(1), gkc_cuda.hpp:4-9).
+ * Plain pointers and sizes only: no C++ or framework types cross this ABI.
+ *
+ * Data conventions
+ *   reads    concatenated read bytes (ASCII; A/C/G/T/U in either case are
+ *            bases, anything else behaves like N)
+ *   offs     n_reads + 1 uint64 offsets into reads; read r is
+ *            reads[offs[r], offs[r+1]).  Device entry points require
+ *            offs[0] == 0; host entry points rebase.
+ *   superkmer descriptor (uint64): (packed byte offset << 24) | length in bases
+ *   packed   2 bits per base (A0 C1 G2 T3, N as T), first base in the top
+ *            bits of the first byte, each superkmer starting on a byte
+ *            boundary, last byte zero padded (superkmers.hpp:63-71)
+ *   k-mer    2k-bit canonical key min(x, revcomp(x)); k <= 32 keys are
+ *            uint64, k <= 64 keys are 16 bytes (low word first)
+ */
+#ifndef GKC_GKC_H
+#define GKC_GKC_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GKC_ABI_VERSION 1
+
+typedef enum gkc_status {
+  GKC_OK = 0,
+  GKC_ERR_INVALID_ARG = 1,
+  GKC_ERR_CUDA = 2,
+  GKC_ERR_NO_DEVICE = 3,
+  GKC_ERR_OUT_OF_MEMORY = 4,
+  GKC_ERR_BUDGET = 5,          /* request exceeds the context's HBM budget */
+  GKC_ERR_CAPACITY = 6,        /* internal buffer too small even after retry */
+  GKC_ERR_DEVICE_TIMEOUT = 7,  /* a bounded device-side wait expired */
+  GKC_ERR_NOT_READY = 8,
+  GKC_ERR_CANCELLED = 9,
+  GKC_ERR_NOT_FOUND = 10,
+  GKC_ERR_INTERNAL = 11
+} gkc_status;
+
+typedef struct gkc_ctx gkc_ctx;
+
+/* Parameters of one partition / count run.  Reference: K_kmer, P_minimizer,
+ * HPC and SKM_partitions of GenSuperkmerGPU (gkc_cuda.hpp:58-61). */
+typedef struct gkc_params {
+  int k;      /* 1..64 (reference: k <= 32) */
+  int p;      /* 3..16, p <= k */
+  int hpc;    /* collapse homopolymer runs before partitioning */
+  int nbins;  /* superkmer partitions: bin = minimizer % nbins */
+} gkc_params;
+
+typedef enum gkc_mode {
+  GKC_MODE_BATCHED = 0, /* persistent kernels, whole pipeline in one CUDA graph */
+  GKC_MODE_PLAIN = 1    /* per-stage, per-batch / per-bin launches */
+} gkc_mode;
+
+/* Device-resident partition (valid until the next call on the context). */
+typedef struct gkc_partition_view {
+  uint64_t n_reads, n_bases;      /* after HPC when enabled */
+  uint64_t n_superkmers, n_packed_bytes, n_kmers;
+  uint32_t nbins;
+  const uint64_t *bin_skm_off;    /* nbins+1: superkmers of bin b are [off[b], off[b+1]) */
+  const uint64_t *bin_kmer_off;   /* nbins+1: k-mer prefix per bin */
+  const uint64_t *skm_desc;       /* bin-ordered descriptors */
+  const uint32_t *skm_minimizer;  /* bin-ordered minimizer values */
+  const uint8_t *packed;
+  const char *hpc_reads;          /* HPC only: compacted reads, offsets, */
+  const uint64_t *hpc_offs;       /*   and in-read original position of  */
+  const int32_t *hpc_orig_pos;    /*   every kept base; else NULL        */
+} gkc_partition_view;
+
+/* Device-resident counts: per bin, ascending canonical keys with counts. */
+typedef struct gkc_count_view {
+  uint64_t n_distinct, n_kmers;
+  uint32_t nbins;
+  int key_words;             /* 1 (k <= 32) or 2 (k <= 64) uint64 per key */
+  const uint64_t *bin_off;   /* nbins+1 */
+  const uint64_t *keys;      /* n_distinct * key_words */
+  const uint32_t *counts;    /* n_distinct, clamped to 2^32-1 */
+} gkc_count_view;
+
+#define GKC_MAX_STAGES 8
+typedef struct gkc_timings {
+  float partition_ms, count_ms, total_ms, h2d_ms, d2h_ms;
+  uint32_t launches;        /* kernels launched by the last pipeline call */
+  uint32_t graph_replayed;  /* 1 if the batched pipeline ran from a cached graph */
+  uint32_t n_stages;        /* batched pipeline: device time of each stage */
+  float stage_ms[GKC_MAX_STAGES];
+} gkc_timings;
+/* Name of stage i of the batched pipeline ("partition", "sort_count", ...). */
+const char *gkc_stage_name(int i);
+
+/* ---- context (reference: GPUReset gkc_cuda.cu:367-373; CUDAParams.device_id) ---- */
+gkc_status gkc_ctx_create(int device_id, uint64_t hbm_budget_bytes, gkc_ctx **out);
+void gkc_ctx_destroy(gkc_ctx *ctx);
+const char *gkc_ctx_last_error(const gkc_ctx *ctx);
+const char *gkc_status_string(gkc_status s);
+gkc_status gkc_ctx_set_stream(gkc_ctx *ctx, void *cuda_stream);
+gkc_status gkc_ctx_synchronize(gkc_ctx *ctx);
+uint64_t gkc_ctx_device_bytes(const gkc_ctx *ctx);
+gkc_status gkc_ctx_release_workspace(gkc_ctx *ctx);
+gkc_status gkc_last_timings(const gkc_ctx *ctx, gkc_timings *out);
+int gkc_abi_version(void);
+
+/* ---- partition (reference: GenSuperkmerGPU gkc_cuda.cu:376-541 with the
+ *      process_func SKMStore::add_skms, superkmers.hpp:167-186) ---- */
+gkc_status gkc_partition_device(gkc_ctx *ctx, const gkc_params *prm, const char *d_reads,
+                                uint64_t n_bytes, const uint64_t *d_offs, uint64_t n_reads,
+                                gkc_partition_view *out);
+gkc_status gkc_partition_host(gkc_ctx *ctx, const gkc_params *prm, const char *reads,
+                              const uint64_t *offs, uint64_t n_reads, gkc_partition_view *out);
+/* Copies the context's partition to host arrays sized from the view:
+ * bin_skm_off[nbins+1], skm_len[n_superkmers], skm_byte_off[n_superkmers]
+ * (into `packed`), packed[n_packed_bytes], minimizer[n_superkmers] (may be NULL). */
+gkc_status gkc_partition_copy_out(gkc_ctx *ctx, uint64_t *bin_skm_off, uint32_t *skm_len,
+                                  uint64_t *skm_byte_off, uint8_t *packed, uint32_t *minimizer);
+
+/* ---- counting (reference: kmc_counting_GPU kmer_counting.cu:59-199, per bin) ---- */
+/* Counts the context's current partition, all bins. */
+gkc_status gkc_count_device(gkc_ctx *ctx, const gkc_params *prm, gkc_mode mode,
+                            gkc_count_view *out);
+/* One group of packed superkmers in host memory (one bin), as
+ * kmc_counting_GPU takes one SKMStore: lengths and each superkmer's bytes
+ * back to back.  The distinct count is returned in *n_distinct; the sorted
+ * list can then be fetched with gkc_count_copy_out. */
+gkc_status gkc_count_superkmers_host(gkc_ctx *ctx, int k, const uint32_t *skm_len,
+                                     const uint8_t *packed, uint64_t n_skm, gkc_mode mode,
+                                     uint64_t *n_distinct);
+/* Copies the last count result: bin_off[nbins+1], keys[n_distinct*key_words],
+ * counts[n_distinct]; any pointer may be NULL. */
+gkc_status gkc_count_copy_out(gkc_ctx *ctx, uint64_t *bin_off, uint64_t *keys, uint32_t *counts);
+
+/* ---- whole pipeline: reads -> superkmer partitions -> sorted (k-mer, count)
+ *      (reference: process_reads_count + gen_skm_and_count_with_TP,
+ *      experiment.cpp:76-89,156-219) ---- */
+gkc_status gkc_pipeline_device(gkc_ctx *ctx, const gkc_params *prm, gkc_mode mode,
+                               const char *d_reads, uint64_t n_bytes, const uint64_t *d_offs,
+                               uint64_t n_reads, gkc_partition_view *part, gkc_count_view *cnt);
+gkc_status gkc_pipeline_host(gkc_ctx *ctx, const gkc_params *prm, gkc_mode mode,
+                             const char *reads, const uint64_t *offs, uint64_t n_reads,
+                             gkc_count_view *cnt);
+
+/* ---- per-window minimizers with position and strand (reference declares
+ *      d_mm_pos / d_mm_strand, gkc_cuda.cu:159-160, but never fills them).
+ *      Arrays have n_bytes entries indexed by window start in the CSR;
+ *      windows that do not fit in their read hold minimizer 0xFFFFFFFF. ---- */
+gkc_status gkc_minimizers_device(gkc_ctx *ctx, const gkc_params *prm, const char *d_reads,
+                                 uint64_t n_bytes, const uint64_t *d_offs, uint64_t n_reads,
+                                 uint32_t *d_minimizer, uint8_t *d_pos, int8_t *d_strand);
+
+/* ---- sub-sampled counting with position lists: k-mers whose window
+ *      minimizer % mod == 0, each with the ascending list of its window start
+ *      offsets in the CSR (README.md:16 use case; no reference code). ---- */
+typedef struct gkc_poslist_view {
+  uint64_t n_distinct, n_positions;
+  int key_words;
+  const uint64_t *keys;      /* ascending */
+  const uint64_t *pos_off;   /* n_distinct + 1 */
+  const uint32_t *positions;
+} gkc_poslist_view;
+gkc_status gkc_subsample_positions_device(gkc_ctx *ctx, const gkc_params *prm, uint32_t mod,
+                                          const char *d_reads, uint64_t n_bytes,
+                                          const uint64_t *d_offs, uint64_t n_reads,
+                                          gkc_poslist_view *out);
+
+/* ---- homopolymer compression alone (reference: GPU_HPCEncoding
+ *      gkc_cuda.cu:164-192, with the per-read start index) ---- */
+gkc_status gkc_hpc_device(gkc_ctx *ctx, const char *d_reads, uint64_t n_bytes,
+                          const uint64_t *d_offs, uint64_t n_reads, char *d_out_reads,
+                          uint64_t *d_out_offs, int32_t *d_orig_pos);
+
+/* ---- serving: continuous batching of counting jobs against an HBM budget ---- */
+typedef struct gkc_server gkc_server;
+typedef enum gkc_job_state {
+  GKC_JOB_QUEUED = 0,
+  GKC_JOB_RUNNING = 1,
+  GKC_JOB_DONE = 2,
+  GKC_JOB_FAILED = 3,
+  GKC_JOB_CANCELLED = 4
+} gkc_job_state;
+typedef struct gkc_job_info {
+  gkc_job_state state;
+  gkc_status status;
+  uint64_t n_bases, n_kmers, n_distinct;
+  uint32_t nbins;
+  int key_words;
+  double submit_s, start_s, end_s;   /* seconds since server start */
+  uint64_t hbm_bytes;                /* admitted budget */
+} gkc_job_info;
+gkc_status gkc_server_create(int device_id, uint64_t hbm_budget_bytes, int max_running,
+                             gkc_server **out);
+void gkc_server_destroy(gkc_server *srv);
+/* The server copies the reads; the caller may free them after return. */
+gkc_status gkc_server_submit(gkc_server *srv, const gkc_params *prm, const char *reads,
+                             const uint64_t *offs, uint64_t n_reads, uint64_t *job_id);
+gkc_status gkc_server_submit_device_synth(gkc_server *srv, const gkc_params *prm, int generator,
+                                          uint64_t seed, uint64_t n_bases, uint64_t *job_id);
+gkc_status gkc_server_poll(gkc_server *srv, uint64_t job_id, gkc_job_info *info);
+gkc_status gkc_server_wait(gkc_server *srv, uint64_t job_id, double timeout_s, gkc_job_info *info);
+gkc_status gkc_server_cancel(gkc_server *srv, uint64_t job_id);
+gkc_status gkc_server_copy_result(gkc_server *srv, uint64_t job_id, uint64_t *bin_off,
+                                  uint64_t *keys, uint32_t *counts);
+gkc_status gkc_server_release(gkc_server *srv, uint64_t job_id);
+uint64_t gkc_job_hbm_estimate(const gkc_params *prm, uint64_t n_bases, uint64_t n_reads);
+
+/* ---- synthetic workloads (seeded; same bytes on host and device) ---- */
+gkc_status gkc_synth_iid_reads(int on_device, uint64_t seed, uint64_t n_reads, uint32_t read_len,
+                               double n_rate, char *out, uint64_t *offs);
+gkc_status gkc_synth_genome(int on_device, uint64_t seed, uint64_t genome_len,
+                            double seg_fraction, double divergence, uint8_t *genome_codes);
+gkc_status gkc_synth_short_reads(int on_device, uint64_t seed, const uint8_t *genome_codes,
+                                 uint64_t genome_len, uint64_t first_read, uint64_t n_reads,
+                                 uint32_t read_len, double err_rate, char *out, uint64_t *offs);
+/* Long-read lengths (host only): lognormal(median, sigma) clipped to
+ * [min_len, max_len], until the sum reaches total_bases; returns the count. */
+uint64_t gkc_synth_long_read_offsets(uint64_t seed, double median, double sigma, uint32_t min_len,
+                                     uint32_t max_len, uint64_t total_bases, uint64_t max_reads,
+                                     uint64_t *offs);
+gkc_status gkc_synth_long_reads(int on_device, uint64_t seed, const uint8_t *genome_codes,
+                                uint64_t genome_len, uint64_t n_reads, const uint64_t *offs,
+                                char *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,209 @@
+"""Parity of the CUDA path (through the C ABI) with the reference's golden
+fixtures and with the oracle.  Partition: identical per-bin multisets of
+(length, packed bytes).  Count: identical per-bin sorted (k-mer, count)."""
+import numpy as np
+import pytest
+
+import gkc_b200 as G
+import golden_cases as GC
+import oracle_ffi as F
+import parity as P
+from gpu_helpers import assert_counts_equal, lib_counts, lib_partition
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = G.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("name", sorted(GC.index()["full"].keys()))
+def test_golden_full(ctx, name):
+    meta, d = GC.full_case(name)
+    k, p, hpc, nb = meta["k"], meta["p"], meta["hpc"], meta["nbins"]
+    skm, _ = lib_partition(ctx, d["reads"], d["offs"], k, p, hpc, nb)
+    assert skm.multisets(nb) == GC.multisets_from_case(d, nb)
+    got, _ = lib_counts(ctx, k, nb)
+    want = dict(bin_off=d["cnt_bin_off"], keys_lo=d["cnt_keys"], counts=d["cnt_counts"])
+    assert_counts_equal(got, want)
+
+
+@pytest.mark.parametrize("name", sorted(GC.index()["digest"].keys()))
+def test_golden_digest(ctx, name):
+    c = GC.index()["digest"][name]
+    reads, offs = GC.digest_case_reads(c)
+    skm, v = lib_partition(ctx, reads, offs, c["k"], c["p"], c["hpc"], c["nbins"])
+    assert v.n_superkmers == c["n_skm"]
+    assert P.partition_digest(skm.multisets(c["nbins"])) == c["partition_sha256"]
+    got, cv = lib_counts(ctx, c["k"], c["nbins"])
+    assert cv.n_kmers == c["n_kmers"]
+    assert P.counts_digest(got["bin_off"], got["keys_lo"], got["counts"]) == c["counts_sha256"]
+
+
+def random_reads(seed, n, lo, hi, alphabet=b"ACGTacgtU", n_rate=0.01):
+    r = np.random.default_rng(seed)
+    lens = r.integers(lo, hi + 1, n)
+    offs = np.zeros(n + 1, np.uint64)
+    offs[1:] = np.cumsum(lens)
+    b = np.frombuffer(alphabet, np.uint8)[r.integers(0, len(alphabet), int(offs[-1]))].copy()
+    b[r.random(len(b)) < n_rate] = ord("N")
+    return b, offs
+
+
+CASES = [
+    # seed, n, lo, hi, k, p, hpc, nbins
+    (1, 400, 31, 900, 31, 11, 0, 256),
+    (2, 300, 21, 700, 21, 7, 1, 31),
+    (3, 200, 17, 5000, 17, 9, 0, 5),
+    (4, 100, 40, 3000, 27, 13, 1, 100),
+    (5, 300, 32, 400, 32, 16, 0, 64),
+    (6, 500, 12, 100, 12, 4, 0, 3),
+    (7, 200, 45, 500, 45, 15, 0, 128),    # 128-bit keys
+    (8, 120, 63, 900, 63, 13, 0, 256),    # config-4 shape
+    (9, 80, 64, 400, 64, 16, 1, 7),
+]
+
+
+@pytest.mark.parametrize("seed,n,lo,hi,k,p,hpc,nb", CASES)
+def test_random_vs_oracle(ctx, seed, n, lo, hi, k, p, hpc, nb):
+    reads, offs = random_reads(seed, n, lo, hi)
+    o = F.oracle_partition(reads, offs, k, p, hpc, nb)
+    skm, _ = lib_partition(ctx, reads, offs, k, p, hpc, nb)
+    assert skm.multisets(nb) == o.multisets(nb)
+    want = F.oracle_count_bins(o, k, nb)
+    got, _ = lib_counts(ctx, k, nb)
+    assert_counts_equal(got, want)
+
+
+def test_short_and_empty_reads(ctx):
+    reads = np.frombuffer(b"ACGTACGTAC" * 10, np.uint8).copy()
+    offs = np.array([0, 0, 5, 5, 36, 37, 100], np.uint64)
+    k, p, nb = 31, 11, 16
+    o = F.oracle_partition(reads, offs, k, p, 0, nb)
+    skm, _ = lib_partition(ctx, reads, offs, k, p, 0, nb)
+    assert skm.multisets(nb) == o.multisets(nb)
+    got, _ = lib_counts(ctx, k, nb)
+    assert_counts_equal(got, F.oracle_count_bins(o, k, nb))
+
+
+def test_empty_input(ctx):
+    reads = np.zeros(0, np.uint8)
+    offs = np.zeros(1, np.uint64)
+    skm, v = lib_partition(ctx, reads, offs, 31, 11, 0, 8)
+    assert v.n_superkmers == 0
+    got, cv = lib_counts(ctx, 31, 8)
+    assert cv.n_distinct == 0 and np.all(got["bin_off"] == 0)
+
+
+def test_homopolymer_reads_oversize_bucket(ctx):
+    """All-A reads: one superkmer per read, every k-mer equal -> one bucket far
+    larger than shared memory (global MSD path, all-equal leaf)."""
+    reads = np.frombuffer(b"A" * 20000 + b"C" * 3000 + b"A" * 9000, np.uint8).copy()
+    offs = np.array([0, 20000, 23000, 32000], np.uint64)
+    k, p, nb = 31, 11, 4
+    o = F.oracle_partition(reads, offs, k, p, 0, nb)
+    skm, _ = lib_partition(ctx, reads, offs, k, p, 0, nb)
+    assert skm.multisets(nb) == o.multisets(nb)
+    got, _ = lib_counts(ctx, k, nb)
+    assert_counts_equal(got, F.oracle_count_bins(o, k, nb))
+
+
+def test_low_complexity_oversize_mixed(ctx):
+    """Mostly-A reads with sparse other bases: many distinct keys share long
+    prefixes, so buckets overflow shared memory and split recursively."""
+    r = np.random.default_rng(21)
+    n, L = 60, 5000
+    b = np.full(n * L, ord("A"), np.uint8)
+    m = r.random(n * L) < 0.02
+    b[m] = np.frombuffer(b"CGT", np.uint8)[r.integers(0, 3, int(m.sum()))]
+    offs = np.arange(0, n * L + 1, L, dtype=np.uint64)
+    k, p, nb = 31, 11, 2
+    o = F.oracle_partition(b, offs, k, p, 0, nb)
+    skm, _ = lib_partition(ctx, b, offs, k, p, 0, nb)
+    assert skm.multisets(nb) == o.multisets(nb)
+    got, _ = lib_counts(ctx, k, nb)
+    assert_counts_equal(got, F.oracle_count_bins(o, k, nb))
+
+
+def test_long_superkmer_beyond_tile_halo(ctx):
+    """A superkmer spanning far more windows than one tile plus halo."""
+    unit = b"A" * 9000
+    rng = np.random.default_rng(3)
+    tail = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 3000)].tobytes()
+    reads = np.frombuffer(tail + unit + tail, np.uint8).copy()
+    offs = np.array([0, len(reads)], np.uint64)
+    k, p, nb = 25, 15, 64
+    o = F.oracle_partition(reads, offs, k, p, 0, nb)
+    skm, _ = lib_partition(ctx, reads, offs, k, p, 0, nb)
+    assert skm.multisets(nb) == o.multisets(nb)
+
+
+def test_pipeline_batched_matches_two_step(ctx):
+    import torch
+    reads, offs = random_reads(31, 3000, 150, 150, alphabet=b"ACGT", n_rate=0.001)
+    k, p, nb = 31, 11, 256
+    o = F.oracle_partition(reads, offs, k, p, 0, nb)
+    want = F.oracle_count_bins(o, k, nb)
+    d_reads = torch.from_numpy(reads).cuda()
+    d_offs = torch.from_numpy(offs.view(np.int64)).cuda()
+    for _ in range(3):  # first call captures the graph, later calls replay it
+        pv, cv = ctx.pipeline_device(d_reads, len(reads), d_offs, len(offs) - 1, G.params(k, p, nb))
+        bin_off, keys, counts = ctx.count_copy_out(cv)
+        assert_counts_equal(dict(bin_off=bin_off, keys_lo=keys[:, 0], counts=counts), want)
+    assert ctx.timings().graph_replayed == 1
+
+
+def test_count_superkmers_host_one_bin(ctx):
+    """kmc_counting_GPU drop-in: one bin's packed superkmers from the host."""
+    meta, d = GC.full_case("iid_n")
+    nb, k = meta["nbins"], meta["k"]
+    for b in (0, 17, 255):
+        sel = d["skm_bin"] == b
+        lens = d["skm_len"][sel]
+        chunks = [d["skm_bytes"][int(o):int(o) + (int(l) + 3) // 4] for o, l in zip(d["skm_off"][sel], lens)]
+        packed = np.concatenate(chunks) if chunks else np.zeros(0, np.uint8)
+        nd = ctx.count_superkmers_host(k, lens, packed)
+        lo, hi = int(d["cnt_bin_off"][b]), int(d["cnt_bin_off"][b + 1])
+        assert nd == hi - lo == int(d["cnt_returned"][b])
+        _, keys, counts = ctx.count_copy_out(ctx.count_device(G.params(k, 3, 1)))
+        assert np.array_equal(keys[:, 0], d["cnt_keys"][lo:hi])
+        assert np.array_equal(counts, d["cnt_counts"][lo:hi])
+
+
+PLAIN_CASES = [
+    (11, 300, 31, 900, 31, 11, 0, 256),
+    (12, 200, 21, 700, 21, 7, 1, 31),
+    (13, 100, 63, 600, 63, 13, 0, 64),
+]
+
+
+@pytest.mark.parametrize("seed,n,lo,hi,k,p,hpc,nb", PLAIN_CASES)
+def test_plain_mode_vs_oracle(ctx, seed, n, lo, hi, k, p, hpc, nb):
+    """The plain per-stage form (per-window minimizers, per-read superkmers,
+    per-bin onesweep sort) gives the same partition and counts."""
+    import torch
+    reads, offs = random_reads(seed, n, lo, hi)
+    o = F.oracle_partition(reads, offs, k, p, hpc, nb)
+    want = F.oracle_count_bins(o, k, nb)
+    d_reads = torch.from_numpy(reads).cuda()
+    d_offs = torch.from_numpy(offs.view(np.int64)).cuda()
+    pv, cv = ctx.pipeline_device(d_reads, len(reads), d_offs, len(offs) - 1, G.params(k, p, nb, hpc),
+                                 mode=G.MODE_PLAIN)
+    bo, lens, boff, packed, _ = ctx.partition_copy_out(pv)
+    bins = np.repeat(np.arange(nb, dtype=np.uint32), np.diff(bo).astype(np.int64))
+    assert F.Skms(bins, lens, boff, packed).multisets(nb) == o.multisets(nb)
+    bin_off, keys, counts = ctx.count_copy_out(cv)
+    got = dict(bin_off=bin_off, keys_lo=keys[:, 0].copy(), counts=counts,
+               keys_hi=keys[:, 1].copy() if keys.shape[1] > 1 else None)
+    assert_counts_equal(got, want)
+
+
+def test_plain_count_after_fused_partition(ctx):
+    meta, d = GC.full_case("mixed_defaults")
+    k, p, hpc, nb = meta["k"], meta["p"], meta["hpc"], meta["nbins"]
+    lib_partition(ctx, d["reads"], d["offs"], k, p, hpc, nb)
+    got, _ = lib_counts(ctx, k, nb, mode=G.MODE_PLAIN)
+    assert_counts_equal(got, dict(bin_off=d["cnt_bin_off"], keys_lo=d["cnt_keys"], counts=d["cnt_counts"]))

@@ -1,0 +1,89 @@
+"""CPU-side checks of the shipped library: it loads, exports every symbol the
+public header declares, rejects use without a device, and its host-side
+generators produce the same bytes as the numpy mirror."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import gkc_b200 as G
+from gkc_b200 import synth
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    src = open(os.path.join(ROOT, "include", "gkc", "gkc.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gkc_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_header_symbol():
+    L = G.lib()
+    missing = [s for s in header_symbols() if not hasattr(L, s)]
+    assert not missing, missing
+    assert L.gkc_abi_version() == 1
+
+
+def test_binding_covers_header():
+    bound = {n for n, _, _ in G.SIGNATURES}
+    assert set(header_symbols()) <= bound
+
+
+def test_status_strings():
+    L = G.lib()
+    assert L.gkc_status_string(0) == b"ok"
+    assert L.gkc_status_string(5) == b"HBM budget exceeded"
+
+
+@pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES") is None and False, reason="")
+def test_ctx_create_without_device_fails_cleanly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    h = C.c_void_p()
+    st = G.lib().gkc_ctx_create(0, 0, C.byref(h))
+    assert st == 3  # GKC_ERR_NO_DEVICE
+
+
+def test_host_iid_generator_matches_numpy():
+    n, L = 50, 150
+    out = np.zeros(n * L, np.uint8)
+    offs = np.zeros(n + 1, np.uint64)
+    assert G.lib().gkc_synth_iid_reads(0, 5, n, L, 0.01, out.ctypes.data, offs.ctypes.data) == 0
+    r2, o2 = synth.iid_reads(5, n, L, 0.01)
+    assert np.array_equal(out, r2) and np.array_equal(offs, o2)
+
+
+def test_host_genome_and_short_reads_match_numpy():
+    Gl = 60000
+    g = np.zeros(Gl, np.uint8)
+    assert G.lib().gkc_synth_genome(0, 3, Gl, 0.05, 0.01, g.ctypes.data) == 0
+    g2 = synth.genome(3, Gl)
+    assert np.array_equal(g, g2)
+    n, L = 300, 150
+    out = np.zeros(n * L, np.uint8)
+    offs = np.zeros(n + 1, np.uint64)
+    assert G.lib().gkc_synth_short_reads(0, 3, g.ctypes.data, Gl, 7, n, L, 0.005, out.ctypes.data,
+                                         offs.ctypes.data) == 0
+    r2, o2 = synth.short_reads(3, g2, n, L, 0.005, first_read=7)
+    assert np.array_equal(out, r2)
+
+
+def test_host_long_reads_are_deterministic():
+    Gl = 100000
+    g = np.zeros(Gl, np.uint8)
+    G.lib().gkc_synth_genome(0, 4, Gl, 0.05, 0.01, g.ctypes.data)
+    offs = np.zeros(1001, np.uint64)
+    n = G.lib().gkc_synth_long_read_offsets(4, 8000.0, 0.6, 1000, 50000, 200000, 1000, offs.ctypes.data)
+    assert 5 < n < 200 and offs[n] >= 200000
+    lens = np.diff(offs[:n + 1])
+    assert lens.min() >= 1000 and lens.max() <= 50000
+    a = np.zeros(int(offs[n]), np.uint8)
+    b = np.zeros(int(offs[n]), np.uint8)
+    for buf in (a, b):
+        assert G.lib().gkc_synth_long_reads(0, 4, g.ctypes.data, Gl, n, offs.ctypes.data, buf.ctypes.data) == 0
+    assert np.array_equal(a, b)
+    assert set(np.unique(a).tolist()) <= set(b"ACGT")
