@@ -301,8 +301,8 @@ def run_ours(args, wl):
     peak, peak_kind = peaks()
 
     # dominant kernel and its model bytes per launch
-    kernel_bytes = {"partition": model["partition"], "bucket_scatter": model["expand"],
-                    "sort_count": model["sort"] + model["count"]}
+    kernel_bytes = {"partition": model["partition"], "coarse_scatter": model["expand"],
+                    "coarse_count": model["sort"] + model["count"]}
     dom = max(kernel_bytes, key=lambda s: stages.get(s, 0.0))
     dom_ms = stages[dom]
     achieved = kernel_bytes[dom] / (dom_ms / 1000.0) / 1e9

@@ -39,8 +39,8 @@ const char *gkc_status_string(gkc_status s) {
 int gkc_abi_version(void) { return GKC_ABI_VERSION; }
 
 // Stages of the batched pipeline, bounded by events sev[i] .. sev[i+1].
-static const char *kStageNames[] = {"prepare", "partition", "bin_scatter", "bucket_hist",
-                                    "bucket_scatter", "sort_count", "finalize"};
+static const char *kStageNames[] = {"prepare", "partition", "bin_scatter", "coarse_hist",
+                                    "coarse_scatter", "coarse_count", "compact"};
 constexpr int kNumStages = 7;
 const char *gkc_stage_name(int i) { return (i >= 0 && i < kNumStages) ? kStageNames[i] : ""; }
 
@@ -397,6 +397,12 @@ static gkc_status read_totals(gkc_ctx *c, bool with_count, uint32_t nbins) {
 
 static gkc_status check_device_err(gkc_ctx *c) {
   uint32_t e = c->h_tot->err;
+  if (e & ERR_BOUNDS) {
+    unsigned long long d[3] = {0, 0, 0};
+    cudaMemcpy(d, c->bufs["dbg"].p, sizeof(d), cudaMemcpyDeviceToHost);
+    return ctx_fail(c, GKC_ERR_INTERNAL, "device bounds check " + std::to_string(d[0]) + " failed: index " +
+                                             std::to_string(d[1]) + " limit " + std::to_string(d[2]));
+  }
   if (e & ERR_SPIN_TIMEOUT) return ctx_fail(c, GKC_ERR_DEVICE_TIMEOUT, "device look-back wait timed out");
   if (e & ERR_BAD_READ) return ctx_fail(c, GKC_ERR_INVALID_ARG, "read longer than supported");
   return GKC_OK;
@@ -453,120 +459,144 @@ template <typename K>
 static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint64_t keys_cap,
                                         uint64_t scratch_keys) {
   const uint32_t nbins = (uint32_t)prm->nbins;
-  uint32_t max_bits = 12;
-  while (max_bits > 0 && ((uint64_t)nbins << max_bits) > (1ull << 22)) max_bits--;
+  uint32_t max_bits = kCoarseMaxBits;
+  while (max_bits > 0 && ((uint64_t)nbins << max_bits) > (1ull << 20)) max_bits--;
   const uint64_t max_buckets = (uint64_t)nbins << max_bits;
   const int cap = sort_count_cap<K>();
+  const uint64_t cap_skm = std::max<uint64_t>(c->part_cap_skm, 1);
+  WS(err, uint32_t, "err", 4);
+  const unsigned long long *n_skm_dev = (const unsigned long long *)c->bufs["cursors"].p;
+  const uint64_t *desc = (const uint64_t *)c->bufs["skm_desc_bin"].p;
+  const uint64_t *bin_start = (const uint64_t *)c->bufs["bin_start"].p;
+  const uint64_t *bin_kstart = (const uint64_t *)c->bufs["bin_kstart"].p;
+
+  // k-mer offset of every bin-ordered superkmer
+  stage_mark(c, 3);
+  WS(nk, unsigned long long, "skm_nk", cap_skm + 1);
+  WS(koff, uint64_t, "skm_koff", cap_skm + 2);
+  WS(stmp, uint64_t, "scan_tmp2", scan_u64_tmp_words(std::max<uint64_t>(cap_skm, max_buckets) + 1) + 8);
+  k_skm_nk<<<c->n_sms * 8, 256, 0, c->st>>>(desc, n_skm_dev, prm->k, nk);
+  LAUNCHED(c);
+  scan_u64_dev(nk, koff, cap_skm, (const uint64_t *)n_skm_dev, stmp, c->st);
+  c->launches += 4;
+
   WS(bin_bits, uint32_t, "bin_bits", nbins + 1);
   WS(bucket_base, uint64_t, "bucket_base", nbins + 1);
   WS(chunk_base, uint64_t, "chunk_base", nbins + 1);
+  WS(hist_base, uint64_t, "hist_base", nbins + 1);
   CountPlan pl;
   pl.nbins = nbins;
-  pl.bin_start = (const uint64_t *)c->bufs["bin_start"].p;
-  pl.bin_kstart = (const uint64_t *)c->bufs["bin_kstart"].p;
-  pl.target_bucket = (uint32_t)(cap * 2 / 5);
-  if (getenv("GKC_TARGET_BUCKET")) pl.target_bucket = (uint32_t)atoi(getenv("GKC_TARGET_BUCKET"));
+  pl.bin_start = bin_start;
+  pl.bin_kstart = bin_kstart;
+  pl.coarse_target = kCoarseTarget;
+  if (getenv("GKC_COARSE_TARGET")) pl.coarse_target = (uint32_t)atoi(getenv("GKC_COARSE_TARGET"));
   pl.max_bits = max_bits;
-  pl.chunk_skm = 1024;
+  pl.chunk_kmers = kChunkKmers;
   pl.k = prm->k;
-  pl.err = (const uint32_t *)c->bufs["err"].p;
+  pl.err = err;
   pl.bin_bits = bin_bits;
   pl.bucket_base = bucket_base;
   pl.chunk_base = chunk_base;
-  stage_mark(c, 3);
+  pl.hist_base = hist_base;
   k_count_plan<<<1, 32, 0, c->st>>>(pl);
   LAUNCHED(c);
 
-  WS(bcount, unsigned long long, "bucket_count", max_buckets + 1);
-  WS(bstart, uint64_t, "bucket_start", max_buckets + 2);
-  WS(bcursor, unsigned long long, "bucket_cursor", max_buckets + 1);
-  WS(stmp, uint64_t, "scan_tmp2", scan_u64_tmp_words(max_buckets) + 8);
+  const uint64_t hist_cap = ((keys_cap / kChunkKmers) + nbins + 1) << max_bits;
+  WS(chunk_hist, unsigned long long, "chunk_hist", hist_cap + 1);
+  WS(chunk_off, uint64_t, "chunk_off", hist_cap + 2);
+  WS(stmp4, uint64_t, "scan_tmp4", scan_u64_tmp_words(hist_cap + 1) + 8);
   WS(keys, K, "keys", keys_cap);
-  WS(counts, uint32_t, "counts", keys_cap);
-  WS(err, uint32_t, "err", 4);
-  CK(cudaMemsetAsync(bcount, 0, (max_buckets + 1) * 8, c->st));
-
   ExpandArgs ea;
   memset(&ea, 0, sizeof(ea));
-  ea.desc = (const uint64_t *)c->bufs["skm_desc_bin"].p;
+  ea.desc = desc;
+  ea.koff = koff;
   ea.packed = (const uint8_t *)c->bufs["packed"].p;
   ea.nbins = nbins;
-  ea.bin_start = pl.bin_start;
+  ea.bin_start = bin_start;
+  ea.bin_kstart = bin_kstart;
   ea.chunk_base = chunk_base;
+  ea.hist_base = hist_base;
   ea.bin_bits = bin_bits;
-  ea.bucket_base = bucket_base;
-  ea.chunk_skm = pl.chunk_skm;
+  ea.max_bits = max_bits;
+  ea.chunk_kmers = kChunkKmers;
   ea.k = prm->k;
-  ea.bucket_count = bcount;
-  ea.bucket_cursor = bcursor;
+  ea.chunk_hist = chunk_hist;
+  ea.chunk_off = chunk_off;
   ea.keys = keys;
   ea.keys_cap = keys_cap;
   ea.err = err;
   const unsigned ex_grid = c->n_sms * 8;
-  k_bucket_hist<K><<<ex_grid, 256, (1u << max_bits) * 4, c->st>>>(ea);
+  k_coarse_hist<K><<<ex_grid, 256, (1u << max_bits) * 4, c->st>>>(ea);
   LAUNCHED(c);
-  scan_u64(bcount, bstart, max_buckets, stmp, c->st);
+  scan_u64_dev(chunk_hist, chunk_off, hist_cap, hist_base + nbins, stmp4, c->st);
   c->launches += 4;
-  CK(cudaMemcpyAsync(bcursor, bstart, max_buckets * 8, cudaMemcpyDeviceToDevice, c->st));
-  const size_t sc_smem = 4096 * 8 + 4096 * 4;
-  CK(cudaFuncSetAttribute(k_bucket_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc_smem));
   stage_mark(c, 4);
-  k_bucket_scatter<K><<<ex_grid, 256, sc_smem, c->st>>>(ea);
+  k_coarse_scatter<K><<<ex_grid, 256, (1u << max_bits) * 12, c->st>>>(ea);
   LAUNCHED(c);
 
-  WS(status, unsigned long long, "lb_status", max_buckets + 1);
+  WS(tkeys, K, "tmp_keys", keys_cap);
+  WS(tcounts, uint32_t, "tmp_counts", keys_cap);
+  WS(cstart, uint64_t, "coarse_start", max_buckets + 1);
+  WS(cd, unsigned long long, "coarse_d", max_buckets + 1);
+  WS(cout_, uint64_t, "coarse_out", max_buckets + 2);
   WS(ticket, unsigned long long, "lb_ticket", 2);
-  WS(bout, uint64_t, "bucket_out", max_buckets + 2);
   scratch_keys = std::max<uint64_t>(scratch_keys, 4ull * cap);
   WS(scratch, K, "sort_scratch", 2 * scratch_keys);
   WS(scnt, uint32_t, "sort_scratch_cnt", 24 * 4096);
-  CK(cudaMemsetAsync(status, 0, (max_buckets + 1) * 8, c->st));
   CK(cudaMemsetAsync(ticket, 0, 16, c->st));
   SortCountArgs sa;
-  sa.bucket_start = bstart;
-  sa.n_buckets_dev = bucket_base + nbins;
-  sa.bucket_base = bucket_base;
-  sa.bin_bits = bin_bits;
+  memset(&sa, 0, sizeof(sa));
   sa.nbins = nbins;
   sa.k = prm->k;
+  sa.bucket_base = bucket_base;
+  sa.chunk_base = chunk_base;
+  sa.hist_base = hist_base;
+  sa.bin_bits = bin_bits;
+  sa.chunk_off = chunk_off;
   sa.keys = keys;
-  sa.out_keys = keys;  // in place: bucket i writes only below its own end (see count.cu)
-  sa.out_counts = counts;
-  sa.bucket_out = bout;
-  sa.status = status;
+  sa.tmp_keys = tkeys;
+  sa.tmp_counts = tcounts;
+  sa.coarse_start = cstart;
+  sa.coarse_d = cd;
   sa.ticket = ticket;
+  sa.scratch_lock = ticket + 1;
   sa.scratch = scratch;
   sa.scratch_keys = scratch_keys;
   sa.scratch_cnt = scnt;
   sa.err = err;
+  sa.probe_limit = 256;
+  sa.tmp_cap = keys_cap;
+  WS(dbg, unsigned long long, "dbg", 8);
+  CK(cudaMemsetAsync(dbg, 0, 64, c->st));
+  sa.dbg = dbg;
+  if (getenv("GKC_PROBE_LIMIT")) sa.probe_limit = atoi(getenv("GKC_PROBE_LIMIT"));
   sa.prof = nullptr;
   if (getenv("GKC_PROFILE_SORT")) {
     WS(prof, unsigned long long, "sort_prof", 16);
     CK(cudaMemsetAsync(prof, 0, 16 * 8, c->st));
     sa.prof = prof;
   }
-  const size_t smem = sort_count_smem_bytes<K>();
-  CK(cudaFuncSetAttribute(k_sort_count<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int occ = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sort_count<K>, kSortThreads, smem));
+  const size_t smem = coarse_smem_bytes<K>();
+  CK(cudaFuncSetAttribute(k_coarse_count<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   stage_mark(c, 5);
-  unsigned sgrid = c->n_sms * std::max(occ, 1);
-  if (getenv("GKC_SORT_GRID")) sgrid = (unsigned)atoi(getenv("GKC_SORT_GRID"));
-  k_sort_count<K><<<sgrid, kSortThreads, smem, c->st>>>(sa);
+  k_coarse_count<K><<<c->n_sms, kSortThreads, smem, c->st>>>(sa);
   LAUNCHED(c);
   stage_mark(c, 6);
   if (sa.prof && !c->capturing) {
     unsigned long long h[16];
     cudaMemcpyAsync(h, sa.prof, sizeof(h), cudaMemcpyDeviceToHost, c->st);
     cudaStreamSynchronize(c->st);
-    fprintf(stderr,
-            "sort_count profile: grid=%u occ=%d smem=%zu buckets=%llu oversize=%llu keys=%llu big=%llu "
-            "cyc load=%llu sort=%llu runs=%llu lookback=%llu write=%llu\n",
-            sgrid, occ, smem, h[6], h[5], h[8], h[7], h[0], h[1], h[2], h[3], h[4]);
+    fprintf(stderr, "coarse_count profile: fallback slices=%llu\n", h[5]);
   }
-  WS(bin_out, uint64_t, "bin_out", nbins + 1);
-  k_bin_out_offsets<<<(nbins + 256) / 256, 256, 0, c->st>>>(bout, bucket_base, nbins, bin_out);
+  scan_u64_dev(cd, cout_, max_buckets, bucket_base + nbins, stmp, c->st);
+  WS(counts, uint32_t, "counts", keys_cap);
+  k_compact<K><<<c->n_sms * 8, 256, 0, c->st>>>(tkeys, tcounts, cstart, cd, cout_, bucket_base, nbins,
+                                                 keys, counts);
   LAUNCHED(c);
+  WS(bin_out, uint64_t, "bin_out", nbins + 1);
+  k_bin_out_offsets<<<(nbins + 256) / 256, 256, 0, c->st>>>(cout_, bucket_base, nbins, bin_out);
+  LAUNCHED(c);
+  c->launches += 4;
   c->count_keys_cap = keys_cap;
   return GKC_OK;
 }
@@ -612,6 +642,7 @@ gkc_status count_device_impl(gkc_ctx *c, const gkc_params *prm, gkc_mode mode) {
   if (c->h_tot->err & ERR_OVERSIZE_SCRATCH)
     return ctx_fail(c, GKC_ERR_CAPACITY, "oversized bucket beyond sort scratch");
   if (c->h_tot->err & ERR_CAPACITY) return ctx_fail(c, GKC_ERR_CAPACITY, "key capacity");
+  if (c->h_tot->err & ERR_BOUNDS) return check_device_err(c);
   s = check_device_err(c);
   if (s != GKC_OK) return s;
   fill_count_view(c, prm);

@@ -15,6 +15,7 @@ enum : uint32_t {
   ERR_CAPACITY = 1u << 1,       // an output buffer sized in advance was too small
   ERR_OVERSIZE_SCRATCH = 1u << 2,
   ERR_BAD_READ = 1u << 3,       // a read longer than the supported superkmer length
+  ERR_BOUNDS = 1u << 4,         // a device bounds check failed (access skipped)
 };
 
 // Bounded spin limit for any wait on another CTA (~0.5-2 s with backoff).

@@ -5,22 +5,25 @@
 // ascending, run-length counted (count clamped to 2^32-1), per bin.
 //
 // Device layout:
-//   1. k_bucket_hist   - expands each bin's superkmers (rolling forward and
-//                        reverse-complement keys) and histograms the top
-//                        `bin_bits[b]` bits of the canonical key per bin;
-//   2. scan            - bucket sizes -> bucket offsets;
-//   3. k_bucket_scatter- re-expands and writes every key into its (bin,
-//                        prefix) bucket, runs staged through shared memory;
-//   4. k_sort_count    - persistent: one bucket per CTA iteration, taken in
-//                        key order; the bucket is sorted in shared memory
-//                        (one MSD counting pass on the next digit, leaves by
-//                        insertion sort, large leaves by a bitonic network),
-//                        run-length counted, and written at its output offset
-//                        found by a decoupled look-back over the buckets
-//                        before it.  Buckets larger than shared memory are
-//                        split by MSD passes through global scratch.
+//   1. k_coarse_hist    - each chunk of a bin's k-mer stream (load-balanced:
+//                         every thread expands the same number of k-mers)
+//                         histograms the top `bin_bits[b]` bits of the
+//                         canonical keys; counts go to a (bin, digit, chunk)
+//                         matrix whose exclusive scan gives every chunk its
+//                         write offset per digit -- no global atomics;
+//   2. k_coarse_scatter - re-expands and writes each key into its coarse
+//                         bucket (bin, top bits);
+//   3. k_coarse_count   - persistent, one coarse bucket per iteration: a
+//                         sub-histogram of the next bits plans slices; each
+//                         slice is aggregated in an order-preserving shared
+//                         memory hash table (duplicates meet in one slot, a
+//                         left-to-right scan is ascending once collision
+//                         clusters are sorted) and written as sorted
+//                         (k-mer, count) runs to a staging area;
+//   4. k_compact        - moves each coarse bucket's runs to its final offset.
 #include "common.cuh"
 #include "kernels.h"
+#include "sortsmem.cuh"
 
 namespace gkc {
 
@@ -29,375 +32,307 @@ namespace gkc {
 __global__ void k_count_plan(CountPlan pl) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const bool dead = (*pl.err & (ERR_CAPACITY | ERR_BAD_READ)) != 0;
-  uint64_t bb = 0, cb = 0;
+  uint64_t bb = 0, cb = 0, hb = 0;
   for (uint32_t b = 0; b < pl.nbins; b++) {
-    uint64_t nk = dead ? 0 : pl.bin_kstart[b + 1] - pl.bin_kstart[b];
-    uint64_t ns = dead ? 0 : pl.bin_start[b + 1] - pl.bin_start[b];
+    const uint64_t nk = dead ? 0 : pl.bin_kstart[b + 1] - pl.bin_kstart[b];
     uint32_t bits = 0;
-    while (bits < pl.max_bits && (int)bits < 2 * pl.k && (nk >> bits) > pl.target_bucket) bits++;
+    while (bits < pl.max_bits && (int)bits < 2 * pl.k && (nk >> bits) > pl.coarse_target) bits++;
+    const uint64_t nch = (nk + pl.chunk_kmers - 1) / pl.chunk_kmers;
     pl.bin_bits[b] = bits;
     pl.bucket_base[b] = bb;
-    bb += 1ull << bits;
     pl.chunk_base[b] = cb;
-    cb += (ns + pl.chunk_skm - 1) / pl.chunk_skm;
+    pl.hist_base[b] = hb;
+    bb += 1ull << bits;
+    cb += nch;
+    hb += nch << bits;
   }
   pl.bucket_base[pl.nbins] = bb;
   pl.chunk_base[pl.nbins] = cb;
+  pl.hist_base[pl.nbins] = hb;
 }
 
 // ----------------------------------------------------------------- expansion
 
-// Calls f(canonical key) for every k-mer of one packed superkmer.  The
-// forward key rolls in from the right; the reverse complement rolls in from
-// the top, so min(x, rc) is the reference's canonicalkmer (kmer_counting.cu:33-44).
+// The 2k bits of bases [o, o+k) of a packed superkmer starting at byte `off`
+// (2 bits per base, first base in the top bits of its byte).
+template <typename K>
+GKC_DEV K extract_kmer(const uint8_t *packed, uint64_t off, uint32_t o, int k);
+
+template <>
+GKC_DEV uint64_t extract_kmer<uint64_t>(const uint8_t *packed, uint64_t off, uint32_t o, int k) {
+  const uint8_t *p = packed + off + (o >> 2);
+  const int sh = 2 * (o & 3);
+  uint64_t hi = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) hi = (hi << 8) | __ldg(p + i);
+  const uint32_t nx = __ldg(p + 8);
+  const uint64_t v = sh ? ((hi << sh) | (nx >> (8 - sh))) : hi;
+  return v >> (64 - 2 * k);
+}
+
+template <>
+GKC_DEV u128 extract_kmer<u128>(const uint8_t *packed, uint64_t off, uint32_t o, int k) {
+  const uint8_t *p = packed + off + (o >> 2);
+  const int sh = 2 * (o & 3);
+  u128 hi = 0;
+#pragma unroll
+  for (int i = 0; i < 16; i++) hi = (hi << 8) | (u128)__ldg(p + i);
+  const uint32_t nx = __ldg(p + 16);
+  const u128 v = sh ? ((hi << sh) | (u128)(nx >> (8 - sh))) : hi;
+  return v >> (128 - 2 * k);
+}
+
+// Calls f(canonical key) for the k-mers with global indices [q0, q1) of the
+// bin-ordered superkmer stream (superkmers [s_lo, s_hi) hold them; koff is
+// the exclusive prefix of their k-mer counts).  The first k-mer of each
+// superkmer segment is extracted whole and reverse-complemented; the rest roll
+// in one base at a time (kmer_counting.cu:99-112, canonical form :33-44).
 template <typename K, typename F>
-GKC_DEV void expand_skm(const uint8_t *packed, uint64_t desc, int k, F &&f) {
-  const uint64_t off = desc >> 24;
-  const uint32_t len = (uint32_t)(desc & 0xFFFFFFu);
-  if (len < (uint32_t)k) return;
+GKC_DEV void expand_range(const uint64_t *desc, const uint64_t *koff, const uint8_t *packed,
+                          uint64_t s_lo, uint64_t s_hi, uint64_t q0, uint64_t q1, int k, F &&f) {
+  if (q0 >= q1) return;
+  uint64_t lo = s_lo, hi = s_hi - 1;
+  while (lo < hi) {
+    uint64_t mid = (lo + hi + 1) >> 1;
+    if (koff[mid] <= q0) lo = mid; else hi = mid - 1;
+  }
+  uint64_t s = lo;
   const K mask = kmer_mask<K>(k);
   const int top = 2 * k - 2;
-  K x = 0, r = 0;
-  const uint8_t *src = packed + off;
-  uint32_t byte = 0;
-  for (uint32_t i = 0; i < len; i++) {
-    if ((i & 3u) == 0) byte = __ldg(src + (i >> 2));
-    uint32_t c = (byte >> (6 - 2 * (i & 3u))) & 3u;
-    x = ((x << 2) | (K)c) & mask;
-    r = (r >> 2) | ((K)(3u - c) << top);
-    if (i + 1 >= (uint32_t)k) f(x < r ? x : r);
+  while (q0 < q1 && s < s_hi) {
+    const uint64_t kb = koff[s], ke = koff[s + 1];
+    if (q0 >= ke) {
+      s++;
+      continue;
+    }
+    const uint64_t off = desc[s] >> 24;
+    const uint32_t o = (uint32_t)(q0 - kb);
+    const uint32_t cnt = (uint32_t)(min(q1, ke) - q0);
+    K x = extract_kmer<K>(packed, off, o, k);
+    K r = revcomp_k<K>(x, k);
+    f(x < r ? x : r);
+    const uint8_t *src = packed + off;
+    uint32_t j = o + (uint32_t)k;
+    uint32_t byte = cnt > 1 ? __ldg(src + (j >> 2)) : 0u;
+    for (uint32_t t = 1; t < cnt; t++, j++) {
+      if ((j & 3u) == 0) byte = __ldg(src + (j >> 2));
+      const uint32_t c = (byte >> (6 - 2 * (j & 3u))) & 3u;
+      x = ((x << 2) | (K)c) & mask;
+      r = (r >> 2) | ((K)(3u - c) << top);
+      f(x < r ? x : r);
+    }
+    q0 += cnt;
+    s++;
   }
 }
 
-// bin owning chunk c: the b with chunk_base[b] <= c < chunk_base[b+1]
-GKC_DEV uint32_t chunk_bin(const uint64_t *chunk_base, uint32_t nbins, uint64_t c) {
+GKC_DEV uint32_t find_bin(const uint64_t *base, uint32_t nbins, uint64_t c) {
   uint32_t lo = 0, hi = nbins - 1;
   while (lo < hi) {
     uint32_t mid = (lo + hi + 1) >> 1;
-    if (chunk_base[mid] <= c) lo = mid; else hi = mid - 1;
+    if (base[mid] <= c) lo = mid; else hi = mid - 1;
   }
   return lo;
 }
 
 constexpr int EX_NT = 256;
 
+struct ChunkInfo {
+  uint32_t b, nbits;
+  uint64_t j, nch, q0, q1, s_lo, s_hi;
+};
+
+GKC_DEV ChunkInfo chunk_info(const ExpandArgs &a, uint64_t c) {
+  ChunkInfo ci;
+  ci.b = find_bin(a.chunk_base, a.nbins, c);
+  ci.j = c - a.chunk_base[ci.b];
+  ci.nch = a.chunk_base[ci.b + 1] - a.chunk_base[ci.b];
+  ci.nbits = a.bin_bits[ci.b];
+  const uint64_t k0 = a.bin_kstart[ci.b] + ci.j * a.chunk_kmers;
+  const uint64_t k1 = min(k0 + a.chunk_kmers, a.bin_kstart[ci.b + 1]);
+  const uint64_t per = (k1 - k0 + EX_NT - 1) / EX_NT;
+  ci.q0 = min(k0 + per * threadIdx.x, k1);
+  ci.q1 = min(ci.q0 + per, k1);
+  ci.s_lo = a.bin_start[ci.b];
+  ci.s_hi = a.bin_start[ci.b + 1];
+  return ci;
+}
+
 template <typename K>
-__global__ void __launch_bounds__(EX_NT) k_bucket_hist(ExpandArgs a) {
+__global__ void __launch_bounds__(EX_NT) k_coarse_hist(ExpandArgs a) {
   extern __shared__ uint32_t hist[];  // 1 << max bits
+  if (*a.err & (ERR_CAPACITY | ERR_BAD_READ)) return;
   const uint64_t n_chunks = a.chunk_base[a.nbins];
   const int key_bits = 2 * a.k;
   for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
-    const uint32_t b = chunk_bin(a.chunk_base, a.nbins, c);
-    const uint32_t nbits = a.bin_bits[b], nd = 1u << nbits;
+    const ChunkInfo ci = chunk_info(a, c);
+    const uint32_t nd = 1u << ci.nbits;
     for (uint32_t d = threadIdx.x; d < nd; d += EX_NT) hist[d] = 0;
     __syncthreads();
-    const uint64_t s0 = a.bin_start[b] + (c - a.chunk_base[b]) * a.chunk_skm;
-    const uint64_t s1 = min(s0 + a.chunk_skm, a.bin_start[b + 1]);
-    for (uint64_t i = s0 + threadIdx.x; i < s1; i += EX_NT) {
-      expand_skm<K>(a.packed, a.desc[i], a.k, [&](K key) {
-        atomicAdd(&hist[key_digit<K>(key, key_bits, 0, (int)nbits)], 1u);
-      });
-    }
+    expand_range<K>(a.desc, a.koff, a.packed, ci.s_lo, ci.s_hi, ci.q0, ci.q1, a.k, [&](K key) {
+      atomicAdd(&hist[key_digit<K>(key, key_bits, 0, (int)ci.nbits)], 1u);
+    });
     __syncthreads();
-    const uint64_t bb = a.bucket_base[b];
-    for (uint32_t d = threadIdx.x; d < nd; d += EX_NT)
-      if (hist[d]) atomicAdd(&a.bucket_count[bb + d], (unsigned long long)hist[d]);
+    unsigned long long *row = a.chunk_hist + a.hist_base[ci.b] + ci.j;
+    for (uint32_t d = threadIdx.x; d < nd; d += EX_NT) row[(uint64_t)d * ci.nch] = hist[d];
     __syncthreads();
   }
 }
 
 template <typename K>
-__global__ void __launch_bounds__(EX_NT) k_bucket_scatter(ExpandArgs a) {
-  extern __shared__ unsigned long long sh_base[];      // 1 << max bits
-  uint32_t *hist = reinterpret_cast<uint32_t *>(sh_base + 4096);
+__global__ void __launch_bounds__(EX_NT) k_coarse_scatter(ExpandArgs a) {
+  extern __shared__ unsigned long long sh_base[];  // 1 << max bits
+  uint32_t *rank = reinterpret_cast<uint32_t *>(sh_base + (1u << a.max_bits));
+  if (*a.err & (ERR_CAPACITY | ERR_BAD_READ)) return;
   K *keys = reinterpret_cast<K *>(a.keys);
   const uint64_t n_chunks = a.chunk_base[a.nbins];
   const int key_bits = 2 * a.k;
   for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
-    const uint32_t b = chunk_bin(a.chunk_base, a.nbins, c);
-    const uint32_t nbits = a.bin_bits[b], nd = 1u << nbits;
-    for (uint32_t d = threadIdx.x; d < nd; d += EX_NT) hist[d] = 0;
-    __syncthreads();
-    const uint64_t s0 = a.bin_start[b] + (c - a.chunk_base[b]) * a.chunk_skm;
-    const uint64_t s1 = min(s0 + a.chunk_skm, a.bin_start[b + 1]);
-    for (uint64_t i = s0 + threadIdx.x; i < s1; i += EX_NT) {
-      expand_skm<K>(a.packed, a.desc[i], a.k, [&](K key) {
-        atomicAdd(&hist[key_digit<K>(key, key_bits, 0, (int)nbits)], 1u);
-      });
-    }
-    __syncthreads();
-    const uint64_t bb = a.bucket_base[b];
+    const ChunkInfo ci = chunk_info(a, c);
+    const uint32_t nd = 1u << ci.nbits;
+    const uint64_t *row = a.chunk_off + a.hist_base[ci.b] + ci.j;
     for (uint32_t d = threadIdx.x; d < nd; d += EX_NT) {
-      uint32_t h = hist[d];
-      sh_base[d] = h ? atomicAdd(&a.bucket_cursor[bb + d], (unsigned long long)h) : 0ull;
-      hist[d] = 0;
+      sh_base[d] = row[(uint64_t)d * ci.nch];
+      rank[d] = 0;
     }
     __syncthreads();
-    for (uint64_t i = s0 + threadIdx.x; i < s1; i += EX_NT) {
-      expand_skm<K>(a.packed, a.desc[i], a.k, [&](K key) {
-        uint32_t d = key_digit<K>(key, key_bits, 0, (int)nbits);
-        uint64_t slot = sh_base[d] + atomicAdd(&hist[d], 1u);
-        if (slot < a.keys_cap) keys[slot] = key;
-        else atomicOr(a.err, ERR_CAPACITY);
-      });
-    }
+    expand_range<K>(a.desc, a.koff, a.packed, ci.s_lo, ci.s_hi, ci.q0, ci.q1, a.k, [&](K key) {
+      const uint32_t d = key_digit<K>(key, key_bits, 0, (int)ci.nbits);
+      const uint64_t slot = sh_base[d] + atomicAdd(&rank[d], 1u);
+      if (slot < a.keys_cap) keys[slot] = key;
+      else atomicOr(a.err, ERR_CAPACITY);
+    });
     __syncthreads();
   }
 }
 
-// ---------------------------------------------------------------- look-back
-
-constexpr unsigned long long LB_AGG = 1ull << 62, LB_PRE = 2ull << 62;
-constexpr unsigned long long LB_VAL = (1ull << 62) - 1;
-
-GKC_DEV void st_release(unsigned long long *p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+// Number of k-mers of each bin-ordered superkmer (for the k-mer prefix).
+__global__ void k_skm_nk(const uint64_t *desc, const unsigned long long *n_skm_dev, int k,
+                         unsigned long long *nk) {
+  const uint64_t n = *n_skm_dev;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t len = (uint32_t)(desc[i] & 0xFFFFFFu);
+    nk[i] = len >= (uint32_t)k ? len - k + 1 : 0;
+  }
 }
-GKC_DEV unsigned long long ld_acquire(const unsigned long long *p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
+
+// ------------------------------------------- coarse bucket: hash-aggregate sort
+
+// Order-preserving shared-memory hash table: a key's home slot is a monotone
+// function of the key (piecewise linear over the slice's sub-buckets, each
+// given slots in proportion to its keys), so duplicates meet in one slot and a
+// left-to-right scan is ascending once each run of occupied slots (a
+// collision cluster) is sorted: every key of a cluster has its home inside
+// it, so clusters are mutually ordered.
+template <typename K> struct SliceTab;
+template <> struct SliceTab<uint64_t> { static constexpr int TS = 16384, OVF = 512; };
+template <> struct SliceTab<u128> { static constexpr int TS = 8192, OVF = 512; };
+constexpr int CC_SUB_BITS = 11;        // sub-histogram inside a coarse bucket
+constexpr int CC_NSUB = 1 << CC_SUB_BITS;
+constexpr int SL_PROBE_LIMIT = 256;
+constexpr int SL_CLUSTER_LIMIT = 512;
+constexpr int SL_LOW_BITS = 20;
+
+template <typename K>
+struct CoarseSmem {
+  static constexpr int TSO = SliceTab<K>::TS + SliceTab<K>::OVF;
+  union {
+    struct {
+      K key[TSO];
+      uint32_t cnt[TSO];
+    } t;
+    SortSmem<K> s;  // fallback sort layout
+  } u;
+  uint32_t sub[CC_NSUB + 1];        // sub-bucket counts, then exclusive starts
+  uint32_t slot_base[CC_NSUB + 1];
+  uint16_t slo[CC_NSUB + 1];        // first sub-bucket of each slice
+  uint32_t tmp[64];
+  uint64_t g, start, n, run;
+  uint32_t b, nsl, cursor;
+  int overflow;
+};
+
+template <typename K> size_t coarse_smem_bytes() { return sizeof(CoarseSmem<K>); }
+template size_t coarse_smem_bytes<uint64_t>();
+template size_t coarse_smem_bytes<u128>();
+
+template <typename K> GKC_DEV K empty_key() { return ~(K)0; }
+
+GKC_DEV uint64_t smem_cas(uint64_t *p, uint64_t cmp, uint64_t val) {
+  return atomicCAS((unsigned long long *)p, (unsigned long long)cmp, (unsigned long long)val);
 }
+GKC_DEV u128 smem_cas(u128 *p, u128 cmp, u128 val) {
+  // 16-byte compare-and-swap on shared memory (sm_90+)
+  uint64_t clo = (uint64_t)cmp, chi = (uint64_t)(cmp >> 64);
+  uint64_t vlo = (uint64_t)val, vhi = (uint64_t)(val >> 64);
+  uint64_t rlo, rhi;
+  unsigned addr = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile(
+      "{\n\t.reg .b128 c, v, r;\n\t"
+      "mov.b128 c, {%2, %3};\n\t"
+      "mov.b128 v, {%4, %5};\n\t"
+      "atom.shared.cas.b128 r, [%6], c, v;\n\t"
+      "mov.b128 {%0, %1}, r;\n\t}"
+      : "=l"(rlo), "=l"(rhi)
+      : "l"(clo), "l"(chi), "l"(vlo), "l"(vhi), "r"(addr)
+      : "memory");
+  return ((u128)rhi << 64) | rlo;
+}
+
+template <typename K>
+GKC_DEV K volatile_load(const K *p) {
+  return *(const volatile K *)p;
+}
+
+GKC_DEV void set_overflow(int *f) { *(volatile int *)f = 1; }
+
 GKC_DEV uint64_t globaltimer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
 
-// Sum of the outputs of buckets [0, i) (waits, bounded, for predecessors).
-GKC_DEV uint64_t lookback_prefix(unsigned long long *status, uint64_t i, uint32_t *err) {
-  uint64_t excl = 0;
-  if (i == 0) return 0;
-  uint64_t j = i - 1;
-  uint64_t t0 = globaltimer_ns();
+// Bounded spin lock (thread 0 of a CTA): false if the wait ran out.
+GKC_DEV bool acquire_lock(unsigned long long *lock, uint32_t *err) {
+  const uint64_t t0 = globaltimer_ns();
   uint32_t it = 0;
-  while (true) {
-    unsigned long long v = ld_acquire(status + j);
-    unsigned long long flag = v & ~LB_VAL;
-    if (flag == 0) {
-      if (++it > (1u << 24) || globaltimer_ns() - t0 > 8000000000ull) {
-        atomicOr(err, ERR_SPIN_TIMEOUT);
-        return excl;
-      }
-      nanosleep_backoff(it);
-      continue;
+  while (atomicCAS(lock, 0ull, 1ull) != 0ull) {
+    if (++it > (1u << 24) || globaltimer_ns() - t0 > 10000000000ull) {
+      atomicOr(err, ERR_SPIN_TIMEOUT);
+      return false;
     }
-    excl += v & LB_VAL;
-    if (flag == LB_PRE || j == 0) return excl;
-    j--;
+    nanosleep_backoff(it);
   }
+  __threadfence();
+  return true;
 }
 
-// -------------------------------------------------------- shared-memory sort
-
-constexpr int SC_NT = kSortThreads;
-constexpr int SC_DMAX = 12;           // bits per MSD counting pass
-constexpr int SC_SMAX = 32;           // leaves up to this size: insertion sort
-constexpr int SC_BIGMAX = 256;        // larger leaves recorded per pass
-
-template <typename K> struct SortCap;
-template <> struct SortCap<uint64_t> { static constexpr int value = 5632; };
-template <> struct SortCap<u128> { static constexpr int value = 2816; };
-
-template <typename K>
-struct SortSmem {
-  K A[SortCap<K>::value];
-  K B[SortCap<K>::value];
-  uint32_t cnt[1 << SC_DMAX];
-  uint32_t tmp[64];
-  uint32_t big_s[SC_BIGMAX], big_m[SC_BIGMAX];
-  uint32_t n_big;
-  uint32_t D;
-  uint64_t bucket, excl, n, start;
-  // oversized-bucket frames
-  struct Frame {
-    uint64_t off, len;
-    int skip, src, split, d;
-    uint32_t cursor;
-  } fr[24];
-  int depth;
-  int act;              // action decided by thread 0 for the oversize walk
-  uint64_t c_off, c_len;
-  int c_skip, c_src;
-  uint64_t out;
-};
-
-template <typename K> int sort_count_cap() { return SortCap<K>::value; }
-template <typename K> size_t sort_count_smem_bytes() { return sizeof(SortSmem<K>); }
-template int sort_count_cap<uint64_t>();
-template int sort_count_cap<u128>();
-template size_t sort_count_smem_bytes<uint64_t>();
-template size_t sort_count_smem_bytes<u128>();
-
-GKC_DEV int ceil_log2_u32(uint32_t n) { return n <= 1 ? 0 : 32 - __clz(n - 1); }
-
-// Exclusive scan of cnt[0, nd) in place; returns the total.
-GKC_DEV uint32_t scan_counters(uint32_t *cnt, uint32_t nd, uint32_t *tmp) {
-  const uint32_t per = (nd + SC_NT - 1) / SC_NT;
-  const uint32_t c0 = threadIdx.x * per;
-  uint32_t s = 0;
-  for (uint32_t j = c0; j < c0 + per && j < nd; j++) s += cnt[j];
-  uint32_t total;
-  uint32_t run = block_exclusive_scan<SC_NT>(s, tmp, &total);
-  for (uint32_t j = c0; j < c0 + per && j < nd; j++) {
-    uint32_t v = cnt[j];
-    cnt[j] = run;
-    run += v;
+// Records the first failed bounds check (code, index, limit); the caller
+// skips the access.
+GKC_DEV bool in_bounds(const SortCountArgs &a, int code, uint64_t idx, uint64_t lim) {
+  if (idx < lim) return true;
+  if (atomicCAS(a.dbg, 0ull, (unsigned long long)code) == 0ull) {
+    a.dbg[1] = idx;
+    a.dbg[2] = lim;
   }
-  __syncthreads();
-  return total;
+  atomicOr(a.err, ERR_BOUNDS);
+  return false;
 }
+GKC_DEV int get_overflow(const int *f) { return *(const volatile int *)f; }
 
-// In-place ascending sort of A[0, m) with a comparator network in which every
-// comparator puts the smaller key at the lower index, so indices >= m can be
-// treated as +infinity (the "flip" form of bitonic sort).
+// Oversized slice fallback: MSD passes through global scratch, depth first in
+// key order; sub-ranges that fit are finished in shared memory.  Input: n keys
+// in scratch half 0.  Output runs are appended at S.out.
 template <typename K>
-GKC_DEV void bitonic_sort(K *A, uint32_t m) {
-  uint32_t P = 1;
-  while (P < m) P <<= 1;
-  for (uint32_t size = 2; size <= P; size <<= 1) {
-    const uint32_t half = size >> 1;
-    for (uint32_t i = threadIdx.x; i < P / 2; i += SC_NT) {
-      uint32_t blk = i / half, off = i % half;
-      uint32_t lo = blk * size + off, hi = blk * size + size - 1 - off;
-      if (hi < m) {
-        K x = A[lo], y = A[hi];
-        if (y < x) { A[lo] = y; A[hi] = x; }
-      }
-    }
-    __syncthreads();
-    for (uint32_t stride = size >> 2; stride >= 1; stride >>= 1) {
-      for (uint32_t i = threadIdx.x; i < P / 2; i += SC_NT) {
-        uint32_t blk = i / stride, off = i % stride;
-        uint32_t lo = blk * 2 * stride + off, hi = lo + stride;
-        if (hi < m) {
-          K x = A[lo], y = A[hi];
-          if (y < x) { A[lo] = y; A[hi] = x; }
-        }
-      }
-      __syncthreads();
-    }
-  }
-}
-
-// Sorts S.A[0, n) ascending; keys agree on their top `skip` bits.
-template <typename K>
-GKC_DEV void smem_sort(SortSmem<K> &S, uint32_t n, int key_bits, int skip) {
-  const int R = key_bits - skip;
-  if (n <= 1 || R <= 0) return;
-  const int d = max(1, min(min(SC_DMAX, R), ceil_log2_u32(n)));
-  const uint32_t nd = 1u << d;
-  for (uint32_t j = threadIdx.x; j < nd; j += SC_NT) S.cnt[j] = 0;
-  if (threadIdx.x == 0) S.n_big = 0;
-  __syncthreads();
-  for (uint32_t i = threadIdx.x; i < n; i += SC_NT)
-    atomicAdd(&S.cnt[key_digit<K>(S.A[i], key_bits, skip, d)], 1u);
-  __syncthreads();
-  scan_counters(S.cnt, nd, S.tmp);
-  for (uint32_t i = threadIdx.x; i < n; i += SC_NT) {
-    K x = S.A[i];
-    uint32_t pos = atomicAdd(&S.cnt[key_digit<K>(x, key_bits, skip, d)], 1u);
-    S.B[pos] = x;
-  }
-  __syncthreads();
-  // cnt[j] is now the end of leaf j
-  for (uint32_t j = threadIdx.x; j < nd; j += SC_NT) {
-    uint32_t s = j ? S.cnt[j - 1] : 0u, e = S.cnt[j], m = e - s;
-    if (m <= (uint32_t)SC_SMAX) {
-      for (uint32_t t = 0; t < m; t++) {
-        K x = S.B[s + t];
-        uint32_t q = t;
-        while (q > 0 && x < S.A[s + q - 1]) {
-          S.A[s + q] = S.A[s + q - 1];
-          q--;
-        }
-        S.A[s + q] = x;
-      }
-    } else {
-      uint32_t slot = atomicAdd(&S.n_big, 1u);
-      if (slot < (uint32_t)SC_BIGMAX) {
-        S.big_s[slot] = s;
-        S.big_m[slot] = m;
-      }
-    }
-  }
-  __syncthreads();
-  const uint32_t nbig = min(S.n_big, (uint32_t)SC_BIGMAX);
-  for (uint32_t t = 0; t < nbig; t++) {
-    const uint32_t s = S.big_s[t], m = S.big_m[t];
-    for (uint32_t i = threadIdx.x; i < m; i += SC_NT) S.A[s + i] = S.B[s + i];
-    __syncthreads();
-    bitonic_sort<K>(S.A + s, m);
-  }
-  // big leaves beyond the list (at most n / SC_SMAX exist, so only when
-  // n > SC_BIGMAX * SC_SMAX) are sorted by one more bitonic pass overall.
-  if (S.n_big > (uint32_t)SC_BIGMAX) {
-    __syncthreads();
-    for (uint32_t j = threadIdx.x; j < nd; j += SC_NT) {
-      uint32_t s = j ? S.cnt[j - 1] : 0u, e = S.cnt[j];
-      if (e - s > (uint32_t)SC_SMAX)
-        for (uint32_t i = s; i < e; i++) S.A[i] = S.B[i];
-    }
-    __syncthreads();
-    bitonic_sort<K>(S.A, n);
-  }
-  __syncthreads();
-}
-
-// Run-length pass over sorted S.A[0, n): run starts go to S.B viewed as
-// uint32 (run j spans [rs[j], rs[j+1])).  Returns the number of runs.
-template <typename K>
-GKC_DEV uint32_t smem_runs(SortSmem<K> &S, uint32_t n) {
-  uint32_t *rs = reinterpret_cast<uint32_t *>(S.B);
-  const uint32_t per = (n + SC_NT - 1) / SC_NT;
-  const uint32_t c0 = threadIdx.x * per;
-  uint32_t cntr = 0;
-  for (uint32_t i = c0; i < c0 + per && i < n; i++) cntr += (i == 0 || S.A[i] != S.A[i - 1]);
-  uint32_t total;
-  uint32_t idx = block_exclusive_scan<SC_NT>(cntr, S.tmp, &total);
-  for (uint32_t i = c0; i < c0 + per && i < n; i++)
-    if (i == 0 || S.A[i] != S.A[i - 1]) rs[idx++] = i;
-  if (threadIdx.x == 0) rs[total] = n;
-  __syncthreads();
-  return total;
-}
-
-template <typename K>
-GKC_DEV void write_runs(SortSmem<K> &S, uint32_t D, K *out_keys, uint32_t *out_counts,
-                        uint64_t out) {
-  const uint32_t *rs = reinterpret_cast<const uint32_t *>(S.B);
-  for (uint32_t j = threadIdx.x; j < D; j += SC_NT) {
-    out_keys[out + j] = S.A[rs[j]];
-    out_counts[out + j] = rs[j + 1] - rs[j];
-  }
-}
-
-template <typename K>
-GKC_DEV void load_keys(K *dst, const K *src, uint32_t n) {
-  for (uint32_t i = threadIdx.x; i < n; i += SC_NT) dst[i] = src[i];
-}
-
-// Oversized bucket: MSD passes through global scratch, depth first in key
-// order; sub-buckets that fit are finished in shared memory.
-template <typename K>
-GKC_DEV void oversize_bucket(SortSmem<K> &S, const SortCountArgs &a, K *keys, K *out_keys,
-                             uint64_t start, uint64_t n, int skip0, uint64_t excl) {
+GKC_DEV void scratch_sort(SortSmem<K> &S, const SortCountArgs &a, uint64_t n, int skip0,
+                          K *out_keys, uint32_t *out_counts) {
   const int key_bits = 2 * a.k;
   const int CAP = SortCap<K>::value;
   K *half[2] = {reinterpret_cast<K *>(a.scratch), reinterpret_cast<K *>(a.scratch) + a.scratch_keys};
-  if (n > a.scratch_keys) {
-    if (threadIdx.x == 0) {
-      atomicOr(a.err, ERR_OVERSIZE_SCRATCH);
-      S.out = excl;
-    }
-    __syncthreads();
-    return;
-  }
-  for (uint64_t i = threadIdx.x; i < n; i += SC_NT) half[0][i] = keys[start + i];
   if (threadIdx.x == 0) {
     S.depth = 0;
     S.fr[0] = {0, n, skip0, 0, 0, 0, 0};
-    S.out = excl;
   }
   __threadfence_block();
   __syncthreads();
@@ -418,9 +353,10 @@ GKC_DEV void oversize_bucket(SortSmem<K> &S, const SortCountArgs &a, K *keys, K 
       for (uint64_t i = threadIdx.x; i < len; i += SC_NT) {
         K x = half[src][off + i];
         uint32_t pos = atomicAdd(&S.cnt[key_digit<K>(x, key_bits, skip, d)], 1u);
-        half[1 - src][off + pos] = x;
+        if (in_bounds(a, 2, off + pos, a.scratch_keys)) half[1 - src][off + pos] = x;
       }
       __syncthreads();
+      if (!in_bounds(a, 3, dep, 24)) return;
       for (uint32_t j = threadIdx.x; j < nd; j += SC_NT) gc[j] = S.cnt[j];  // leaf ends
       __threadfence_block();
       __syncthreads();
@@ -431,22 +367,38 @@ GKC_DEV void oversize_bucket(SortSmem<K> &S, const SortCountArgs &a, K *keys, K 
       }
       __syncthreads();
     }
-    // thread 0 walks to the next non-empty child and decides what to do
     if (threadIdx.x == 0) {
-      S.act = 0;  // 0: frame done
+      // next action: a run of consecutive children that fits in shared memory
+      // is sorted together (it is contiguous and in key order); a single child
+      // too large to fit is split further, or emitted whole if all its bits
+      // are consumed (all keys equal)
+      S.act = 0;
       auto &F = S.fr[dep];
       const uint32_t nd = 1u << F.d;
       while (F.cursor < nd) {
-        uint32_t j = F.cursor++;
-        uint64_t s = j ? gc[j - 1] : 0, e = gc[j];
-        if (e == s) continue;
-        S.c_off = F.off + s;
-        S.c_len = e - s;
-        S.c_skip = F.skip + F.d;
+        uint32_t j = F.cursor;
+        uint64_t s0 = j ? gc[j - 1] : 0, e = gc[j];
+        if (e == s0) {
+          F.cursor++;
+          continue;
+        }
+        if (e - s0 > (uint64_t)CAP) {
+          F.cursor++;
+          S.c_off = F.off + s0;
+          S.c_len = e - s0;
+          S.c_skip = F.skip + F.d;
+          S.c_src = 1 - F.src;
+          S.act = (S.c_skip >= key_bits) ? 2 : 3;
+          break;
+        }
+        uint32_t jn = j + 1;
+        while (jn < nd && gc[jn] - s0 <= (uint64_t)CAP) jn++;
+        F.cursor = jn;
+        S.c_off = F.off + s0;
+        S.c_len = gc[jn - 1] - s0;
+        S.c_skip = F.skip;  // the run shares only the parent's prefix
         S.c_src = 1 - F.src;
-        if (S.c_len <= (uint64_t)CAP) S.act = 1;            // finish in shared memory
-        else if (S.c_skip >= key_bits) S.act = 2;           // all keys equal
-        else S.act = 3;                                     // split further
+        S.act = 1;
         break;
       }
       if (S.act == 3) {
@@ -460,17 +412,19 @@ GKC_DEV void oversize_bucket(SortSmem<K> &S, const SortCountArgs &a, K *keys, K 
     const int act = S.act;
     if (act == 1) {
       const uint32_t m = (uint32_t)S.c_len;
+      if (!in_bounds(a, 4, m, (uint64_t)CAP + 1) || !in_bounds(a, 5, S.c_off + m, a.scratch_keys + 1)) return;
       load_keys<K>(S.A, half[S.c_src] + S.c_off, m);
       __syncthreads();
       smem_sort<K>(S, m, key_bits, S.c_skip);
       uint32_t D = smem_runs<K>(S, m);
-      write_runs<K>(S, D, out_keys, a.out_counts, S.out);
+      if (!in_bounds(a, 6, S.out + D, a.tmp_cap + 1)) return;
+      write_runs<K>(S, D, out_keys, out_counts, S.out);
       __syncthreads();
       if (threadIdx.x == 0) S.out += D;
     } else if (act == 2) {
-      if (threadIdx.x == 0) {
+      if (threadIdx.x == 0 && in_bounds(a, 7, S.out, a.tmp_cap)) {
         out_keys[S.out] = half[S.c_src][S.c_off];
-        a.out_counts[S.out] = S.c_len > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)S.c_len;
+        out_counts[S.out] = S.c_len > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)S.c_len;
         S.out += 1;
       }
     }
@@ -479,92 +433,265 @@ GKC_DEV void oversize_bucket(SortSmem<K> &S, const SortCountArgs &a, K *keys, K 
 }
 
 template <typename K>
-__global__ void __launch_bounds__(SC_NT, 2) k_sort_count(SortCountArgs a) {
+__global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
-  SortSmem<K> &S = *reinterpret_cast<SortSmem<K> *>(smem_raw);
-  K *keys = reinterpret_cast<K *>(a.keys);
-  K *out_keys = reinterpret_cast<K *>(a.out_keys);
+  CoarseSmem<K> &S = *reinterpret_cast<CoarseSmem<K> *>(smem_raw);
+  constexpr int TS = SliceTab<K>::TS, TSO = CoarseSmem<K>::TSO;
+  const K *keys = reinterpret_cast<const K *>(a.keys);
+  K *tkeys = reinterpret_cast<K *>(a.tmp_keys);
   const int key_bits = 2 * a.k;
-  const int CAP = SortCap<K>::value;
+  const int tid = threadIdx.x;
   if (*a.err & (ERR_CAPACITY | ERR_BAD_READ)) return;  // keys incomplete: the host re-runs
-  const uint64_t n_buckets = *a.n_buckets_dev;
+  const uint64_t n_buckets = a.bucket_base[a.nbins];
+  const uint32_t target = SliceTab<K>::TS / 2;
   while (true) {
-    if (threadIdx.x == 0) S.bucket = atomicAdd(a.ticket, 1ull);
-    __syncthreads();
-    const uint64_t i = S.bucket;
-    if (i >= n_buckets) break;
-    const uint64_t start = a.bucket_start[i], n = a.bucket_start[i + 1] - start;
-    // bucket -> bin -> prefix bits shared by the bucket's keys
-    uint32_t lo = 0, hi = a.nbins - 1;
-    while (lo < hi) {
-      uint32_t mid = (lo + hi + 1) >> 1;
-      if (a.bucket_base[mid] <= i) lo = mid; else hi = mid - 1;
+    if (tid == 0) {
+      S.g = atomicAdd(a.ticket, 1ull);
+      if (S.g < n_buckets) {
+        const uint32_t b = find_bin(a.bucket_base, a.nbins, S.g);
+        const uint64_t d = S.g - a.bucket_base[b];
+        const uint64_t nch = a.chunk_base[b + 1] - a.chunk_base[b];
+        const uint64_t hb = a.hist_base[b];
+        S.b = b;
+        S.start = a.chunk_off[hb + d * nch];
+        S.n = a.chunk_off[hb + (d + 1) * nch] - S.start;
+      }
+      S.run = 0;
     }
-    const int skip = (int)a.bin_bits[lo];
-    long long t0 = clock64();
-    if (n <= (uint64_t)CAP) {
-      load_keys<K>(S.A, keys + start, (uint32_t)n);
-      __syncthreads();
-      long long t1 = clock64();
-      smem_sort<K>(S, (uint32_t)n, key_bits, skip);
-      long long t2 = clock64();
-      const uint32_t D = smem_runs<K>(S, (uint32_t)n);
-      long long t3 = clock64();
-      if (threadIdx.x == 0 && a.prof) {
-        atomicAdd(a.prof + 0, (unsigned long long)(t1 - t0));
-        atomicAdd(a.prof + 1, (unsigned long long)(t2 - t1));
-        atomicAdd(a.prof + 2, (unsigned long long)(t3 - t2));
-        atomicAdd(a.prof + 6, 1ull);
-        atomicAdd(a.prof + 7, (unsigned long long)S.n_big);
-        atomicAdd(a.prof + 8, (unsigned long long)n);
+    __syncthreads();
+    const uint64_t g = S.g;
+    if (g >= n_buckets) break;
+    const uint64_t start = S.start, n = S.n;
+    const int cb = (int)a.bin_bits[S.b];
+    const int SB = min(CC_SUB_BITS, key_bits - cb);
+    const uint32_t nsub = 1u << SB;
+    const int lbits = min(SL_LOW_BITS, key_bits - cb - SB);
+    if (n == 0) {
+      if (tid == 0) {
+        a.coarse_start[g] = start;
+        a.coarse_d[g] = 0;
       }
-      if (threadIdx.x == 0) {
-        if (i == 0) {
-          S.excl = 0;
-          st_release(a.status, LB_PRE | D);
-        } else {
-          st_release(a.status + i, LB_AGG | D);
-          S.excl = lookback_prefix(a.status, i, a.err);
-          st_release(a.status + i, LB_PRE | (S.excl + D));
+      __syncthreads();
+      continue;
+    }
+    // sub-histogram of the next SB bits
+    for (uint32_t j = tid; j <= nsub; j += SC_NT) S.sub[j] = 0;
+    __syncthreads();
+    for (uint64_t i = tid; i < n; i += SC_NT)
+      atomicAdd(&S.sub[key_digit<K>(keys[start + i], key_bits, cb, SB)], 1u);
+    __syncthreads();
+    scan_counters(S.sub, nsub, S.tmp);
+    if (tid == 0) S.sub[nsub] = (uint32_t)n;
+    __syncthreads();
+    // slices: runs of sub-buckets whose exclusive start falls in the same
+    // multiple of `target` (a slice holds < target keys plus one sub-bucket)
+    {
+      const uint32_t per = (nsub + SC_NT - 1) / SC_NT, j0 = tid * per;
+      uint32_t cnt = 0;
+      for (uint32_t j = j0; j < j0 + per && j < nsub; j++)
+        cnt += (j == 0 || S.sub[j] / target != S.sub[j - 1] / target);
+      uint32_t total;
+      uint32_t idx = block_exclusive_scan<SC_NT>(cnt, S.tmp, &total);
+      for (uint32_t j = j0; j < j0 + per && j < nsub; j++)
+        if (j == 0 || S.sub[j] / target != S.sub[j - 1] / target) S.slo[idx++] = (uint16_t)j;
+      if (tid == 0) S.nsl = total;
+      __syncthreads();
+    }
+    const uint32_t nsl = S.nsl;
+    for (uint32_t sl = 0; sl < nsl; sl++) {
+      const uint32_t j_lo = S.slo[sl];
+      const uint32_t j_hi = (sl + 1 < nsl) ? S.slo[sl + 1] : nsub;
+      const uint32_t base_cnt = S.sub[j_lo];
+      const uint32_t ns = S.sub[j_hi] - base_cnt;
+      if (ns == 0) continue;
+      for (uint32_t j = j_lo + tid; j < j_hi; j += SC_NT)
+        S.slot_base[j - j_lo] = (uint32_t)(((uint64_t)(S.sub[j] - base_cnt) * TS) / ns);
+      if (tid == 0) {
+        S.slot_base[j_hi - j_lo] = TS;
+        S.overflow = 0;
+      }
+      for (int s = tid; s < TSO; s += SC_NT) {
+        S.u.t.key[s] = empty_key<K>();
+        S.u.t.cnt[s] = 0;
+      }
+      __syncthreads();
+      for (uint64_t i = tid; i < n; i += SC_NT) {
+        const K x = keys[start + i];
+        const uint32_t sd = key_digit<K>(x, key_bits, cb, SB);
+        if (sd < j_lo || sd >= j_hi) continue;
+        const uint32_t j = sd - j_lo;
+        const uint32_t low = key_digit<K>(x, key_bits, cb + SB, lbits);
+        const uint32_t w = S.slot_base[j + 1] - S.slot_base[j];
+        int slot = (int)(S.slot_base[j] + (uint32_t)(((uint64_t)low * w) >> lbits));
+        int probes = 0;
+        while (true) {
+          if (slot >= TSO || probes > a.probe_limit) {
+            set_overflow(&S.overflow);
+            break;
+          }
+          // 8-byte keys are read atomically; 16-byte keys only through the CAS
+          K cur = sizeof(K) == 8 ? volatile_load<K>(&S.u.t.key[slot]) : empty_key<K>();
+          if (cur == x) {
+            atomicAdd(&S.u.t.cnt[slot], 1u);
+            break;
+          }
+          if (cur == empty_key<K>()) {
+            K prev = smem_cas(&S.u.t.key[slot], empty_key<K>(), x);
+            if (prev == empty_key<K>() || prev == x) {
+              atomicAdd(&S.u.t.cnt[slot], 1u);
+              break;
+            }
+          }
+          slot++;
+          probes++;
         }
-        a.bucket_out[i] = S.excl;
-        if (i + 1 == n_buckets) a.bucket_out[i + 1] = S.excl + D;
+        if (get_overflow(&S.overflow)) break;
       }
       __syncthreads();
-      long long t4 = clock64();
-      write_runs<K>(S, D, out_keys, a.out_counts, S.excl);
-      __syncthreads();
-      if (threadIdx.x == 0 && a.prof) {
-        atomicAdd(a.prof + 3, (unsigned long long)(t4 - t3));
-        atomicAdd(a.prof + 4, (unsigned long long)(clock64() - t4));
+      constexpr int PER = (TSO + SC_NT - 1) / SC_NT;
+      const int s0 = tid * PER, s1 = min(s0 + PER, TSO);
+      uint32_t occ = 0;
+      if (!S.overflow) {
+        for (int s = s0; s < s1; s++) {
+          if (S.u.t.cnt[s] == 0) continue;
+          occ++;
+          if (s > 0 && S.u.t.cnt[s - 1] != 0) continue;  // not a cluster start
+          int e = s + 1;
+          while (e < TSO && S.u.t.cnt[e] != 0) e++;
+          if (e - s > SL_CLUSTER_LIMIT) {
+            set_overflow(&S.overflow);
+            break;
+          }
+          for (int q = s + 1; q < e; q++) {  // insertion sort of (key, count)
+            K x = S.u.t.key[q];
+            uint32_t c = S.u.t.cnt[q];
+            int r = q;
+            while (r > s && x < S.u.t.key[r - 1]) {
+              S.u.t.key[r] = S.u.t.key[r - 1];
+              S.u.t.cnt[r] = S.u.t.cnt[r - 1];
+              r--;
+            }
+            S.u.t.key[r] = x;
+            S.u.t.cnt[r] = c;
+          }
+        }
       }
-    } else {
-      if (threadIdx.x == 0 && a.prof) atomicAdd(a.prof + 5, 1ull);
-      if (threadIdx.x == 0) S.excl = lookback_prefix(a.status, i, a.err);
       __syncthreads();
-      const uint64_t excl = S.excl;
-      oversize_bucket<K>(S, a, keys, out_keys, start, n, skip, excl);
-      if (threadIdx.x == 0) {
-        st_release(a.status + i, LB_PRE | S.out);
-        a.bucket_out[i] = excl;
-        if (i + 1 == n_buckets) a.bucket_out[i + 1] = S.out;
+      if (!S.overflow) {
+        uint32_t D;
+        const uint32_t pos = block_exclusive_scan<SC_NT>(occ, S.tmp, &D);
+        const uint64_t base = start + S.run + pos;
+        uint32_t o = 0;
+        for (int s = s0; s < s1; s++) {
+          if (S.u.t.cnt[s] == 0) continue;
+          if (!in_bounds(a, 8, base + o, a.tmp_cap)) break;
+          tkeys[base + o] = S.u.t.key[s];
+          a.tmp_counts[base + o] = S.u.t.cnt[s];
+          o++;
+        }
+        __syncthreads();
+        if (tid == 0) S.run += D;
+        __syncthreads();
+        continue;
+      }
+      // ---- fallback: gather the slice's keys and sort them ----
+      if (tid == 0 && a.prof) atomicAdd(a.prof + 5, 1ull);
+      const uint32_t fh = j_hi - 1;
+      const int skip = (j_lo == fh) ? cb + SB : cb + SB - (32 - __clz(j_lo ^ fh));
+      SortSmem<K> &T = S.u.s;
+      if (tid == 0) S.cursor = 0;
+      __syncthreads();
+      const bool fits = ns <= (uint32_t)SortCap<K>::value;
+      if (!fits && ns > a.scratch_keys) {
+        if (tid == 0) atomicOr(a.err, ERR_OVERSIZE_SCRATCH);
+        __syncthreads();
+        continue;
+      }
+      if (!fits) {
+        // the global scratch area is shared by all CTAs: one user at a time
+        if (tid == 0) S.overflow = acquire_lock(a.scratch_lock, a.err) ? 0 : 1;
+        __syncthreads();
+        if (S.overflow) continue;  // wait ran out: reported through the error word
+      }
+      K *dst = fits ? T.A : reinterpret_cast<K *>(a.scratch);
+      for (uint64_t i = tid; i < n; i += SC_NT) {
+        const K x = keys[start + i];
+        const uint32_t sd = key_digit<K>(x, key_bits, cb, SB);
+        if (sd >= j_lo && sd < j_hi) {
+          const uint32_t w = atomicAdd(&S.cursor, 1u);
+          if (in_bounds(a, 1, w, fits ? (uint64_t)SortCap<K>::value : a.scratch_keys)) dst[w] = x;
+        }
       }
       __syncthreads();
+      if (tid == 0) T.out = start + S.run;
+      __syncthreads();
+      if (!in_bounds(a, 9, S.cursor, (uint64_t)ns + 1)) {
+        __syncthreads();
+        continue;
+      }
+      if (fits) {
+        smem_sort<K>(T, ns, key_bits, skip);
+        const uint32_t D = smem_runs<K>(T, ns);
+        if (!in_bounds(a, 10, T.out + D, a.tmp_cap + 1)) {
+          __syncthreads();
+          continue;
+        }
+        write_runs<K>(T, D, tkeys, a.tmp_counts, T.out);
+        __syncthreads();
+        if (tid == 0) S.run += D;
+      } else {
+        __threadfence_block();
+        scratch_sort<K>(T, a, ns, skip, tkeys, a.tmp_counts);
+        if (tid == 0) S.run = T.out - start;
+        // release the scratch area (all threads are past their last access)
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) atomicExch(a.scratch_lock, 0ull);
+      }
+      __syncthreads();
+    }
+    if (tid == 0) {
+      a.coarse_start[g] = start;
+      a.coarse_d[g] = S.run;
+    }
+    __syncthreads();
+  }
+}
+
+// Moves each coarse bucket's sorted runs to its final offset.
+template <typename K>
+__global__ void k_compact(const K *tkeys, const uint32_t *tcounts, const uint64_t *coarse_start,
+                          const unsigned long long *coarse_d, const uint64_t *coarse_out,
+                          const uint64_t *bucket_base, uint32_t nbins, K *out_keys,
+                          uint32_t *out_counts) {
+  const uint64_t nb = bucket_base[nbins];
+  for (uint64_t g = blockIdx.x; g < nb; g += gridDim.x) {
+    const uint64_t s = coarse_start[g], d = coarse_d[g], o = coarse_out[g];
+    for (uint64_t i = threadIdx.x; i < d; i += blockDim.x) {
+      out_keys[o + i] = tkeys[s + i];
+      out_counts[o + i] = tcounts[s + i];
     }
   }
 }
 
-__global__ void k_bin_out_offsets(const uint64_t *bucket_out, const uint64_t *bucket_base,
+// bin_out[b] = output offset of the first coarse bucket of bin b.
+__global__ void k_bin_out_offsets(const uint64_t *coarse_out, const uint64_t *bucket_base,
                                   uint32_t nbins, uint64_t *bin_out) {
   for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b <= nbins; b += gridDim.x * blockDim.x)
-    bin_out[b] = bucket_out[bucket_base[b]];
+    bin_out[b] = coarse_out[bucket_base[b]];
 }
 
-template __global__ void k_bucket_hist<uint64_t>(ExpandArgs);
-template __global__ void k_bucket_hist<u128>(ExpandArgs);
-template __global__ void k_bucket_scatter<uint64_t>(ExpandArgs);
-template __global__ void k_bucket_scatter<u128>(ExpandArgs);
-template __global__ void k_sort_count<uint64_t>(SortCountArgs);
-template __global__ void k_sort_count<u128>(SortCountArgs);
+template __global__ void k_coarse_hist<uint64_t>(ExpandArgs);
+template __global__ void k_coarse_hist<u128>(ExpandArgs);
+template __global__ void k_coarse_scatter<uint64_t>(ExpandArgs);
+template __global__ void k_coarse_scatter<u128>(ExpandArgs);
+template __global__ void k_coarse_count<uint64_t>(SortCountArgs);
+template __global__ void k_coarse_count<u128>(SortCountArgs);
+template __global__ void k_compact<uint64_t>(const uint64_t *, const uint32_t *, const uint64_t *,
+                                             const unsigned long long *, const uint64_t *,
+                                             const uint64_t *, uint32_t, uint64_t *, uint32_t *);
+template __global__ void k_compact<u128>(const u128 *, const uint32_t *, const uint64_t *,
+                                         const unsigned long long *, const uint64_t *,
+                                         const uint64_t *, uint32_t, u128 *, uint32_t *);
 
 }  // namespace gkc

@@ -43,68 +43,90 @@ struct CountPlan {
   uint32_t nbins;
   const uint64_t *bin_start;   // superkmers per bin (exclusive prefix, nbins+1)
   const uint64_t *bin_kstart;  // k-mers per bin (exclusive prefix, nbins+1)
-  uint32_t target_bucket;      // desired mean keys per bucket
-  uint32_t max_bits;           // bucket bits cap (<= 12)
-  uint32_t chunk_skm;          // superkmers per expansion chunk
+  uint32_t coarse_target;      // desired mean keys per coarse bucket
+  uint32_t max_bits;           // coarse bucket bits cap (<= 10)
+  uint64_t chunk_kmers;        // k-mers per expansion chunk
   int k;
   const uint32_t *err;         // nothing is planned after an upstream overflow
   // outputs
-  uint32_t *bin_bits;          // bucket bits per bin
-  uint64_t *bucket_base;       // first bucket of each bin (nbins+1)
+  uint32_t *bin_bits;          // coarse bucket bits per bin
+  uint64_t *bucket_base;       // first coarse bucket of each bin (nbins+1)
   uint64_t *chunk_base;        // first chunk of each bin (nbins+1)
+  uint64_t *hist_base;         // first (digit, chunk) entry of each bin (nbins+1)
 };
 __global__ void k_count_plan(CountPlan pl);
 
 struct ExpandArgs {
   const uint64_t *desc;        // bin-ordered superkmer descriptors
+  const uint64_t *koff;        // k-mer offset of each bin-ordered superkmer (n + 1)
   const uint8_t *packed;
   uint32_t nbins;
   const uint64_t *bin_start;
+  const uint64_t *bin_kstart;
   const uint64_t *chunk_base;
+  const uint64_t *hist_base;
   const uint32_t *bin_bits;
-  const uint64_t *bucket_base;
-  uint32_t chunk_skm;
+  uint32_t max_bits;
+  uint64_t chunk_kmers;
   int k;
-  unsigned long long *bucket_count;   // histogram pass output
-  unsigned long long *bucket_cursor;  // scatter pass: running fill
-  void *keys;                         // scatter pass output (uint64 or u128)
+  unsigned long long *chunk_hist;  // (bin, digit, chunk) counts
+  const uint64_t *chunk_off;       // their exclusive scan
+  void *keys;                      // scatter output (uint64 or u128)
   uint64_t keys_cap;
   uint32_t *err;
 };
-template <typename K> __global__ void k_bucket_hist(ExpandArgs a);
-template <typename K> __global__ void k_bucket_scatter(ExpandArgs a);
+template <typename K> __global__ void k_coarse_hist(ExpandArgs a);
+template <typename K> __global__ void k_coarse_scatter(ExpandArgs a);
+__global__ void k_skm_nk(const uint64_t *desc, const unsigned long long *n_skm_dev, int k,
+                         unsigned long long *nk);
 
 struct SortCountArgs {
-  const uint64_t *bucket_start;   // n_buckets + 1 (device exclusive prefix of bucket sizes)
-  const uint64_t *n_buckets_dev;  // device-side bucket count (bucket_base[nbins])
-  const uint64_t *bucket_base;    // per bin
-  const uint32_t *bin_bits;
   uint32_t nbins;
   int k;
-  void *keys;                     // bucketed keys (sorted output may alias it)
-  void *out_keys;
-  uint32_t *out_counts;
-  uint64_t *bucket_out;           // exclusive output offset per bucket (n_buckets + 1)
-  unsigned long long *status;     // look-back words, zeroed
+  const uint64_t *bucket_base;    // coarse buckets per bin (prefix, nbins+1)
+  const uint64_t *chunk_base;
+  const uint64_t *hist_base;
+  const uint32_t *bin_bits;
+  const uint64_t *chunk_off;      // coarse bucket (bin, digit) starts: entry (b, d, chunk 0)
+  const void *keys;               // coarse-bucketed keys
+  void *tmp_keys;                 // sorted runs per coarse bucket, at the bucket's start
+  uint32_t *tmp_counts;
+  uint64_t *coarse_start;         // per coarse bucket
+  unsigned long long *coarse_d;   // distinct keys per coarse bucket
   unsigned long long *ticket;     // zeroed
-  void *scratch;                  // 2 * scratch_keys keys for oversized buckets
+  unsigned long long *scratch_lock;  // zeroed; one CTA at a time uses the scratch
+  void *scratch;                  // 2 * scratch_keys keys for oversized slices
   uint64_t scratch_keys;
-  uint32_t *scratch_cnt;          // 16 * 4096 counters
+  uint32_t *scratch_cnt;          // 24 * 4096 counters
   uint32_t *err;
-  unsigned long long *prof;       // optional cycle counters (GKC_PROFILE_SORT), else null
+  unsigned long long *prof;       // optional counters, else null
+  int probe_limit;                // table probes before a slice falls back to sorting
+  uint64_t tmp_cap;               // capacity of tmp_keys / tmp_counts
+  unsigned long long *dbg;        // first failed bounds check: code, index, limit
 };
-template <typename K> __global__ void k_sort_count(SortCountArgs a);
-template <typename K> size_t sort_count_smem_bytes();
+template <typename K> __global__ void k_coarse_count(SortCountArgs a);
+template <typename K>
+__global__ void k_compact(const K *tkeys, const uint32_t *tcounts, const uint64_t *coarse_start,
+                          const unsigned long long *coarse_d, const uint64_t *coarse_out,
+                          const uint64_t *bucket_base, uint32_t nbins, K *out_keys,
+                          uint32_t *out_counts);
+template <typename K> size_t coarse_smem_bytes();
 template <typename K> int sort_count_cap();
-constexpr int kSortThreads = 512;
+constexpr int kSortThreads = 1024;
+constexpr uint32_t kCoarseTarget = 8192;
+constexpr uint32_t kCoarseMaxBits = 10;
+constexpr uint64_t kChunkKmers = 65536;
 
-__global__ void k_bin_out_offsets(const uint64_t *bucket_out, const uint64_t *bucket_base,
+__global__ void k_bin_out_offsets(const uint64_t *coarse_out, const uint64_t *bucket_base,
                                   uint32_t nbins, uint64_t *bin_out);
 
 // device-wide exclusive scan of uint64 counters (n <= 2^31)
 void scan_u64(const unsigned long long *in, uint64_t *out, uint64_t n, uint64_t *block_tmp,
               cudaStream_t st);
 size_t scan_u64_tmp_words(uint64_t n);
+// the same over a device-side length min(*n_dev, n_cap); out[n] = total
+void scan_u64_dev(const unsigned long long *in, uint64_t *out, uint64_t n_cap, const uint64_t *n_dev,
+                  uint64_t *block_tmp, cudaStream_t st);
 
 }  // namespace gkc
 

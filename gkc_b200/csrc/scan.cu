@@ -99,6 +99,74 @@ __global__ void k_scan_total(const uint64_t *tile_sum, uint64_t n_tiles, uint64_
 
 size_t scan_u64_tmp_words(uint64_t n) { return (n + SCAN_TILE - 1) / SCAN_TILE + 2; }
 
+// Same scan over a device-side length n = min(*n_dev, n_cap): blocks past it
+// contribute zero, out[n] receives the total.
+__global__ void k_scan_reduce_dev(const unsigned long long *in, uint64_t n_cap, const uint64_t *n_dev,
+                                  uint64_t *tile_sum) {
+  __shared__ uint64_t tmp[32];
+  const uint64_t n = min(n_cap, *n_dev);
+  uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE;
+  uint64_t s = 0;
+  for (int t = 0; t < SCAN_ITEMS; t++) {
+    uint64_t i = base + (uint64_t)t * SCAN_NT + threadIdx.x;
+    if (i < n) s += in[i];
+  }
+  s = block_sum_u64<SCAN_NT>(s, tmp);
+  if (threadIdx.x == 0) tile_sum[blockIdx.x] = s;
+}
+
+__global__ void k_scan_apply_dev(const unsigned long long *in, uint64_t n_cap, const uint64_t *n_dev,
+                                 const uint64_t *tile_sum, uint64_t *out) {
+  const uint64_t n = min(n_cap, *n_dev);
+  if ((uint64_t)blockIdx.x * SCAN_TILE >= n) return;
+  __shared__ uint64_t wsum[SCAN_NT / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
+  uint64_t v[SCAN_ITEMS], s = 0;
+  for (int t = 0; t < SCAN_ITEMS; t++) {
+    uint64_t i = base + t;
+    v[t] = i < n ? in[i] : 0;
+    s += v[t];
+  }
+  uint64_t x = s;
+  for (int d = 1; d < 32; d <<= 1) {
+    uint64_t y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t r = 0;
+    for (int w = 0; w < SCAN_NT / 32; w++) {
+      uint64_t t = wsum[w];
+      wsum[w] = r;
+      r += t;
+    }
+  }
+  __syncthreads();
+  uint64_t run = tile_sum[blockIdx.x] + wsum[warp] + x - s;
+  for (int t = 0; t < SCAN_ITEMS; t++) {
+    uint64_t i = base + t;
+    if (i < n) out[i] = run;
+    run += v[t];
+  }
+}
+
+__global__ void k_scan_total_dev(const uint64_t *tile_sum, uint64_t n_tiles, uint64_t n_cap,
+                                 const uint64_t *n_dev, uint64_t *out) {
+  out[min(n_cap, *n_dev)] = tile_sum[n_tiles];
+}
+
+void scan_u64_dev(const unsigned long long *in, uint64_t *out, uint64_t n_cap, const uint64_t *n_dev,
+                  uint64_t *block_tmp, cudaStream_t st) {
+  uint64_t n_tiles = (n_cap + SCAN_TILE - 1) / SCAN_TILE;
+  if (n_tiles == 0) n_tiles = 1;
+  k_scan_reduce_dev<<<(unsigned)n_tiles, SCAN_NT, 0, st>>>(in, n_cap, n_dev, block_tmp);
+  k_scan_tiles<<<1, SCAN_NT, 0, st>>>(block_tmp, n_tiles);
+  k_scan_apply_dev<<<(unsigned)n_tiles, SCAN_NT, 0, st>>>(in, n_cap, n_dev, block_tmp, out);
+  k_scan_total_dev<<<1, 1, 0, st>>>(block_tmp, n_tiles, n_cap, n_dev, out);
+}
+
 void scan_u64(const unsigned long long *in, uint64_t *out, uint64_t n, uint64_t *block_tmp,
               cudaStream_t st) {
   uint64_t n_tiles = (n + SCAN_TILE - 1) / SCAN_TILE;

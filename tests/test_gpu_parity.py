@@ -207,3 +207,16 @@ def test_plain_count_after_fused_partition(ctx):
     lib_partition(ctx, d["reads"], d["offs"], k, p, hpc, nb)
     got, _ = lib_counts(ctx, k, nb, mode=G.MODE_PLAIN)
     assert_counts_equal(got, dict(bin_off=d["cnt_bin_off"], keys_lo=d["cnt_keys"], counts=d["cnt_counts"]))
+
+
+@pytest.mark.parametrize("seed,n,lo,hi,k,p,hpc,nb", [CASES[0], CASES[2], CASES[7]])
+def test_sort_fallback_forced(ctx, seed, n, lo, hi, k, p, hpc, nb, monkeypatch):
+    """With a probe limit of 0 every slice that has a collision falls back to
+    the shared-memory / global-scratch sort (serialised through the scratch
+    lock); results must not change."""
+    monkeypatch.setenv("GKC_PROBE_LIMIT", "0")
+    reads, offs = random_reads(seed, n, lo, hi)
+    o = F.oracle_partition(reads, offs, k, p, hpc, nb)
+    lib_partition(ctx, reads, offs, k, p, hpc, nb)
+    got, _ = lib_counts(ctx, k, nb)
+    assert_counts_equal(got, F.oracle_count_bins(o, k, nb))
