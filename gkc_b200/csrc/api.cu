@@ -933,6 +933,10 @@ gkc_status gkc_count_superkmers_host(gkc_ctx *c, int k, const uint32_t *skm_len,
   c->pv.skm_minimizer = dmm;
   c->pv.packed = dp;
   c->part_nbytes_dev = nullptr;
+  // the count path sizes its per-superkmer arrays from the partition's
+  // capacities, which a fresh context has not set
+  c->part_cap_skm = n_skm + 1;
+  c->part_cap_bytes = off + 16;
   c->have_part = true;
   gkc_params prm{k, 3, 0, 1};
   c->pp = prm;

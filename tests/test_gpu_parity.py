@@ -173,6 +173,28 @@ def test_count_superkmers_host_one_bin(ctx):
         assert np.array_equal(counts, d["cnt_counts"][lo:hi])
 
 
+@pytest.mark.parametrize("mode", [G.MODE_BATCHED, G.MODE_PLAIN])
+def test_count_superkmers_host_fresh_context(mode):
+    """A context that has never partitioned counts a superkmer group (with
+    superkmers shorter than k among them) exactly as the oracle does."""
+    r = np.random.default_rng(40 + mode)
+    k, pool, n = 27, 300, 9000
+    base_lens = r.integers(10, 110, pool).astype(np.uint32)
+    base = [r.integers(0, 256, int((ln + 3) // 4), dtype=np.uint8) for ln in base_lens]
+    pick = r.integers(0, pool, n)
+    lens = base_lens[pick]
+    packed = np.concatenate([base[i] for i in pick])
+    boff = np.zeros(n, np.uint64)
+    boff[1:] = np.cumsum((lens[:-1].astype(np.uint64) + 3) // 4)
+    want = F.oracle_count_bins(F.Skms(np.zeros(n, np.uint32), lens, boff, packed), k, 1)
+    with G.Context(0) as fresh:
+        nd = fresh.count_superkmers_host(k, lens, packed, mode)
+        assert nd == len(want["keys_lo"])
+        _, keys, counts = fresh.count_copy_out(fresh.count_device(G.params(k, 3, 1), mode))
+    assert np.array_equal(keys[:, 0], want["keys_lo"])
+    assert np.array_equal(counts, want["counts"])
+
+
 PLAIN_CASES = [
     (11, 300, 31, 900, 31, 11, 0, 256),
     (12, 200, 21, 700, 21, 7, 1, 31),
