@@ -95,6 +95,7 @@ SIGNATURES = [
     ("gkc_count_device", C.c_int, [vp, P(Params), C.c_int, P(CountView)]),
     ("gkc_count_superkmers_host", C.c_int, [vp, C.c_int, vp, vp, u64, C.c_int, P(u64)]),
     ("gkc_count_copy_out", C.c_int, [vp, vp, vp, vp]),
+    ("gkc_count_superkmers_device_noalloc", C.c_int, [C.c_int, vp, vp, u64, u64, vp, vp, P(u64), vp]),
     ("gkc_pipeline_device", C.c_int, [vp, P(Params), C.c_int, vp, u64, vp, u64, P(PartitionView),
                                       P(CountView)]),
     ("gkc_pipeline_host", C.c_int, [vp, P(Params), C.c_int, vp, vp, u64, P(CountView)]),

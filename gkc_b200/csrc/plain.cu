@@ -12,6 +12,7 @@
 //   per bin: expand -> onesweep LSD radix sort -> run-length count.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -400,4 +401,185 @@ gkc_status count_plain_impl(gkc_ctx *c, const gkc_params *prm) {
   CK(cudaMemsetAsync(c->bufs["err"].p, 0, 16, c->st));
   if (prm->k <= 32) return count_plain_t<uint64_t>(c, prm);
   return count_plain_t<u128>(c, prm);
+}
+
+// ---------------------------------------------------------------------------
+// Counting one group of packed superkmers without allocating any memory.
+//
+// Some callers cannot allocate device memory while they run: a host program
+// that hands the GPU to this library inside its own fixed memory pool, a
+// framework whose allocator owns all of HBM, or code on a path where a
+// cudaMalloc would synchronise the device or fail under a hard memory cap.
+// This entry point serves them.  It runs the same kernels as the per-stage
+// counting path above (expand, onesweep radix sort, run-length encoding), but
+// all its scratch memory is carved out of one fixed array of device memory
+// that the library declares at file scope; the caller passes only the inputs
+// and the output buffers.  Every GPU that loads the library holds the array
+// (about 23 MB) until the process exits.
+// ---------------------------------------------------------------------------
+namespace gkc {
+namespace noalloc {
+
+constexpr uint64_t kMaxKmers = 1ull << 20;  // k-mers per call
+constexpr uint64_t kMaxSkm = 1ull << 17;    // superkmers per call
+constexpr int kMaxDevices = 64;
+
+constexpr uint64_t round_up(uint64_t w) { return (w + 31) & ~31ull; }  // 256-byte steps
+constexpr uint64_t kOsTileMax = 4096;  // keys per onesweep tile (checked at set-up)
+constexpr uint64_t kRleBlocks = (kMaxKmers + RLE_TILE - 1) / RLE_TILE + 1;
+// word offsets of the parts of the array
+constexpr uint64_t W_SORT = 0;
+constexpr uint64_t W_STARTS = W_SORT + round_up(kMaxKmers + 16);
+constexpr uint64_t W_NBYTES = W_STARTS + round_up(kMaxKmers + 16);
+constexpr uint64_t W_BOFF = W_NBYTES + round_up(kMaxSkm + 2);
+constexpr uint64_t W_NK = W_BOFF + round_up(kMaxSkm + 2);
+constexpr uint64_t W_KOFF = W_NK + round_up(kMaxSkm + 2);
+constexpr uint64_t W_DESC = W_KOFF + round_up(kMaxSkm + 2);
+constexpr uint64_t W_STMP = W_DESC + round_up(kMaxSkm + 2);
+constexpr uint64_t W_HIST = W_STMP + round_up(kMaxSkm / 1024 + 16);
+constexpr uint64_t W_LB = W_HIST + round_up(16 * 256);
+constexpr uint64_t W_TICKET = W_LB + round_up(((kMaxKmers + kOsTileMax - 1) / kOsTileMax + 1) * 256);
+constexpr uint64_t W_ERR = W_TICKET + 32;
+constexpr uint64_t W_RBLK = W_ERR + 32;
+constexpr uint64_t W_ROFF = W_RBLK + round_up(kRleBlocks + 1);
+constexpr uint64_t W_RTMP = W_ROFF + round_up(kRleBlocks + 2);
+constexpr uint64_t W_CURSOR = W_RTMP + round_up(kRleBlocks / 1024 + 16);
+constexpr uint64_t W_BINOUT = W_CURSOR + 32;
+constexpr uint64_t kWords = W_BINOUT + 32;
+
+// The scratch array.  In host code this name is only a stand-in for the
+// device symbol, not a device address; the host takes the real address with
+// cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned long long scratch[kWords];
+
+// per superkmer: packed bytes, k-mers; flags lengths the descriptor cannot hold
+__global__ void k_prepare(const uint32_t *len, uint64_t n, int k, unsigned long long *nbytes,
+                          unsigned long long *nk, uint32_t *err) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t l = len[i];
+    if (l > 0xFFFFFFu) atomicOr(err, ERR_BAD_READ);
+    nbytes[i] = (l + 3u) / 4u;
+    nk[i] = l >= (uint32_t)k ? l - k + 1 : 0;
+  }
+}
+
+// descriptor of superkmer i: (first packed byte << 24) | length
+__global__ void k_desc(const uint32_t *len, const uint64_t *boff, uint64_t n, uint64_t *desc) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    desc[i] = (boff[i] << 24) | (len[i] & 0xFFFFFFu);
+}
+
+struct Dev {
+  unsigned long long *base = nullptr;
+  int sms = 0;
+};
+static std::mutex g_mu;
+static Dev g_dev[kMaxDevices];
+
+// Set-up for the current device, once: the array's device address and the
+// SM count.
+static gkc_status setup(int dev, Dev *out) {
+  if (dev < 0 || dev >= kMaxDevices) return GKC_ERR_NO_DEVICE;
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (!g_dev[dev].base) {
+    if (onesweep_lookback_words(kMaxKmers) > W_TICKET - W_LB) return GKC_ERR_INTERNAL;
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      return GKC_ERR_CUDA;
+    }
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess || sms <= 0) {
+      cudaGetLastError();
+      return GKC_ERR_CUDA;
+    }
+    g_dev[dev].base = static_cast<unsigned long long *>(p);
+    g_dev[dev].sms = sms;
+  }
+  *out = g_dev[dev];
+  return GKC_OK;
+}
+
+}  // namespace noalloc
+}  // namespace gkc
+
+#define NA_CK(call)                    \
+  do {                                 \
+    if ((call) != cudaSuccess) {       \
+      cudaGetLastError();              \
+      return GKC_ERR_CUDA;             \
+    }                                  \
+  } while (0)
+
+extern "C" gkc_status gkc_count_superkmers_device_noalloc(int k, const uint32_t *d_skm_len,
+                                                          const uint8_t *d_packed, uint64_t n_skm,
+                                                          uint64_t out_capacity, uint64_t *d_keys_out,
+                                                          uint32_t *d_counts_out, uint64_t *n_distinct,
+                                                          void *cuda_stream) {
+  using namespace gkc;
+  using namespace gkc::noalloc;
+  if (k < 1 || k > 32 || !n_distinct) return GKC_ERR_INVALID_ARG;
+  if (n_skm > kMaxSkm) return GKC_ERR_CAPACITY;
+  if (n_skm && (!d_skm_len || !d_packed)) return GKC_ERR_INVALID_ARG;
+  if (out_capacity && (!d_keys_out || !d_counts_out)) return GKC_ERR_INVALID_ARG;
+  *n_distinct = 0;
+  if (n_skm == 0) return GKC_OK;
+  int dev = 0;
+  NA_CK(cudaGetDevice(&dev));
+  Dev d;
+  gkc_status s = setup(dev, &d);
+  if (s != GKC_OK) return s;
+  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+  unsigned long long *w = d.base;
+  auto u64p = [&](uint64_t off) { return reinterpret_cast<uint64_t *>(w + off); };
+  uint32_t *err = reinterpret_cast<uint32_t *>(w + W_ERR);
+  const unsigned grid = (unsigned)d.sms * 8;
+
+  // the array keeps the previous call's contents: clear what must start at zero
+  NA_CK(cudaMemsetAsync(w + W_ERR, 0, 32 * 8, st));
+  NA_CK(cudaMemsetAsync(w + W_CURSOR, 0, 32 * 8, st));
+  NA_CK(cudaMemsetAsync(w + W_BINOUT, 0, 32 * 8, st));
+  k_prepare<<<grid, 256, 0, st>>>(d_skm_len, n_skm, k, w + W_NBYTES, w + W_NK, err);
+  scan_u64(w + W_NBYTES, u64p(W_BOFF), n_skm, u64p(W_STMP), st);
+  scan_u64(w + W_NK, u64p(W_KOFF), n_skm, u64p(W_STMP), st);
+  NA_CK(cudaPeekAtLastError());
+  uint64_t total = 0;
+  uint32_t e = 0;
+  NA_CK(cudaMemcpyAsync(&total, u64p(W_KOFF) + n_skm, 8, cudaMemcpyDeviceToHost, st));
+  NA_CK(cudaMemcpyAsync(&e, err, 4, cudaMemcpyDeviceToHost, st));
+  NA_CK(cudaStreamSynchronize(st));
+  if (e & ERR_BAD_READ) return GKC_ERR_INVALID_ARG;  // a length above 2^24 - 1
+  if (total > kMaxKmers || total > out_capacity) return GKC_ERR_CAPACITY;
+  if (total == 0) return GKC_OK;
+
+  k_desc<<<grid, 256, 0, st>>>(d_skm_len, u64p(W_BOFF), n_skm, u64p(W_DESC));
+  uint64_t *keys = u64p(W_SORT);
+  k_plain_expand<uint64_t><<<grid, 256, 0, st>>>(u64p(W_DESC), d_packed, 0, n_skm, u64p(W_KOFF), 0, k,
+                                                  keys);
+  // the caller's key buffer serves as the sort's second buffer
+  OnesweepScratch os{w + W_HIST, w + W_LB, w + W_TICKET, err, d.sms * 4};
+  uint32_t launches = 0;
+  OnesweepStatus r = onesweep_sort<uint64_t>(keys, d_keys_out, u64p(W_KOFF) + n_skm, total, 2 * k, os,
+                                             st, &launches);
+  if (r.result_in_alt) NA_CK(cudaMemcpyAsync(keys, d_keys_out, total * 8, cudaMemcpyDeviceToDevice, st));
+  const uint64_t nblk = (total + RLE_TILE - 1) / RLE_TILE;
+  unsigned long long *cursor = w + W_CURSOR;
+  k_rle_mark<uint64_t><<<(unsigned)nblk, RLE_NT, 0, st>>>(keys, total, w + W_RBLK);
+  scan_u64(w + W_RBLK, u64p(W_ROFF), nblk, u64p(W_RTMP), st);
+  k_rle_emit<uint64_t><<<(unsigned)nblk, RLE_NT, 0, st>>>(keys, total, u64p(W_ROFF), cursor, d_keys_out,
+                                                          u64p(W_STARTS));
+  k_rle_counts<<<grid, 256, 0, st>>>(u64p(W_STARTS), u64p(W_ROFF), nblk, total, cursor, d_counts_out);
+  k_rle_advance<<<1, 1, 0, st>>>(u64p(W_ROFF), nblk, cursor, u64p(W_BINOUT), 0, 0);
+  NA_CK(cudaPeekAtLastError());
+  uint64_t nd = 0;
+  NA_CK(cudaMemcpyAsync(&nd, cursor, 8, cudaMemcpyDeviceToHost, st));
+  NA_CK(cudaMemcpyAsync(&e, err, 4, cudaMemcpyDeviceToHost, st));
+  NA_CK(cudaStreamSynchronize(st));
+  if (e & ERR_SPIN_TIMEOUT) return GKC_ERR_DEVICE_TIMEOUT;
+  *n_distinct = nd;
+  return GKC_OK;
 }

@@ -135,6 +135,33 @@ gkc_status gkc_count_superkmers_host(gkc_ctx *ctx, int k, const uint32_t *skm_le
 /* Copies the last count result: bin_off[nbins+1], keys[n_distinct*key_words],
  * counts[n_distinct]; any pointer may be NULL. */
 gkc_status gkc_count_copy_out(gkc_ctx *ctx, uint64_t *bin_off, uint64_t *keys, uint32_t *counts);
+/* Counts one group of packed superkmers already in device memory without
+ * allocating anything.  No counterpart in the reference: it exists for callers
+ * that cannot allocate device memory while they run (a program that owns the
+ * whole GPU through its own memory pool, a framework whose allocator holds all
+ * of HBM, or a path where a cudaMalloc would stall the device or break a hard
+ * memory cap).  It needs no context; it runs on the calling thread's current
+ * device and on `cuda_stream` (NULL: the default stream), and returns after
+ * the stream has finished its work.
+ *   Input: skm_len[n_skm] and the packed bytes back to back, as for
+ *   gkc_count_superkmers_host (k <= 32).  Output: the distinct canonical
+ *   k-mers in ascending order in d_keys_out and their counts in d_counts_out;
+ *   both must hold out_capacity >= the group's k-mer count entries (the key
+ *   buffer is also the sort's second buffer).  *n_distinct receives the count.
+ * Scratch memory is one fixed array of about 23 MB of device memory inside
+ * the library, held by every GPU that loads it until the process exits.  It
+ * bounds a call to 131,072 superkmers and 1,048,576 k-mers: larger groups are
+ * rejected with GKC_ERR_CAPACITY (GKC_ERR_INVALID_ARG for k > 32).  The first
+ * call on a device looks up the array's device address; make that first call
+ * before any stream capture.  All calls share the one array and each leaves
+ * its contents behind (the next call clears what must start at zero), so
+ * calls that overlap on the GPU, from different streams or threads, race and
+ * must not be made. */
+gkc_status gkc_count_superkmers_device_noalloc(int k, const uint32_t *d_skm_len,
+                                               const uint8_t *d_packed, uint64_t n_skm,
+                                               uint64_t out_capacity, uint64_t *d_keys_out,
+                                               uint32_t *d_counts_out, uint64_t *n_distinct,
+                                               void *cuda_stream);
 
 /* ---- whole pipeline: reads -> superkmer partitions -> sorted (k-mer, count)
  *      (reference: process_reads_count + gen_skm_and_count_with_TP,
