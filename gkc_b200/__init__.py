@@ -142,6 +142,8 @@ def _ptr(a):
     """Address of a numpy array or a torch tensor."""
     if a is None:
         return None
+    if isinstance(a, int):  # a raw device address
+        return a or None
     if hasattr(a, "data_ptr"):
         return a.data_ptr()
     return a.ctypes.data

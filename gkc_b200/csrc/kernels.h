@@ -135,4 +135,10 @@ __global__ void k_hpc_count(const uint8_t *reads, const uint64_t *offs, uint64_t
                             unsigned long long *run_len);
 __global__ void k_hpc_write(const uint8_t *reads, const uint64_t *offs, uint64_t n_reads,
                             const uint64_t *hpc_offs, uint8_t *out, int32_t *orig_pos);
+// Run-length pass over sorted keys (distinct keys + first indices).
+uint64_t rle_block_count(uint64_t n);
+template <typename K>
+void rle_runs(const K *sorted, uint64_t n, unsigned long long *blk, uint64_t *blk_off, uint64_t *tmp,
+              const unsigned long long *cursor, K *out_keys, uint64_t *starts, cudaStream_t st);
+
 }  // namespace gkc

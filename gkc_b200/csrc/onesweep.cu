@@ -71,9 +71,11 @@ __global__ void k_os_digit_offsets(unsigned long long *hist, int passes) {
   }
 }
 
-template <typename K>
-__global__ void __launch_bounds__(OS_NT) k_os_pass(const K *in, K *out, const uint64_t *n_dev,
-                                                   int pass, const unsigned long long *digit_base,
+// One digit pass.  With KV, a uint32 value moves with each key (vin -> vout).
+template <typename K, bool KV>
+__global__ void __launch_bounds__(OS_NT) k_os_pass(const K *in, K *out, const uint32_t *vin,
+                                                   uint32_t *vout, const uint64_t *n_dev, int pass,
+                                                   const unsigned long long *digit_base,
                                                    unsigned long long *lookback,
                                                    unsigned long long *ticket, uint32_t *err) {
   __shared__ uint32_t warp_cnt[OS_WARPS][OS_RADIX];
@@ -94,11 +96,13 @@ __global__ void __launch_bounds__(OS_NT) k_os_pass(const K *in, K *out, const ui
     const uint64_t seg = tile * OS_TILE + (uint64_t)warp * 32 * OS_ITEMS;
     K key[OS_ITEMS];
     uint32_t rank[OS_ITEMS];
+    uint32_t val[KV ? OS_ITEMS : 1];
 #pragma unroll
     for (int r = 0; r < OS_ITEMS; r++) {
       const uint64_t i = seg + (uint64_t)r * 32 + lane;
       const bool v = i < n;
       key[r] = v ? in[i] : (K)0;
+      if (KV) val[KV ? r : 0] = v ? vin[i] : 0u;
       const uint32_t d = v ? os_digit<K>(key[r], pass) : 0xFFFFFFFFu;
       const uint32_t peers = __match_any_sync(0xffffffffu, d);
       const uint32_t below = __popc(peers & ((1u << lane) - 1u));
@@ -153,16 +157,19 @@ __global__ void __launch_bounds__(OS_NT) k_os_pass(const K *in, K *out, const ui
       const uint64_t i = seg + (uint64_t)r * 32 + lane;
       if (i < n) {
         const uint32_t d = os_digit<K>(key[r], pass);
-        out[tile_prefix[d] + warp_cnt[warp][d] + rank[r]] = key[r];
+        const uint64_t dst = tile_prefix[d] + warp_cnt[warp][d] + rank[r];
+        out[dst] = key[r];
+        if (KV) vout[dst] = val[KV ? r : 0];
       }
     }
     __syncthreads();
   }
 }
 
-template <typename K>
-OnesweepStatus onesweep_sort(K *keys, K *alt, const uint64_t *n_dev, uint64_t n_max, int key_bits,
-                             OnesweepScratch s, cudaStream_t st, uint32_t *launches) {
+template <typename K, bool KV>
+static OnesweepStatus onesweep_run(K *keys, K *alt, uint32_t *vals, uint32_t *valt, const uint64_t *n_dev,
+                                   uint64_t n_max, int key_bits, OnesweepScratch s, cudaStream_t st,
+                                   uint32_t *launches) {
   const int passes = (key_bits + 7) / 8;
   const uint64_t tiles = (n_max + OS_TILE - 1) / OS_TILE;
   cudaMemsetAsync(s.hist, 0, sizeof(unsigned long long) * 16 * OS_RADIX, st);
@@ -171,17 +178,35 @@ OnesweepStatus onesweep_sort(K *keys, K *alt, const uint64_t *n_dev, uint64_t n_
   k_os_digit_offsets<<<1, 32 * 8, 0, st>>>(s.hist, passes);
   *launches += 2;
   K *src = keys, *dst = alt;
+  uint32_t *vsrc = vals, *vdst = valt;
   for (int p = 0; p < passes; p++) {
     cudaMemsetAsync(s.lookback, 0, sizeof(unsigned long long) * (tiles + 1) * OS_RADIX, st);
     cudaMemsetAsync(s.ticket, 0, sizeof(unsigned long long), st);
     unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)s.max_ctas));
-    k_os_pass<K><<<grid, OS_NT, 0, st>>>(src, dst, n_dev, p, s.hist, s.lookback, s.ticket, s.err);
+    k_os_pass<K, KV><<<grid, OS_NT, 0, st>>>(src, dst, vsrc, vdst, n_dev, p, s.hist, s.lookback,
+                                              s.ticket, s.err);
     *launches += 1;
     K *t = src;
     src = dst;
     dst = t;
+    uint32_t *vt = vsrc;
+    vsrc = vdst;
+    vdst = vt;
   }
   return OnesweepStatus{src == keys ? 0 : 1};
+}
+
+template <typename K>
+OnesweepStatus onesweep_sort(K *keys, K *alt, const uint64_t *n_dev, uint64_t n_max, int key_bits,
+                             OnesweepScratch s, cudaStream_t st, uint32_t *launches) {
+  return onesweep_run<K, false>(keys, alt, nullptr, nullptr, n_dev, n_max, key_bits, s, st, launches);
+}
+
+template <typename K>
+OnesweepStatus onesweep_sort_kv(K *keys, K *alt, uint32_t *vals, uint32_t *valt, const uint64_t *n_dev,
+                                uint64_t n_max, int key_bits, OnesweepScratch s, cudaStream_t st,
+                                uint32_t *launches) {
+  return onesweep_run<K, true>(keys, alt, vals, valt, n_dev, n_max, key_bits, s, st, launches);
 }
 
 size_t onesweep_lookback_words(uint64_t n_max) {
@@ -192,5 +217,10 @@ template OnesweepStatus onesweep_sort<uint64_t>(uint64_t *, uint64_t *, const ui
                                                 int, OnesweepScratch, cudaStream_t, uint32_t *);
 template OnesweepStatus onesweep_sort<u128>(u128 *, u128 *, const uint64_t *, uint64_t, int,
                                             OnesweepScratch, cudaStream_t, uint32_t *);
+template OnesweepStatus onesweep_sort_kv<uint64_t>(uint64_t *, uint64_t *, uint32_t *, uint32_t *,
+                                                   const uint64_t *, uint64_t, int, OnesweepScratch,
+                                                   cudaStream_t, uint32_t *);
+template OnesweepStatus onesweep_sort_kv<u128>(u128 *, u128 *, uint32_t *, uint32_t *, const uint64_t *,
+                                               uint64_t, int, OnesweepScratch, cudaStream_t, uint32_t *);
 
 }  // namespace gkc

@@ -188,6 +188,24 @@ __global__ void k_rle_advance(const uint64_t *blk_off, uint64_t n_blk, unsigned 
   bin_out[b + 1] = *out_cursor;
 }
 
+// Distinct keys of sorted[0, n) to out_keys (after *cursor) and the index of
+// each one's first occurrence to starts: the run-length kernels above.
+uint64_t rle_block_count(uint64_t n) { return (n + RLE_TILE - 1) / RLE_TILE; }
+
+template <typename K>
+void rle_runs(const K *sorted, uint64_t n, unsigned long long *blk, uint64_t *blk_off, uint64_t *tmp,
+              const unsigned long long *cursor, K *out_keys, uint64_t *starts, cudaStream_t st) {
+  const uint64_t nblk = rle_block_count(n);
+  if (nblk == 0) return;
+  k_rle_mark<K><<<(unsigned)nblk, RLE_NT, 0, st>>>(sorted, n, blk);
+  scan_u64(blk, blk_off, nblk, tmp, st);
+  k_rle_emit<K><<<(unsigned)nblk, RLE_NT, 0, st>>>(sorted, n, blk_off, cursor, out_keys, starts);
+}
+template void rle_runs<uint64_t>(const uint64_t *, uint64_t, unsigned long long *, uint64_t *, uint64_t *,
+                                 const unsigned long long *, uint64_t *, uint64_t *, cudaStream_t);
+template void rle_runs<u128>(const u128 *, uint64_t, unsigned long long *, uint64_t *, uint64_t *,
+                             const unsigned long long *, u128 *, uint64_t *, cudaStream_t);
+
 }  // namespace gkc
 
 #define CK(call)                                  \

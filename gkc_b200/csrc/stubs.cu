@@ -1,18 +1,6 @@
 // Entry points whose kernels are not in this build yet.
 #include "ctx.h"
 
-gkc_status gkc_minimizers_device(gkc_ctx *c, const gkc_params *, const char *, uint64_t,
-                                 const uint64_t *, uint64_t, uint32_t *, uint8_t *, int8_t *) {
-  return ctx_fail(c, GKC_ERR_INTERNAL, "not built");
-}
-gkc_status gkc_subsample_positions_device(gkc_ctx *c, const gkc_params *, uint32_t, const char *,
-                                          uint64_t, const uint64_t *, uint64_t, gkc_poslist_view *) {
-  return ctx_fail(c, GKC_ERR_INTERNAL, "not built");
-}
-gkc_status gkc_hpc_device(gkc_ctx *c, const char *, uint64_t, const uint64_t *, uint64_t, char *,
-                          uint64_t *, int32_t *) {
-  return ctx_fail(c, GKC_ERR_INTERNAL, "not built");
-}
 gkc_status gkc_server_create(int, uint64_t, int, gkc_server **) { return GKC_ERR_INTERNAL; }
 void gkc_server_destroy(gkc_server *) {}
 gkc_status gkc_server_submit(gkc_server *, const gkc_params *, const char *, const uint64_t *,
