@@ -292,3 +292,88 @@ def skms_from_copy(bin_off, lens, boff, packed):
     nb = len(bin_off) - 1
     bins = np.repeat(np.arange(nb, dtype=np.uint32), np.diff(bin_off).astype(np.int64))
     return bins, lens, boff, packed
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = range(5)
+GEN_IID, GEN_GENOME_SHORT, GEN_GENOME_LONG = 1, 2, 3
+
+
+class Server:
+    """Continuous-batching counting server on one device (gkc_server_*)."""
+
+    def __init__(self, device=0, hbm_budget=0, max_running=4):
+        self._L = lib()
+        h = C.c_void_p()
+        st = self._L.gkc_server_create(int(device), int(hbm_budget), int(max_running), C.byref(h))
+        if st != 0:
+            raise GkcError(st, "gkc_server_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self._L.gkc_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st, what):
+        if st != 0:
+            raise GkcError(st, what)
+
+    def submit(self, reads, offs, prm):
+        reads = np.ascontiguousarray(reads, np.uint8)
+        offs = np.ascontiguousarray(offs, np.uint64)
+        jid = C.c_uint64()
+        self._check(self._L.gkc_server_submit(self.h, C.byref(prm), _ptr(reads), _ptr(offs),
+                                              len(offs) - 1, C.byref(jid)), "submit")
+        return int(jid.value)
+
+    def submit_synth(self, prm, generator, seed, n_bases):
+        jid = C.c_uint64()
+        self._check(self._L.gkc_server_submit_device_synth(self.h, C.byref(prm), int(generator),
+                                                           int(seed), int(n_bases), C.byref(jid)),
+                    "submit_device_synth")
+        return int(jid.value)
+
+    def poll(self, jid):
+        info = JobInfo()
+        self._check(self._L.gkc_server_poll(self.h, int(jid), C.byref(info)), "poll")
+        return info
+
+    def wait(self, jid, timeout=-1.0):
+        info = JobInfo()
+        st = self._L.gkc_server_wait(self.h, int(jid), float(timeout), C.byref(info))
+        if st not in (0, 8):
+            raise GkcError(st, "wait")
+        return info
+
+    def cancel(self, jid):
+        self._check(self._L.gkc_server_cancel(self.h, int(jid)), "cancel")
+
+    def result(self, jid):
+        """-> (bin_off, keys (n, key_words), counts) of a finished job."""
+        info = self.poll(jid)
+        nd, nb, kw = int(info.n_distinct), int(info.nbins), int(info.key_words)
+        bin_off = np.zeros(nb + 1, np.uint64)
+        keys = np.zeros(max(nd * kw, 1), np.uint64)
+        counts = np.zeros(max(nd, 1), np.uint32)
+        self._check(self._L.gkc_server_copy_result(self.h, int(jid), _ptr(bin_off), _ptr(keys),
+                                                   _ptr(counts)), "copy_result")
+        return bin_off, keys[:nd * kw].reshape(nd, kw), counts[:nd]
+
+    def release(self, jid):
+        self._check(self._L.gkc_server_release(self.h, int(jid)), "release")
+
+
+def job_hbm_estimate(prm, n_bases, n_reads):
+    return int(lib().gkc_job_hbm_estimate(C.byref(prm), int(n_bases), int(n_reads)))

@@ -259,6 +259,32 @@ static void partition_caps(const gkc_params *prm, uint64_t n_bytes, uint64_t n_r
   *cap_bytes = (w + s * (uint64_t)(prm->k - 1)) / 4 + s + tiles * 16 + 64;
 }
 
+// Device bytes one pipeline run over n_bases bases in n_reads reads needs:
+// the workspaces the batched pipeline sizes for it (reads uploaded from the
+// host, optional HPC copies, the read-start bitmap, superkmers in tile and bin
+// order, k-mer offsets, coarse-bucket matrices, keys, runs, counts, sort
+// scratch) plus a fixed allowance for the small per-bin arrays.
+uint64_t gkc_job_hbm_estimate(const gkc_params *prm, uint64_t n_bases, uint64_t n_reads) {
+  if (!prm || prm->k < 1 || prm->k > 64 || prm->nbins < 1) return 0;
+  const uint64_t B = n_bases, R = n_reads, w = prm->k <= 32 ? 8 : 16;
+  uint64_t cap_skm, cap_bytes;
+  partition_caps(prm, B, R, &cap_skm, &cap_bytes);
+  uint64_t e = (B + 64) + 8 * (R + 1);                                  // reads, offsets
+  if (prm->hpc) e += 8 * (R + 1) + 8 * (R + 2) + (B + 64) + 4 * (B + 16);  // HPC copies
+  e += (B + 1) / 8 + 16;                                                 // read starts
+  e += cap_skm * (8 + 4 + 8 + 4) + cap_bytes;                            // superkmers
+  e += cap_skm * 16;                                                     // k-mer offsets
+  const uint64_t kc = std::max<uint64_t>(B, 16);
+  uint32_t max_bits = kCoarseMaxBits;
+  while (max_bits > 0 && ((uint64_t)prm->nbins << max_bits) > (1ull << 20)) max_bits--;
+  const uint64_t hist_cap = ((kc / kChunkKmers) + prm->nbins + 1) << max_bits;
+  e += 16 * hist_cap;                                                    // chunk matrices
+  e += w * kc * 2 + 4 * kc * 2;                                          // keys, runs, counts
+  e += 2 * w * (kc / 16) + 24 * 4096 * 4;                                // sort scratch
+  e += ((uint64_t)prm->nbins << max_bits) * 8 * 4;                       // coarse buckets
+  return e + (64ull << 20);
+}
+
 // Enqueues HPC (optional), partition and bin scatter on c->st.
 static gkc_status enqueue_partition(gkc_ctx *c, const gkc_params *prm, const char *d_reads,
                                     uint64_t n_bytes, const uint64_t *d_offs, uint64_t n_reads,
