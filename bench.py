@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--seed", type=int, default=SEED)
+    ap.add_argument("--serve", action="store_true",
+                    help="only the serving mix (config 5): 1000 jobs at 50/80/95%% load")
+    ap.add_argument("--serve-jobs", type=int, default=None)
+    ap.add_argument("--no-serve", action="store_true")
     return ap.parse_args()
 
 
@@ -217,6 +221,109 @@ def run_reference(args, wl):
                          "sample": sample},
         "e2e": {"value": value, "unit": "kmers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def serve_mix(G, device, n_jobs, loads, seed, max_running=4, lo=1e5, hi=1e9, calib_jobs=40):
+    """The serving mix: jobs of log-uniform size in [lo, hi] bases, each from
+    the config-2 (short reads of a genome, 30x) or config-3 (long reads, 20x,
+    HPC) generator at random, k in {25, 31}, Poisson arrivals at each load
+    (a fraction of the capacity measured by a burst of calib_jobs jobs).
+    Latency = job end - submission, on the server's clock; reads are
+    generated on the device when a job starts, inside its latency."""
+    import threading
+    rng = np.random.default_rng(seed)
+
+    def draw(n):
+        sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), n)).astype(np.int64)
+        return list(zip(sizes.tolist(), rng.choice([2, 3], n).tolist(), rng.choice([25, 31], n).tolist()))
+
+    def prm_for(gen, k):
+        return G.params(k, 15, 256, True) if gen == 3 else G.params(k, 11, 256)
+
+    out = {"generators": "config-2 short reads 30x (p=11) / config-3 long reads 20x HPC (p=15)",
+           "sizes_bases": [lo, hi], "k": [25, 31], "slots": max_running}
+    with G.Server(device, max_running=max_running) as srv:
+        def collect(ids, infos):
+            for j in ids:
+                infos.append(srv.wait(j))
+                srv.release(j)
+
+        cal = draw(calib_jobs)
+        t0 = time.perf_counter()
+        ids = [srv.submit_synth(prm_for(g, k), g, seed * 7919 + i, sz) for i, (sz, g, k) in enumerate(cal)]
+        infos = []
+        collect(ids, infos)
+        wall = time.perf_counter() - t0
+        cap = sum(int(i.n_bases) for i in infos) / wall
+        out["capacity_bases_per_s"] = cap
+        out["loads"] = {}
+        for li, load in enumerate(loads):
+            jobs = draw(n_jobs)
+            mean_bases = float(np.mean([sz for sz, _, _ in jobs]))
+            rate = load * cap / mean_bases
+            gaps = rng.exponential(1.0 / rate, n_jobs)
+            ids, infos = [], []
+            lock = threading.Lock()
+            done = threading.Event()
+
+            def collector():
+                k = 0
+                while True:
+                    with lock:
+                        j = ids[k] if k < len(ids) else None
+                    if j is None:
+                        if done.is_set() and k >= len(ids):
+                            return
+                        time.sleep(0.001)
+                        continue
+                    infos.append(srv.wait(j))
+                    srv.release(j)
+                    k += 1
+
+            th = threading.Thread(target=collector)
+            th.start()
+            start, t = time.perf_counter(), 0.0
+            for i, ((sz, g, k), gap) in enumerate(zip(jobs, gaps)):
+                t += gap
+                dt = start + t - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                jid = srv.submit_synth(prm_for(g, k), g, seed * 100003 + li * 10007 + i, sz)
+                with lock:
+                    ids.append(jid)
+            done.set()
+            th.join()
+            ok = [i for i in infos if i.state == 2]
+            lat = np.array([i.end_s - i.submit_s for i in ok])
+            span = max(i.end_s for i in ok) - min(i.submit_s for i in ok)
+            out["loads"][f"{load:.2f}"] = {
+                "jobs": n_jobs, "failed": n_jobs - len(ok),
+                "failed_status": sorted({int(i.status) for i in infos if i.state != 2}),
+                "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+                "mean_latency_s": float(lat.mean()),
+                "kmers_per_s": sum(int(i.n_kmers) for i in ok) / span,
+                "bases_per_s": sum(int(i.n_bases) for i in ok) / span,
+                "offered_bases_per_s": load * cap, "span_s": span}
+    return out
+
+
+def run_serve(args):
+    import torch
+    import gkc_b200 as G
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    n = args.serve_jobs or 1000
+    res = serve_mix(G, local, n, (0.5, 0.8, 0.95), args.seed)
+    l80 = res["loads"]["0.80"]
+    print(json.dumps({
+        "metric": "served canonical k-mers counted/s at 80% load (p50/p99 job latency in serving)",
+        "value": l80["kmers_per_s"], "unit": "kmers/s", "n_gpus": 1, "steps": n, "warmup": 40,
+        "ms_per_step": 1000 * l80["mean_latency_s"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"config5-serving-mix-{n}-jobs", "loads": [0.5, 0.8, 0.95]},
+        "serving": res}))
 
 
 def wl_name(args):
@@ -422,6 +529,14 @@ def run_ours(args, wl):
             result["cpu_baseline"] = {"value": None, "unit": "kmers/s", "cores": 0, "kind": "reference",
                                       "sample": "oracle/_ref not built"}
     ctx.close()
+    # served latency: a shorter serving mix at 80% load (full mix: --serve)
+    if not args.no_serve and rank == 0 and world == 1:
+        del ctx
+        torch.cuda.empty_cache()
+        try:
+            result["serving"] = serve_mix(G, local, args.serve_jobs or 200, (0.8,), args.seed)
+        except Exception as e:  # reported, not fatal to the throughput line
+            result["serving"] = {"error": str(e)}
     if rank == 0:
         print(json.dumps(result))
     if dist:
@@ -434,6 +549,8 @@ def main():
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, wl)
+    elif args.serve:
+        run_serve(args)
     else:
         run_ours(args, wl)
 

@@ -86,16 +86,65 @@ gkc_status ctx_cuda(gkc_ctx *c, cudaError_t e, const char *what) {
     if (_e != cudaSuccess) return ctx_cuda((c), _e, "kernel launch"); \
   } while (0)
 
+// Workspaces come from one stream-ordered memory pool per device, owned by
+// the library: allocations and frees are ordered on the context's stream and
+// do not synchronise the device, and freed blocks stay cached in the pool for
+// the next request (from any context) until a context is destroyed or its
+// workspace released through the public call, which trims the pool.
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pool[64];
+
+static cudaMemPool_t device_pool(int dev, cudaError_t *err) {
+  *err = cudaSuccess;
+  if (dev < 0 || dev >= 64) {
+    *err = cudaErrorInvalidDevice;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    *err = cudaMemPoolCreate(&pool, &props);
+    if (*err != cudaSuccess) return nullptr;
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pool[dev] = pool;
+  }
+  return g_pool[dev];
+}
+
+static void trim_pool(int dev) {
+  cudaError_t e;
+  cudaMemPool_t pool = device_pool(dev, &e);
+  if (pool) cudaMemPoolTrimTo(pool, 0);
+}
+
+// A buffer from the device pool outside any context (ordered on st).
+cudaError_t result_alloc(int dev, void **p, size_t bytes, cudaStream_t st) {
+  cudaError_t e;
+  cudaMemPool_t pool = device_pool(dev, &e);
+  if (!pool) return e;
+  return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
 void *ws_get(gkc_ctx *c, const char *name, size_t bytes, gkc_status *st) {
   *st = GKC_OK;
   if (bytes == 0) bytes = 16;
   bytes = (bytes + 255) & ~(size_t)255;
   auto it = c->bufs.find(name);
   if (it != c->bufs.end() && it->second.bytes >= bytes) return it->second.p;
+  if (c->capturing) {  // the capture pass repeats the sizing pass: nothing may grow
+    *st = ctx_fail(c, GKC_ERR_INTERNAL, std::string("workspace '") + name + "' grew during capture");
+    return nullptr;
+  }
   size_t old = 0;
   if (it != c->bufs.end()) {
     old = it->second.bytes;
-    cudaFree(it->second.p);
+    cudaFreeAsync(it->second.p, c->st);
     c->used -= old;
     c->bufs.erase(it);
     c->graph_valid = false;
@@ -107,16 +156,33 @@ void *ws_get(gkc_ctx *c, const char *name, size_t bytes, gkc_status *st) {
                                           std::to_string(bytes) + " bytes beyond the HBM budget");
     return nullptr;
   }
+  cudaError_t e;
+  cudaMemPool_t pool = device_pool(c->dev, &e);
   void *p = nullptr;
-  cudaError_t e = cudaMalloc(&p, want);
+  if (pool) e = cudaMallocFromPoolAsync(&p, want, pool, c->st);
   if (e != cudaSuccess) {
-    *st = ctx_cuda(c, e, (std::string("cudaMalloc ") + name).c_str());
+    *st = ctx_cuda(c, e, (std::string("allocating ") + name).c_str());
     return nullptr;
   }
   c->used += want;
   c->bufs[name] = DevBuf{p, want};
   c->graph_valid = false;
   return p;
+}
+
+// Frees every workspace of c into the pool (ordered on c's stream).
+void ws_release_all(gkc_ctx *c) {
+  cudaStreamSynchronize(c->st);
+  if (c->gexec) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  for (auto &kv : c->bufs) cudaFreeAsync(kv.second.p, c->st);
+  cudaStreamSynchronize(c->st);
+  c->bufs.clear();
+  c->used = 0;
+  c->graph_valid = false;
+  c->have_part = c->have_count = false;
 }
 
 #define WS(ptr, type, name, count)                                      \
@@ -165,8 +231,8 @@ void gkc_ctx_destroy(gkc_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
-  if (c->gexec) cudaGraphExecDestroy(c->gexec);
-  for (auto &kv : c->bufs) cudaFree(kv.second.p);
+  ws_release_all(c);
+  trim_pool(c->dev);
   for (int i = 0; i < 4; i++)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   for (int i = 0; i <= GKC_MAX_STAGES; i++)
@@ -200,16 +266,8 @@ uint64_t gkc_ctx_device_bytes(const gkc_ctx *c) { return c ? c->used : 0; }
 gkc_status gkc_ctx_release_workspace(gkc_ctx *c) {
   if (!c) return GKC_ERR_INVALID_ARG;
   cudaSetDevice(c->dev);
-  cudaStreamSynchronize(c->st);
-  if (c->gexec) {
-    cudaGraphExecDestroy(c->gexec);
-    c->gexec = nullptr;
-  }
-  for (auto &kv : c->bufs) cudaFree(kv.second.p);
-  c->bufs.clear();
-  c->used = 0;
-  c->graph_valid = false;
-  c->have_part = c->have_count = false;
+  ws_release_all(c);
+  trim_pool(c->dev);
   return GKC_OK;
 }
 
@@ -736,6 +794,10 @@ static gkc_status pipeline_batched(gkc_ctx *c, const gkc_params *prm, const char
       if (s == GKC_OK) s = read_totals(c, true, (uint32_t)prm->nbins);
       if (s != GKC_OK) return s;
       CK(cudaStreamSynchronize(c->st));
+      if (c->one_shot && !(c->h_tot->err & (ERR_CAPACITY | ERR_OVERSIZE_SCRATCH))) {
+        c->tm.graph_replayed = 0;
+        break;
+      }
       if (!(c->h_tot->err & (ERR_CAPACITY | ERR_OVERSIZE_SCRATCH))) {
         // capture the same sequence into a graph for later replays
         c->graph_valid = true;

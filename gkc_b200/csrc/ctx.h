@@ -60,6 +60,7 @@ struct gkc_ctx {
   gkc_count_view cv{};
   uint64_t count_keys_cap = 0;
   bool scratch_full = false;  // oversized buckets needed a full-size sort scratch
+  bool one_shot = false;      // inputs are not run again: no graph capture
   // graph of the batched pipeline
   bool graph_valid = false;
   GraphKey gkey{};
@@ -72,6 +73,8 @@ struct gkc_ctx {
 gkc_status ctx_fail(gkc_ctx *c, gkc_status s, const std::string &msg);
 gkc_status ctx_cuda(gkc_ctx *c, cudaError_t e, const char *what);
 void *ws_get(gkc_ctx *c, const char *name, size_t bytes, gkc_status *st);
+void ws_release_all(gkc_ctx *c);
+cudaError_t result_alloc(int dev, void **p, size_t bytes, cudaStream_t st);  // from the device pool  // workspaces back to the device pool, which keeps them
 gkc_status partition_plain_impl(gkc_ctx *c, const gkc_params *prm, const char *d_reads,
                                 uint64_t n_bytes, const uint64_t *d_offs, uint64_t n_reads);
 gkc_status count_plain_impl(gkc_ctx *c, const gkc_params *prm);

@@ -8,16 +8,22 @@
 // has left; the slot's context is capped at that amount for the job.  The
 // queue is served in arrival order, except that up to kMaxBypass later jobs
 // that fit may start ahead of a head job that does not; after that the head
-// waits alone until memory frees up.  When nothing fits, idle slots give
-// their resident workspaces back.  Results are copied to host memory when a
-// job finishes, so a slot can take the next job at once.
+// waits alone until memory frees up.  A finished job's workspaces go back to
+// the library's device memory pool, which keeps them for the next job of any
+// slot (no allocation or free synchronises the device).  A finished job's
+// result stays in device memory (copied out of the slot's workspaces, so the
+// slot can take the next job at once) and counts against the budget until
+// the job is released; gkc_server_copy_result copies it to host buffers.
 //
 // The reference has no serving layer; its driver counts one batch of reads at
 // a time (process_reads_count, experiment.cpp:76-89).
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -45,8 +51,10 @@ struct Job {
   bool cancel = false;
   int bypassed = 0;
   gkc_job_info info{};
-  std::vector<uint64_t> bin_off, keys;
-  std::vector<uint32_t> counts;
+  // the result, in device memory from the library's pool until released:
+  // bin offsets (nbins+1), keys (n_distinct * key_words), counts (n_distinct)
+  void *d_res = nullptr;
+  uint64_t res_bytes = 0;
 };
 
 struct Slot {
@@ -81,6 +89,7 @@ struct gkc_server {
   int ready = 0;
   gkc_status init_status = GKC_OK;
   uint64_t next_id = 1, committed = 0;
+  uint64_t held = 0;  // device bytes of finished jobs' results (in `committed`)
   bool stop = false;
   Clock::time_point t0 = Clock::now();
 
@@ -107,15 +116,6 @@ struct gkc_server {
     return nullptr;
   }
 
-  // Gives back the resident workspaces of idle slots (lock held).
-  void release_idle() {
-    for (Slot &s : slots) {
-      if (s.busy || !s.ctx || s.charged == 0) continue;
-      gkc_ctx_release_workspace(s.ctx);
-      committed -= s.charged;
-      s.charged = 0;
-    }
-  }
 
   bool any_busy() const {
     for (const Slot &s : slots)
@@ -135,12 +135,13 @@ struct gkc_server {
   }
 
   void worker(int i);
-  gkc_status run(gkc_ctx *c, Job *j);
+  gkc_status run(gkc_ctx *c, Job *j, double *t_gen, double *t_pipe);
 };
 
-gkc_status gkc_server::run(gkc_ctx *c, Job *j) {
+gkc_status gkc_server::run(gkc_ctx *c, Job *j, double *t_gen, double *t_pipe) {
   gkc_count_view cv{};
   gkc_status s;
+  const double t0 = now();
   if (!j->synth) {
     s = gkc_pipeline_host(c, &j->prm, GKC_MODE_BATCHED, j->reads.data(), j->offs.data(), j->n_reads, &cv);
   } else {
@@ -167,22 +168,38 @@ gkc_status gkc_server::run(gkc_ctx *c, Job *j) {
     }
     cudaError_t e = cudaPeekAtLastError();
     if (e != cudaSuccess) return ctx_cuda(c, e, "synthetic reads");
+    if (t_gen) {
+      cudaStreamSynchronize(c->st);
+      *t_gen = now() - t0;
+    }
     s = gkc_pipeline_device(c, &j->prm, GKC_MODE_BATCHED, reads, nb, offs, R, nullptr, &cv);
   }
+  if (t_pipe) *t_pipe = now() - t0;
   if (s != GKC_OK) return s;
   j->info.n_kmers = cv.n_kmers;
   j->info.n_distinct = cv.n_distinct;
   j->info.nbins = cv.nbins;
   j->info.key_words = cv.key_words;
-  j->bin_off.resize(cv.nbins + 1);
-  j->keys.resize(std::max<uint64_t>(cv.n_distinct * cv.key_words, 1));
-  j->counts.resize(std::max<uint64_t>(cv.n_distinct, 1));
-  return gkc_count_copy_out(c, j->bin_off.data(), j->keys.data(), j->counts.data());
+  const uint64_t b_bo = 8 * (cv.nbins + 1), b_keys = 8 * cv.n_distinct * cv.key_words,
+                 b_cnt = 4 * cv.n_distinct;
+  j->res_bytes = (b_bo + b_keys + b_cnt + 511) & ~511ull;
+  cudaError_t e = result_alloc(c->dev, &j->d_res, j->res_bytes, c->st);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "result buffer");
+  char *r = static_cast<char *>(j->d_res);
+  e = cudaMemcpyAsync(r, cv.bin_off, b_bo, cudaMemcpyDeviceToDevice, c->st);
+  if (e == cudaSuccess && b_keys) e = cudaMemcpyAsync(r + b_bo, cv.keys, b_keys, cudaMemcpyDeviceToDevice, c->st);
+  if (e == cudaSuccess && b_cnt)
+    e = cudaMemcpyAsync(r + b_bo + b_keys, cv.counts, b_cnt, cudaMemcpyDeviceToDevice, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  if (e != cudaSuccess) return ctx_cuda(c, e, "result copy");
+  return GKC_OK;
 }
 
 void gkc_server::worker(int i) {
   gkc_ctx *c = nullptr;
   gkc_status s = gkc_ctx_create(dev, 0, &c);
+  if (s == GKC_OK) c->one_shot = true;  // every job is a new input
+  const bool debug = getenv("GKC_SERVER_DEBUG") != nullptr;
   {
     std::lock_guard<std::mutex> lk(mu);
     slots[i].ctx = c;
@@ -197,10 +214,6 @@ void gkc_server::worker(int i) {
     while (!stop) {
       fail_head_if_impossible();
       j = pick(slots[i]);
-      if (!j && !queue.empty()) {
-        release_idle();
-        j = pick(slots[i]);
-      }
       if (j) break;
       cv.notify_all();  // waiters on failed jobs
       cv.wait(lk);
@@ -212,14 +225,30 @@ void gkc_server::worker(int i) {
     j->info.hbm_bytes = slots[i].charged;
     c->budget = slots[i].charged;
     lk.unlock();
-    gkc_status st = run(c, j);
+    const double t_run = now();
+    double t_gen = 0, t_pipe = 0;
+    gkc_status st = run(c, j, debug ? &t_gen : nullptr, debug ? &t_pipe : nullptr);
+    if (debug)
+      fprintf(stderr,
+              "gkc server: job %llu slot %d bases %llu k %d hpc %d status %d (%s) run %.3f s gen %.3f pipe %.3f "
+              "distinct %llu hbm %.2f GB\n",
+              (unsigned long long)j->id, i, (unsigned long long)j->n_bases, j->prm.k, j->prm.hpc, (int)st,
+              st == GKC_OK ? "" : gkc_ctx_last_error(c), now() - t_run, t_gen, t_pipe,
+              (unsigned long long)j->info.n_distinct, slots[i].charged / 1e9);
     lk.lock();
     j->reads.clear();
     j->reads.shrink_to_fit();
+    ws_release_all(c);  // the memory stays in the device pool for the next job
+    if (st != GKC_OK || j->cancel) {
+      if (j->d_res) cudaFreeAsync(j->d_res, c->st);
+      j->d_res = nullptr;
+      j->res_bytes = 0;
+    }
+    held += j->res_bytes;
+    committed += j->res_bytes;
     j->info.end_s = now();
     j->info.status = st;
     j->info.state = j->cancel ? GKC_JOB_CANCELLED : (st == GKC_OK ? GKC_JOB_DONE : GKC_JOB_FAILED);
-    if (st != GKC_OK) gkc_ctx_release_workspace(c);  // leave no half-sized buffers behind
     const uint64_t resident = gkc_ctx_device_bytes(c);
     committed = committed - slots[i].charged + resident;
     slots[i].charged = resident;
@@ -277,7 +306,12 @@ void gkc_server_destroy(gkc_server *S) {
   }
   S->cv.notify_all();
   for (auto &t : S->workers) t.join();
-  for (auto &kv : S->jobs) delete kv.second;
+  cudaSetDevice(S->dev);
+  for (auto &kv : S->jobs) {
+    if (kv.second->d_res) cudaFreeAsync(kv.second->d_res, 0);
+    delete kv.second;
+  }
+  cudaDeviceSynchronize();
   delete S;
 }
 
@@ -395,10 +429,18 @@ gkc_status gkc_server_copy_result(gkc_server *S, uint64_t id, uint64_t *bin_off,
   if (it == S->jobs.end()) return GKC_ERR_NOT_FOUND;
   Job *j = it->second;
   if (j->info.state != GKC_JOB_DONE) return j->info.state == GKC_JOB_FAILED ? j->info.status : GKC_ERR_NOT_READY;
-  const uint64_t nd = j->info.n_distinct;
-  if (bin_off) std::copy(j->bin_off.begin(), j->bin_off.end(), bin_off);
-  if (keys) std::copy(j->keys.begin(), j->keys.begin() + nd * j->info.key_words, keys);
-  if (counts) std::copy(j->counts.begin(), j->counts.begin() + nd, counts);
+  const uint64_t b_bo = 8 * (j->info.nbins + 1), b_keys = 8 * j->info.n_distinct * j->info.key_words,
+                 b_cnt = 4 * j->info.n_distinct;
+  const char *r = static_cast<const char *>(j->d_res);
+  cudaSetDevice(S->dev);
+  cudaError_t e = cudaSuccess;
+  if (bin_off) e = cudaMemcpy(bin_off, r, b_bo, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && keys && b_keys) e = cudaMemcpy(keys, r + b_bo, b_keys, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && counts && b_cnt) e = cudaMemcpy(counts, r + b_bo + b_keys, b_cnt, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return GKC_ERR_CUDA;
+  }
   return GKC_OK;
 }
 
@@ -409,6 +451,13 @@ gkc_status gkc_server_release(gkc_server *S, uint64_t id) {
   if (it == S->jobs.end()) return GKC_ERR_NOT_FOUND;
   Job *j = it->second;
   if (!gkc_server::finished(j)) return GKC_ERR_NOT_READY;  // cancel it first
+  if (j->d_res) {
+    cudaSetDevice(S->dev);
+    cudaFreeAsync(j->d_res, 0);
+    S->held -= j->res_bytes;
+    S->committed -= j->res_bytes;
+    S->cv.notify_all();
+  }
   delete j;
   S->jobs.erase(it);
   return GKC_OK;
