@@ -670,7 +670,7 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
     unsigned long long h[16];
     cudaMemcpyAsync(h, sa.prof, sizeof(h), cudaMemcpyDeviceToHost, c->st);
     cudaStreamSynchronize(c->st);
-    fprintf(stderr, "coarse_count profile: fallback slices=%llu\n", h[5]);
+    fprintf(stderr, "coarse_count profile: fallback slices=%llu split slices=%llu\n", h[5], h[6]);
   }
   scan_u64_dev(cd, cout_, max_buckets, bucket_base + nbins, stmp, c->st);
   WS(counts, uint32_t, "counts", keys_cap);

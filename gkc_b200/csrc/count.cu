@@ -233,6 +233,7 @@ constexpr int CC_NSUB = 1 << CC_SUB_BITS;
 constexpr int SL_PROBE_LIMIT = 256;
 constexpr int SL_CLUSTER_LIMIT = 512;
 constexpr int SL_LOW_BITS = 20;
+constexpr int kSliceStack = 32;  // > 2 * log2(CC_NSUB) + 1: splits halve a slice's keys
 
 template <typename K>
 struct CoarseSmem {
@@ -251,6 +252,8 @@ struct CoarseSmem {
   uint64_t g, start, n, run;
   uint32_t b, nsl, cursor;
   int overflow;
+  int sp;                    // slice stack: (first << 16) | end sub-bucket
+  uint32_t stk[kSliceStack];
 };
 
 template <typename K> size_t coarse_smem_bytes() { return sizeof(CoarseSmem<K>); }
@@ -499,8 +502,22 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
     }
     const uint32_t nsl = S.nsl;
     for (uint32_t sl = 0; sl < nsl; sl++) {
-      const uint32_t j_lo = S.slo[sl];
-      const uint32_t j_hi = (sl + 1 < nsl) ? S.slo[sl + 1] : nsub;
+      // A slice that overflows the table is split at its key midpoint and the
+      // halves retried, the left one first (a stack), so that the output
+      // stays in key order; only a single sub-bucket falls back to sorting.
+      if (tid == 0) {
+        S.stk[0] = ((uint32_t)S.slo[sl] << 16) | ((sl + 1 < nsl) ? (uint32_t)S.slo[sl + 1] : nsub);
+        S.sp = 1;
+      }
+     while (true) {
+      __syncthreads();
+      const int sp = S.sp;
+      if (sp == 0) break;
+      const uint32_t top = S.stk[sp - 1];
+      __syncthreads();  // every thread has read the top before it is popped
+      if (tid == 0) S.sp = sp - 1;
+      const uint32_t j_lo = top >> 16;
+      const uint32_t j_hi = top & 0xFFFFu;
       const uint32_t base_cnt = S.sub[j_lo];
       const uint32_t ns = S.sub[j_hi] - base_cnt;
       if (ns == 0) continue;
@@ -594,6 +611,21 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
         __syncthreads();
         continue;
       }
+      if (j_hi - j_lo > 1 && sp + 1 <= kSliceStack) {
+        if (tid == 0) {  // split: smallest mid in [j_lo+1, j_hi-1] with half the keys before it
+          const uint32_t half = base_cnt + ns / 2;
+          uint32_t lo = j_lo + 1, hi = j_hi - 1;
+          while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (S.sub[mid] >= half) hi = mid; else lo = mid + 1;
+          }
+          S.stk[sp - 1] = (lo << 16) | j_hi;  // the popped entry's place, then one more
+          S.stk[sp] = (j_lo << 16) | lo;
+          S.sp = sp + 1;
+          if (a.prof) atomicAdd(a.prof + 6, 1ull);
+        }
+        continue;
+      }
       // ---- fallback: gather the slice's keys and sort them ----
       if (tid == 0 && a.prof) atomicAdd(a.prof + 5, 1ull);
       const uint32_t fh = j_hi - 1;
@@ -649,6 +681,7 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
         if (tid == 0) atomicExch(a.scratch_lock, 0ull);
       }
       __syncthreads();
+     }
     }
     if (tid == 0) {
       a.coarse_start[g] = start;
