@@ -37,6 +37,9 @@ WORKLOADS = {
                     hpc=0),
     "config4": dict(gen="genome", genome_len=100_000_000, coverage=30, read_len=250, err=0.005,
                     k=63, p=13, nbins=256, hpc=0),
+    # long reads: lognormal lengths (median 8 kbp, sigma 0.5, clipped to 1-50 kbp), 20x
+    "config3": dict(gen="long", genome_len=100_000_000, coverage=20, median=8000.0, sigma=0.5,
+                    min_len=1000, max_len=50000, k=25, p=15, nbins=256, hpc=1),
 }
 METRIC = "canonical k-mers counted/s"
 SEED = 2026
@@ -68,6 +71,26 @@ def parse():
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), \
         int(os.environ.get("LOCAL_RANK", 0))
+
+
+def max_over_ranks(value, dist, device):
+    """The largest value over all ranks (the job's time is its slowest rank)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_first_read(wl, rank):
+    """Weak scaling: rank r samples reads [r * n, (r + 1) * n) of the same genome."""
+    return rank * (wl["coverage"] * wl["genome_len"] // wl["read_len"])
+
+
+def whole_job_rate(units_per_rank, world, steps, max_ms):
+    """Units all ranks processed in the timed steps over the slowest rank's time."""
+    return units_per_rank * world * steps / (max_ms / 1000.0)
 
 
 def peaks():
@@ -159,18 +182,45 @@ def make_workload_device(wl, seed, rank, torch, G):
     Gl = wl["genome_len"]
     genome = torch.empty(Gl, dtype=torch.uint8, device=dev)
     assert L.gkc_synth_genome(1, seed, Gl, 0.05, 0.01, genome.data_ptr()) == 0
+    if wl["gen"] == "long":
+        offs_h = long_read_offsets(wl, seed + rank, G)
+        n = len(offs_h) - 1
+        nb = int(offs_h[-1])
+        reads = torch.empty(nb + 64, dtype=torch.uint8, device=dev)
+        offs = torch.from_numpy(offs_h.view(np.int64)).to(dev)
+        assert L.gkc_synth_long_reads(1, seed + rank, genome.data_ptr(), Gl, n, offs.data_ptr(),
+                                      reads.data_ptr()) == 0
+        return reads, offs, n, nb, genome
     n = wl["coverage"] * Gl // wl["read_len"]
     reads = torch.empty(n * wl["read_len"] + 64, dtype=torch.uint8, device=dev)
     offs = torch.empty(n + 1, dtype=torch.int64, device=dev)
     # each rank samples its own reads of the same genome (weak scaling)
-    assert L.gkc_synth_short_reads(1, seed, genome.data_ptr(), Gl, rank * n, n, wl["read_len"],
+    assert L.gkc_synth_short_reads(1, seed, genome.data_ptr(), Gl, rank_first_read(wl, rank), n, wl["read_len"],
                                    wl["err"], reads.data_ptr(), offs.data_ptr()) == 0
     return reads, offs, n, n * wl["read_len"], genome
+
+
+def long_read_offsets(wl, seed, G, total=None):
+    total = total or wl["genome_len"] * wl["coverage"]
+    maxr = total // wl["min_len"] + 2
+    offs = np.zeros(maxr + 1, np.uint64)
+    n = G.lib().gkc_synth_long_read_offsets(seed, wl["median"], wl["sigma"], wl["min_len"], wl["max_len"],
+                                            total, maxr, offs.ctypes.data)
+    return offs[:n + 1].copy()
 
 
 def host_sample(wl, seed, n_reads, genome_host=None):
     """The first n_reads reads of the workload, generated on the host."""
     from gkc_b200 import synth
+    if wl["gen"] == "long":
+        import gkc_b200 as G
+        g = genome_host if genome_host is not None else synth.genome(seed, wl["genome_len"])
+        g = np.ascontiguousarray(g, np.uint8)
+        offs = long_read_offsets(wl, seed, G)[:n_reads + 1]
+        out = np.zeros(int(offs[-1]) + 64, np.uint8)
+        assert G.lib().gkc_synth_long_reads(0, seed, g.ctypes.data, len(g), len(offs) - 1,
+                                            offs.ctypes.data, out.ctypes.data) == 0
+        return out[:int(offs[-1])], offs
     if wl["gen"] == "iid":
         return synth.iid_reads(seed, min(n_reads, wl["n_reads"]), wl["read_len"], wl["n_rate"])
     g = genome_host if genome_host is not None else synth.genome(seed, wl["genome_len"])
@@ -199,7 +249,7 @@ def run_reference(args, wl):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference tree absent at build time)"}))
         return
     threads = os.cpu_count() or 1
-    n = args.cpu_sample_reads if wl["gen"] != "iid" else wl["n_reads"]
+    n = sample_reads(args, wl)
     reads, offs = host_sample(wl, args.seed, n)
     for _ in range(args.warmup):
         cpu_reference_rate(reads, offs, wl, threads)
@@ -328,7 +378,17 @@ def run_serve(args):
 
 def wl_name(args):
     return {"ns": "ns-100Mbp-30x-150bp-k31", "config2": "config2-10Mbp-30x-150bp-k31",
-            "config1": "config1-iid-20000x150bp-k31", "config4": "config4-100Mbp-30x-250bp-k63"}[args.workload]
+            "config1": "config1-iid-20000x150bp-k31", "config4": "config4-100Mbp-30x-250bp-k63",
+            "config3": "config3-100Mbp-20x-long-hpc-k25"}[args.workload]
+
+
+def sample_reads(args, wl):
+    """Reads in the bounded CPU-baseline sample (about 30 M bases of long reads)."""
+    if wl["gen"] == "iid":
+        return wl["n_reads"]
+    if wl["gen"] == "long":
+        return max(100, int(30e6 // wl["median"]))
+    return args.cpu_sample_reads
 
 
 def config_dict(args, wl, n_reads, n_bases):
@@ -339,6 +399,10 @@ def config_dict(args, wl, n_reads, n_bases):
     if wl["gen"] == "genome":
         d.update(genome_bp=wl["genome_len"], coverage=wl["coverage"], read_len=wl["read_len"],
                  error_rate=wl["err"])
+    if wl["gen"] == "long":
+        d.update(genome_bp=wl["genome_len"], coverage=wl["coverage"],
+                 read_len=f"lognormal median {wl['median']:.0f} sigma {wl['sigma']} clipped {wl['min_len']}-{wl['max_len']}",
+                 errors="5%: 40% substitution, 30% insertion, 30% deletion (indels likelier in homopolymers)")
     return d
 
 
@@ -392,17 +456,13 @@ def run_ours(args, wl):
                 stage_acc.setdefault(name, []).append(ms)
         e1.record(stream)
         barrier()
-    ms_total = e0.elapsed_time(e1)
-    if dist:
-        tt = torch.tensor([ms_total], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_total = float(tt.item())
+    ms_total = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     clocks = clk.summary()
 
     N, D, S = int(cv.n_kmers), int(cv.n_distinct), int(pv.n_superkmers)
     B, R = int(pv.n_bases), int(pv.n_reads)
     ms_step = ms_total / args.steps
-    value = N * world * args.steps / (ms_total / 1000.0)
+    value = whole_job_rate(N, world, args.steps, ms_total)
     stages = {k: float(np.mean(v)) for k, v in stage_acc.items()}
     model = algorithmic_bytes(B, R, S, N, D, wl["k"])
     peak, peak_kind = peaks()
@@ -501,13 +561,9 @@ def run_ours(args, wl):
             c = e2e_step()
         ee1.record(stream)
         barrier()
-        e_ms = ee0.elapsed_time(ee1)
-        if dist:
-            tt = torch.tensor([e_ms], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e_ms = float(tt.item())
+        e_ms = max_over_ranks(ee0.elapsed_time(ee1), dist, "cuda")
         nd = int(c.n_distinct)
-        result["e2e"] = {"value": N * world * args.e2e_steps / (e_ms / 1000.0), "unit": "kmers/s",
+        result["e2e"] = {"value": whole_job_rate(N, world, args.e2e_steps, e_ms), "unit": "kmers/s",
                          "h2d_bytes_per_step": n_bases + (n_reads + 1) * 8,
                          "d2h_bytes_per_step": (wl["nbins"] + 1) * 8 + nd * 8 * kw + nd * 4,
                          "ms_per_step": e_ms / args.e2e_steps, "steps": args.e2e_steps,
@@ -518,7 +574,7 @@ def run_ours(args, wl):
         import oracle_ffi as F
         if F.ref_available():
             threads = os.cpu_count() or 1
-            n = args.cpu_sample_reads if wl["gen"] != "iid" else wl["n_reads"]
+            n = sample_reads(args, wl)
             gh = genome.cpu().numpy() if genome is not None else None
             sr, so = host_sample(wl, args.seed, n, gh)
             rate, dt, km, _ = cpu_reference_rate(sr, so, wl, threads)

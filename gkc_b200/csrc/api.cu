@@ -215,6 +215,19 @@ gkc_status gkc_ctx_create(int device_id, uint64_t hbm_budget_bytes, gkc_ctx **ou
   cudaGetDeviceProperties(&prop, device_id);
   c->n_sms = prop.multiProcessorCount;
   c->max_smem_optin = (int)prop.sharedMemPerBlockOptin;
+  // The dynamic shared-memory limit of a kernel is process-wide: set it to
+  // the device maximum once, here, and never per launch, where one thread
+  // could lower it between another thread's setting and launch.
+  if (cudaFuncSetAttribute(k_partition, cudaFuncAttributeMaxDynamicSharedMemorySize, c->max_smem_optin) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_coarse_count<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           c->max_smem_optin) != cudaSuccess ||
+      cudaFuncSetAttribute(k_coarse_count<u128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           c->max_smem_optin) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return GKC_ERR_CUDA;
+  }
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMallocHost(&c->h_tot, sizeof(DevTotals)) != cudaSuccess) {
     delete c;
@@ -416,7 +429,7 @@ static gkc_status enqueue_partition(gkc_ctx *c, const gkc_params *prm, const cha
   a.bin_nkmers = bin_nkm;
   a.err = err;
   size_t smem = partition_smem_bytes(a.nbins_smem);
-  CK(cudaFuncSetAttribute(k_partition, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if ((int)smem > c->max_smem_optin) return ctx_fail(c, GKC_ERR_INVALID_ARG, "too many bins for shared memory");
   int occ = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_partition, kPartThreads, smem));
   uint64_t tiles = (n_bytes + kPartTile - 1) / kPartTile;
@@ -661,7 +674,7 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
     sa.prof = prof;
   }
   const size_t smem = coarse_smem_bytes<K>();
-  CK(cudaFuncSetAttribute(k_coarse_count<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if ((int)smem > c->max_smem_optin) return ctx_fail(c, GKC_ERR_INTERNAL, "count tables exceed shared memory");
   stage_mark(c, 5);
   k_coarse_count<K><<<c->n_sms, kSortThreads, smem, c->st>>>(sa);
   LAUNCHED(c);

@@ -234,6 +234,10 @@ constexpr int SL_PROBE_LIMIT = 256;
 constexpr int SL_CLUSTER_LIMIT = 512;
 constexpr int SL_LOW_BITS = 20;
 constexpr int kSliceStack = 32;  // > 2 * log2(CC_NSUB) + 1: splits halve a slice's keys
+// clusters longer than CW_MIN slots are sorted by a warp (up to CW_LIST a slice)
+constexpr int CW_MIN = 16;
+constexpr int CW_LIST = 128;
+static_assert(SL_CLUSTER_LIMIT < 1024, "cluster lengths are packed in 10 bits");
 
 template <typename K>
 struct CoarseSmem {
@@ -245,7 +249,7 @@ struct CoarseSmem {
     } t;
     SortSmem<K> s;  // fallback sort layout
   } u;
-  uint32_t sub[CC_NSUB + 1];        // sub-bucket counts, then exclusive starts
+  uint32_t sub[CC_NSUB + 2];        // sub-bucket counts, then first placed keys
   uint32_t slot_base[CC_NSUB + 1];
   uint16_t slo[CC_NSUB + 1];        // first sub-bucket of each slice
   uint32_t tmp[64];
@@ -254,6 +258,10 @@ struct CoarseSmem {
   int overflow;
   int sp;                    // slice stack: (first << 16) | end sub-bucket
   uint32_t stk[kSliceStack];
+  uint64_t tot_n, tot_d;     // keys and distinct keys of this CTA's slices so far
+  int sort_mode;
+  uint32_t nbig;             // long clusters: (first slot << 10) | length
+  uint32_t bigl[CW_LIST];
 };
 
 template <typename K> size_t coarse_smem_bytes() { return sizeof(CoarseSmem<K>); }
@@ -435,6 +443,47 @@ GKC_DEV void scratch_sort(SortSmem<K> &S, const SortCountArgs &a, uint64_t n, in
   }
 }
 
+// In-place ascending sort of m (key, count) pairs by one warp: a bitonic
+// network in the form where every comparator puts the smaller key at the
+// lower index, so positions >= m act as +infinity.
+template <typename K>
+GKC_DEV void warp_sort_pairs(K *key, uint32_t *cnt, uint32_t m) {
+  uint32_t P = 1;
+  while (P < m) P <<= 1;
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t size = 2; size <= P; size <<= 1) {
+    const uint32_t half = size >> 1;
+    for (uint32_t i = lane; i < P / 2; i += 32) {
+      const uint32_t blk = i / half, off = i % half;
+      const uint32_t lo = blk * size + off, hi = blk * size + size - 1 - off;
+      if (hi < m && key[hi] < key[lo]) {
+        const K x = key[lo];
+        key[lo] = key[hi];
+        key[hi] = x;
+        const uint32_t c = cnt[lo];
+        cnt[lo] = cnt[hi];
+        cnt[hi] = c;
+      }
+    }
+    __syncwarp();
+    for (uint32_t stride = size >> 2; stride >= 1; stride >>= 1) {
+      for (uint32_t i = lane; i < P / 2; i += 32) {
+        const uint32_t blk = i / stride, off = i % stride;
+        const uint32_t lo = blk * 2 * stride + off, hi = lo + stride;
+        if (hi < m && key[hi] < key[lo]) {
+          const K x = key[lo];
+          key[lo] = key[hi];
+          key[hi] = x;
+          const uint32_t c = cnt[lo];
+          cnt[lo] = cnt[hi];
+          cnt[hi] = c;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
 template <typename K>
 __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
@@ -446,7 +495,10 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
   const int tid = threadIdx.x;
   if (*a.err & (ERR_CAPACITY | ERR_BAD_READ)) return;  // keys incomplete: the host re-runs
   const uint64_t n_buckets = a.bucket_base[a.nbins];
-  const uint32_t target = SliceTab<K>::TS / 2;
+  if (tid == 0) {
+    S.tot_n = 0;
+    S.tot_d = 0;
+  }
   while (true) {
     if (tid == 0) {
       S.g = atomicAdd(a.ticket, 1ull);
@@ -460,8 +512,14 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
         S.n = a.chunk_off[hb + (d + 1) * nch] - S.start;
       }
       S.run = 0;
+      // Mostly distinct keys gain little from the table (and near-equal ones
+      // make long probe chains): when this CTA's slices so far were more
+      // than 55% distinct, the bucket's slices are sorted directly instead.
+      S.sort_mode = S.tot_n > 0 && S.tot_d * 20 > S.tot_n * 11;
     }
     __syncthreads();
+    const bool sort_mode = S.sort_mode;
+    const uint32_t target = sort_mode ? (uint32_t)SortCap<K>::value : (uint32_t)(SliceTab<K>::TS / 2);
     const uint64_t g = S.g;
     if (g >= n_buckets) break;
     const uint64_t start = S.start, n = S.n;
@@ -477,14 +535,46 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
       __syncthreads();
       continue;
     }
-    // sub-histogram of the next SB bits
+    // Sub-bucket counts at sub[1 + j]; their exclusive scan is the cursor of
+    // sub-bucket j while the keys are placed in sub-bucket order in the
+    // bucket's own range of tmp_keys (where they stay in L2), after which
+    // sub[j] is the first placed key of sub-bucket j.  A slice then reads only
+    // its own keys.  Its runs are written at or before its first key, after
+    // all of its keys were read, so the placed keys of later slices survive.
+    K *placed = tkeys + start;
+    if (!in_bounds(a, 11, start + n, a.tmp_cap + 1)) return;
     for (uint32_t j = tid; j <= nsub; j += SC_NT) S.sub[j] = 0;
     __syncthreads();
-    for (uint64_t i = tid; i < n; i += SC_NT)
-      atomicAdd(&S.sub[key_digit<K>(keys[start + i], key_bits, cb, SB)], 1u);
-    __syncthreads();
-    scan_counters(S.sub, nsub, S.tmp);
-    if (tid == 0) S.sub[nsub] = (uint32_t)n;
+    {
+      constexpr int U = 8;
+      for (uint64_t i0 = 0; i0 < n; i0 += (uint64_t)SC_NT * U) {
+        K xs[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const uint64_t i = i0 + (uint64_t)u * SC_NT + tid;
+          xs[u] = i < n ? keys[start + i] : (K)0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+          if (i0 + (uint64_t)u * SC_NT + tid < n) atomicAdd(&S.sub[1 + key_digit<K>(xs[u], key_bits, cb, SB)], 1u);
+      }
+      __syncthreads();
+      scan_counters(S.sub + 1, nsub, S.tmp);
+      for (uint64_t i0 = 0; i0 < n; i0 += (uint64_t)SC_NT * U) {
+        K xs[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const uint64_t i = i0 + (uint64_t)u * SC_NT + tid;
+          xs[u] = i < n ? keys[start + i] : (K)0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+          if (i0 + (uint64_t)u * SC_NT + tid < n) {
+            const uint32_t pos = atomicAdd(&S.sub[1 + key_digit<K>(xs[u], key_bits, cb, SB)], 1u);
+            if (in_bounds(a, 12, pos, n)) placed[pos] = xs[u];
+          }
+      }
+    }
     __syncthreads();
     // slices: runs of sub-buckets whose exclusive start falls in the same
     // multiple of `target` (a slice holds < target keys plus one sub-bucket)
@@ -521,22 +611,26 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
       const uint32_t base_cnt = S.sub[j_lo];
       const uint32_t ns = S.sub[j_hi] - base_cnt;
       if (ns == 0) continue;
+      if (!in_bounds(a, 13, (uint64_t)base_cnt + ns, n + 1)) continue;  // slice inside its bucket
       for (uint32_t j = j_lo + tid; j < j_hi; j += SC_NT)
         S.slot_base[j - j_lo] = (uint32_t)(((uint64_t)(S.sub[j] - base_cnt) * TS) / ns);
       if (tid == 0) {
         S.slot_base[j_hi - j_lo] = TS;
         S.overflow = 0;
+        S.nbig = 0;
       }
+      // slices of a sort-mode bucket that fit the shared-memory sort go there
+      // directly; larger ones (one heavy sub-bucket) still use the table
+      const bool direct_sort = sort_mode && ns <= (uint32_t)SortCap<K>::value;
+      if (!direct_sort) {  // aggregate in the table
       for (int s = tid; s < TSO; s += SC_NT) {
         S.u.t.key[s] = empty_key<K>();
         S.u.t.cnt[s] = 0;
       }
       __syncthreads();
-      for (uint64_t i = tid; i < n; i += SC_NT) {
-        const K x = keys[start + i];
-        const uint32_t sd = key_digit<K>(x, key_bits, cb, SB);
-        if (sd < j_lo || sd >= j_hi) continue;
-        const uint32_t j = sd - j_lo;
+      for (uint32_t i = tid; i < ns; i += SC_NT) {
+        const K x = placed[base_cnt + i];
+        const uint32_t j = key_digit<K>(x, key_bits, cb, SB) - j_lo;
         const uint32_t low = key_digit<K>(x, key_bits, cb + SB, lbits);
         const uint32_t w = S.slot_base[j + 1] - S.slot_base[j];
         int slot = (int)(S.slot_base[j] + (uint32_t)(((uint64_t)low * w) >> lbits));
@@ -579,6 +673,13 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
             set_overflow(&S.overflow);
             break;
           }
+          if (e - s > CW_MIN) {  // long: sorted by a warp below
+            const uint32_t t = atomicAdd(&S.nbig, 1u);
+            if (t < (uint32_t)CW_LIST) {
+              S.bigl[t] = ((uint32_t)s << 10) | (uint32_t)(e - s);
+              continue;
+            }
+          }
           for (int q = s + 1; q < e; q++) {  // insertion sort of (key, count)
             K x = S.u.t.key[q];
             uint32_t c = S.u.t.cnt[q];
@@ -595,6 +696,12 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
       }
       __syncthreads();
       if (!S.overflow) {
+        const uint32_t nbl = min(S.nbig, (uint32_t)CW_LIST);
+        for (uint32_t t = threadIdx.x >> 5; t < nbl; t += SC_NT / 32)
+          warp_sort_pairs<K>(S.u.t.key + (S.bigl[t] >> 10), S.u.t.cnt + (S.bigl[t] >> 10), S.bigl[t] & 1023u);
+      }
+      __syncthreads();
+      if (!S.overflow) {
         uint32_t D;
         const uint32_t pos = block_exclusive_scan<SC_NT>(occ, S.tmp, &D);
         const uint64_t base = start + S.run + pos;
@@ -607,7 +714,11 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
           o++;
         }
         __syncthreads();
-        if (tid == 0) S.run += D;
+        if (tid == 0) {
+          S.run += D;
+          S.tot_n += ns;
+          S.tot_d += D;
+        }
         __syncthreads();
         continue;
       }
@@ -626,8 +737,9 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
         }
         continue;
       }
-      // ---- fallback: gather the slice's keys and sort them ----
-      if (tid == 0 && a.prof) atomicAdd(a.prof + 5, 1ull);
+      }  // table
+      // ---- gather the slice's keys and sort them ----
+      if (tid == 0 && a.prof) atomicAdd(a.prof + (direct_sort ? 7 : 5), 1ull);
       const uint32_t fh = j_hi - 1;
       const int skip = (j_lo == fh) ? cb + SB : cb + SB - (32 - __clz(j_lo ^ fh));
       SortSmem<K> &T = S.u.s;
@@ -646,14 +758,8 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
         if (S.overflow) continue;  // wait ran out: reported through the error word
       }
       K *dst = fits ? T.A : reinterpret_cast<K *>(a.scratch);
-      for (uint64_t i = tid; i < n; i += SC_NT) {
-        const K x = keys[start + i];
-        const uint32_t sd = key_digit<K>(x, key_bits, cb, SB);
-        if (sd >= j_lo && sd < j_hi) {
-          const uint32_t w = atomicAdd(&S.cursor, 1u);
-          if (in_bounds(a, 1, w, fits ? (uint64_t)SortCap<K>::value : a.scratch_keys)) dst[w] = x;
-        }
-      }
+      for (uint32_t i = tid; i < ns; i += SC_NT) dst[i] = placed[base_cnt + i];
+      if (tid == 0) S.cursor = ns;
       __syncthreads();
       if (tid == 0) T.out = start + S.run;
       __syncthreads();
@@ -670,7 +776,11 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
         }
         write_runs<K>(T, D, tkeys, a.tmp_counts, T.out);
         __syncthreads();
-        if (tid == 0) S.run += D;
+        if (tid == 0) {
+          S.run += D;
+          S.tot_n += ns;
+          S.tot_d += D;
+        }
       } else {
         __threadfence_block();
         scratch_sort<K>(T, a, ns, skip, tkeys, a.tmp_counts);
