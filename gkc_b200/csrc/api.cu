@@ -345,6 +345,8 @@ uint64_t gkc_job_hbm_estimate(const gkc_params *prm, uint64_t n_bases, uint64_t 
   e += (B + 1) / 8 + 16;                                                 // read starts
   e += cap_skm * (8 + 4 + 8 + 4) + cap_bytes;                            // superkmers
   e += cap_skm * 16;                                                     // k-mer offsets
+  if ((uint32_t)prm->nbins <= (uint32_t)kBinPlaceMaxBins)                // bin placement matrices
+    e += 17 * ((cap_skm + kBinChunk - 1) / kBinChunk) * (uint64_t)prm->nbins;
   const uint64_t kc = std::max<uint64_t>(B, 16);
   uint32_t max_bits = kCoarseMaxBits;
   while (max_bits > 0 && ((uint64_t)prm->nbins << max_bits) > (1ull << 20)) max_bits--;
@@ -443,13 +445,29 @@ static gkc_status enqueue_partition(gkc_ctx *c, const gkc_params *prm, const cha
   WS(bin_kstart, uint64_t, "bin_kstart", nbins + 1);
   k_bin_prefix<<<1, 32, 0, c->st>>>(bin_nskm, bin_nkm, nbins, bin_start, bin_kstart);
   LAUNCHED(c);
-  WS(bfill, unsigned long long, "bin_fill", nbins + 1);
-  CK(cudaMemsetAsync(bfill, 0, (nbins + 1) * 8, c->st));
   WS(bdesc, uint64_t, "skm_desc_bin", cap_skm);
   WS(bmm, uint32_t, "skm_mm_bin", cap_skm);
-  k_bin_scatter<<<c->n_sms * 8, 256, 0, c->st>>>(tot, desc, mm, nbins, bin_start, bfill, bdesc,
-                                                 bmm, nullptr, nullptr, err);
-  LAUNCHED(c);
+  if (nbins <= (uint32_t)kBinPlaceMaxBins) {
+    // (bin, chunk) counts, one scan, then placement: no global atomics
+    const uint64_t nch_cap = (cap_skm + kBinChunk - 1) / kBinChunk;
+    const uint64_t cells = nch_cap * nbins;
+    WS(bmat, unsigned long long, "bin_chunk_cnt", cells + 1);
+    WS(boff, uint64_t, "bin_chunk_off", cells + 2);
+    WS(btmp, uint64_t, "bin_chunk_scan", scan_u64_tmp_words(cells + 1) + 8);
+    const unsigned g = (unsigned)std::min<uint64_t>(nch_cap, (uint64_t)c->n_sms * 8);
+    k_bin_count<<<g, 256, nbins * 4, c->st>>>(tot, mm, nbins, nch_cap, bmat, err);
+    LAUNCHED(c);
+    scan_u64(bmat, boff, cells, btmp, c->st);
+    c->launches += 4;
+    k_bin_place<<<g, 256, nbins * 8, c->st>>>(tot, desc, mm, nbins, nch_cap, boff, bdesc, bmm, err);
+    LAUNCHED(c);
+  } else {
+    WS(bfill, unsigned long long, "bin_fill", nbins + 1);
+    CK(cudaMemsetAsync(bfill, 0, (nbins + 1) * 8, c->st));
+    k_bin_scatter<<<c->n_sms * 8, 256, 0, c->st>>>(tot, desc, mm, nbins, bin_start, bfill, bdesc,
+                                                   bmm, nullptr, nullptr, err);
+    LAUNCHED(c);
+  }
 
   c->part_cap_skm = cap_skm;
   c->part_cap_bytes = cap_bytes;

@@ -28,6 +28,13 @@ constexpr int kPartThreads = 512;
 constexpr int kPartTile = 4096;
 size_t partition_smem_bytes(int nbins_smem);
 __global__ void k_partition(PartArgs a);
+constexpr int kBinChunk = 8192;          // superkmers per placement chunk
+constexpr int kBinPlaceMaxBins = 2048;   // larger bin counts use k_bin_scatter
+__global__ void k_bin_count(const unsigned long long *n_skm_ptr, const uint32_t *mm, uint32_t nbins,
+                            uint64_t nch_cap, unsigned long long *mat, const uint32_t *err);
+__global__ void k_bin_place(const unsigned long long *n_skm_ptr, const uint64_t *desc, const uint32_t *mm,
+                            uint32_t nbins, uint64_t nch_cap, const uint64_t *off, uint64_t *out_desc,
+                            uint32_t *out_mm, const uint32_t *err);
 __global__ void k_read_start_bits(const uint64_t *offs, uint64_t n_reads, uint32_t *bits);
 __global__ void k_bin_scatter(const unsigned long long *n_skm_ptr, const uint64_t *desc,
                               const uint32_t *mm, uint32_t nbins, const uint64_t *bin_start,

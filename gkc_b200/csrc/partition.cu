@@ -407,6 +407,49 @@ __global__ void k_bin_scatter(const unsigned long long *n_skm_ptr, const uint64_
   }
 }
 
+// Bin placement without global atomics, for nbins <= kBinPlaceMaxBins.
+// k_bin_count: superkmers per (bin, chunk of kBinChunk superkmers), stored
+// bin-major (mat[b * nch_cap + c]) so that one exclusive scan gives every
+// (bin, chunk) its first slot in bin order; k_bin_place then moves each
+// chunk's superkmers with shared-memory cursors per bin.
+__global__ void k_bin_count(const unsigned long long *n_skm_ptr, const uint32_t *mm, uint32_t nbins,
+                            uint64_t nch_cap, unsigned long long *mat, const uint32_t *err) {
+  extern __shared__ uint32_t hcnt[];
+  if (*err & (ERR_CAPACITY | ERR_BAD_READ)) return;
+  const uint64_t n = *n_skm_ptr;
+  for (uint64_t c = blockIdx.x; c < nch_cap; c += gridDim.x) {
+    for (uint32_t b = threadIdx.x; b < nbins; b += blockDim.x) hcnt[b] = 0;
+    __syncthreads();
+    const uint64_t i1 = min(n, (c + 1) * (uint64_t)kBinChunk);
+    for (uint64_t i = c * (uint64_t)kBinChunk + threadIdx.x; i < i1; i += blockDim.x)
+      atomicAdd(&hcnt[mm[i] % nbins], 1u);
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < nbins; b += blockDim.x) mat[(uint64_t)b * nch_cap + c] = hcnt[b];
+    __syncthreads();
+  }
+}
+
+__global__ void k_bin_place(const unsigned long long *n_skm_ptr, const uint64_t *desc, const uint32_t *mm,
+                            uint32_t nbins, uint64_t nch_cap, const uint64_t *off, uint64_t *out_desc,
+                            uint32_t *out_mm, const uint32_t *err) {
+  extern __shared__ unsigned long long cur[];
+  if (*err & (ERR_CAPACITY | ERR_BAD_READ)) return;
+  const uint64_t n = *n_skm_ptr;
+  const uint64_t nch = min(nch_cap, (n + kBinChunk - 1) / kBinChunk);
+  for (uint64_t c = blockIdx.x; c < nch; c += gridDim.x) {
+    for (uint32_t b = threadIdx.x; b < nbins; b += blockDim.x) cur[b] = off[(uint64_t)b * nch_cap + c];
+    __syncthreads();
+    const uint64_t i1 = min(n, (c + 1) * (uint64_t)kBinChunk);
+    for (uint64_t i = c * (uint64_t)kBinChunk + threadIdx.x; i < i1; i += blockDim.x) {
+      const uint32_t m = mm[i];
+      const uint64_t slot = atomicAdd(&cur[m % nbins], 1ull);
+      out_desc[slot] = desc[i];
+      out_mm[slot] = m;
+    }
+    __syncthreads();
+  }
+}
+
 // Exclusive scans of the per-bin counters (one thread; nbins is small).
 __global__ void k_bin_prefix(const unsigned long long *bin_nskm, const unsigned long long *bin_nkmers,
                              uint32_t nbins, uint64_t *bin_start, uint64_t *bin_kstart) {
