@@ -195,6 +195,13 @@ void ws_release_all(gkc_ctx *c) {
 
 // ------------------------------------------------------------------ context
 
+static cudaError_t set_dyn_smem_limit(const void *f, int optin) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, f);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
 gkc_status gkc_ctx_create(int device_id, uint64_t hbm_budget_bytes, gkc_ctx **out) {
   if (!out) return GKC_ERR_INVALID_ARG;
   *out = nullptr;
@@ -216,14 +223,14 @@ gkc_status gkc_ctx_create(int device_id, uint64_t hbm_budget_bytes, gkc_ctx **ou
   c->n_sms = prop.multiProcessorCount;
   c->max_smem_optin = (int)prop.sharedMemPerBlockOptin;
   // The dynamic shared-memory limit of a kernel is process-wide: set it to
-  // the device maximum once, here, and never per launch, where one thread
-  // could lower it between another thread's setting and launch.
-  if (cudaFuncSetAttribute(k_partition, cudaFuncAttributeMaxDynamicSharedMemorySize, c->max_smem_optin) !=
-          cudaSuccess ||
-      cudaFuncSetAttribute(k_coarse_count<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           c->max_smem_optin) != cudaSuccess ||
-      cudaFuncSetAttribute(k_coarse_count<u128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           c->max_smem_optin) != cudaSuccess) {
+  // the device maximum (less the kernel's static shared memory) once, here,
+  // and never per launch, where one thread could lower it between another
+  // thread's setting and launch.
+  if (set_dyn_smem_limit((const void *)k_partition, c->max_smem_optin) != cudaSuccess ||
+      set_dyn_smem_limit((const void *)k_coarse_count<uint64_t>, c->max_smem_optin) != cudaSuccess ||
+      set_dyn_smem_limit((const void *)k_coarse_count<u128>, c->max_smem_optin) != cudaSuccess ||
+      set_dyn_smem_limit((const void *)k_coarse_scatter<uint64_t>, c->max_smem_optin) != cudaSuccess ||
+      set_dyn_smem_limit((const void *)k_coarse_scatter<u128>, c->max_smem_optin) != cudaSuccess) {
     cudaGetLastError();
     delete c;
     return GKC_ERR_CUDA;
@@ -646,7 +653,9 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   scan_u64_dev(chunk_hist, chunk_off, hist_cap, hist_base + nbins, stmp4, c->st);
   c->launches += 4;
   stage_mark(c, 4);
-  k_coarse_scatter<K><<<ex_grid, 256, (1u << max_bits) * 12, c->st>>>(ea);
+  const size_t sct_smem = coarse_scatter_smem_bytes<K>(max_bits);
+  if ((int)sct_smem + 1024 > c->max_smem_optin) return ctx_fail(c, GKC_ERR_INTERNAL, "scatter stage exceeds shared memory");
+  k_coarse_scatter<K><<<c->n_sms, SCT_NT, sct_smem, c->st>>>(ea);
   LAUNCHED(c);
 
   WS(tkeys, K, "tmp_keys", keys_cap);

@@ -179,32 +179,96 @@ __global__ void __launch_bounds__(EX_NT) k_coarse_hist(ExpandArgs a) {
   }
 }
 
+// Writes every k-mer key at its (bin, coarse digit, chunk) slot.  A chunk is
+// processed in sub-chunks of SctSub<K> k-mers: expanded into shared memory
+// (with a digit histogram), permuted there into digit order, then written out
+// linearly, so that consecutive threads store consecutive keys of one digit's
+// run and global writes come in whole sectors instead of scattered words.
 template <typename K>
-__global__ void __launch_bounds__(EX_NT) k_coarse_scatter(ExpandArgs a) {
-  extern __shared__ unsigned long long sh_base[];  // 1 << max bits
-  uint32_t *rank = reinterpret_cast<uint32_t *>(sh_base + (1u << a.max_bits));
+__global__ void __launch_bounds__(SCT_NT) k_coarse_scatter(ExpandArgs a) {
+  constexpr int SUB = SctSub<K>::value;
+  extern __shared__ __align__(16) uint8_t sct_raw[];
+  K *stage = reinterpret_cast<K *>(sct_raw);
+  K *sorted = stage + SUB;
+  unsigned long long *gbase = reinterpret_cast<unsigned long long *>(sorted + SUB);
+  uint32_t *cursor = reinterpret_cast<uint32_t *>(gbase + (1u << a.max_bits));
+  uint32_t *hstart = cursor + (1u << a.max_bits);
+  __shared__ uint32_t tmp[64];
+  __shared__ uint64_t s_first, s_last;
   if (*a.err & (ERR_CAPACITY | ERR_BAD_READ)) return;
   K *keys = reinterpret_cast<K *>(a.keys);
   const uint64_t n_chunks = a.chunk_base[a.nbins];
   const int key_bits = 2 * a.k;
+  const int tid = threadIdx.x;
   for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
-    const ChunkInfo ci = chunk_info(a, c);
-    const uint32_t nd = 1u << ci.nbits;
-    const uint64_t *row = a.chunk_off + a.hist_base[ci.b] + ci.j;
-    for (uint32_t d = threadIdx.x; d < nd; d += EX_NT) {
-      sh_base[d] = row[(uint64_t)d * ci.nch];
-      rank[d] = 0;
+    const uint32_t b = find_bin(a.chunk_base, a.nbins, c);
+    const uint64_t j = c - a.chunk_base[b];
+    const uint64_t nch = a.chunk_base[b + 1] - a.chunk_base[b];
+    const uint32_t nbits = a.bin_bits[b], nd = 1u << nbits;
+    const uint64_t k0 = a.bin_kstart[b] + j * a.chunk_kmers;
+    const uint64_t k1 = min(k0 + a.chunk_kmers, a.bin_kstart[b + 1]);
+    const uint64_t s_lo = a.bin_start[b], s_hi = a.bin_start[b + 1];
+    const uint64_t *row = a.chunk_off + a.hist_base[b] + j;
+    for (uint32_t d = tid; d < nd; d += SCT_NT) gbase[d] = row[(uint64_t)d * nch];
+    for (uint64_t q0s = k0; q0s < k1; q0s += SUB) {
+      const uint64_t q1s = min(q0s + SUB, k1);
+      const uint32_t m = (uint32_t)(q1s - q0s);
+      // the superkmers holding k-mers [q0s, q1s): last with koff <= q0s, last with koff < q1s
+      if (tid < 2) {
+        const uint64_t target = tid == 0 ? q0s : q1s - 1;
+        uint64_t lo = s_lo, hi = s_hi - 1;
+        while (lo < hi) {
+          const uint64_t mid = (lo + hi + 1) >> 1;
+          if (a.koff[mid] <= target) lo = mid; else hi = mid - 1;
+        }
+        if (tid == 0) s_first = lo; else s_last = lo;
+      }
+      for (uint32_t d = tid; d < nd; d += SCT_NT) cursor[d] = 0;
+      __syncthreads();
+      // expand into the stage in k-mer order, counting digits
+      const uint32_t per = (m + SCT_NT - 1) / SCT_NT;
+      const uint32_t p0 = min(m, (uint32_t)tid * per), p1 = min(m, p0 + per);
+      uint32_t p = p0;
+      expand_range<K>(a.desc, a.koff, a.packed, s_first, s_last + 1, q0s + p0, q0s + p1, a.k, [&](K key) {
+        stage[p++] = key;
+        atomicAdd(&cursor[key_digit<K>(key, key_bits, 0, (int)nbits)], 1u);
+      });
+      __syncthreads();
+      // digit starts inside the sub-chunk (nd <= SCT_NT: one digit per thread)
+      {
+        const uint32_t v = (uint32_t)tid < nd ? cursor[tid] : 0u;
+        uint32_t total;
+        const uint32_t ex = block_exclusive_scan<SCT_NT>(v, tmp, &total);
+        if ((uint32_t)tid < nd) {
+          hstart[tid] = ex;
+          cursor[tid] = ex;
+        }
+      }
+      __syncthreads();
+      for (uint32_t i = tid; i < m; i += SCT_NT) {
+        const K x = stage[i];
+        sorted[atomicAdd(&cursor[key_digit<K>(x, key_bits, 0, (int)nbits)], 1u)] = x;
+      }
+      __syncthreads();
+      for (uint32_t i = tid; i < m; i += SCT_NT) {
+        const K x = sorted[i];
+        const uint32_t d = key_digit<K>(x, key_bits, 0, (int)nbits);
+        const uint64_t slot = gbase[d] + (i - hstart[d]);
+        if (slot < a.keys_cap) keys[slot] = x;
+        else atomicOr(a.err, ERR_CAPACITY);
+      }
+      __syncthreads();
+      for (uint32_t d = tid; d < nd; d += SCT_NT) gbase[d] += cursor[d] - hstart[d];
+      __syncthreads();
     }
-    __syncthreads();
-    expand_range<K>(a.desc, a.koff, a.packed, ci.s_lo, ci.s_hi, ci.q0, ci.q1, a.k, [&](K key) {
-      const uint32_t d = key_digit<K>(key, key_bits, 0, (int)ci.nbits);
-      const uint64_t slot = sh_base[d] + atomicAdd(&rank[d], 1u);
-      if (slot < a.keys_cap) keys[slot] = key;
-      else atomicOr(a.err, ERR_CAPACITY);
-    });
-    __syncthreads();
   }
 }
+
+template <typename K> size_t coarse_scatter_smem_bytes(uint32_t max_bits) {
+  return 2 * (size_t)SctSub<K>::value * sizeof(K) + ((size_t)1 << max_bits) * 16;
+}
+template size_t coarse_scatter_smem_bytes<uint64_t>(uint32_t);
+template size_t coarse_scatter_smem_bytes<u128>(uint32_t);
 
 // Number of k-mers of each bin-ordered superkmer (for the k-mer prefix).
 __global__ void k_skm_nk(const uint64_t *desc, const unsigned long long *n_skm_dev, int k,

@@ -84,6 +84,9 @@ struct ExpandArgs {
 };
 template <typename K> __global__ void k_coarse_hist(ExpandArgs a);
 template <typename K> __global__ void k_coarse_scatter(ExpandArgs a);
+constexpr int SCT_NT = 1024;  // k_coarse_scatter block
+template <typename K> struct SctSub { static constexpr int value = sizeof(K) == 8 ? 8192 : 4096; };
+template <typename K> size_t coarse_scatter_smem_bytes(uint32_t max_bits);
 __global__ void k_skm_nk(const uint64_t *desc, const unsigned long long *n_skm_dev, int k,
                          unsigned long long *nk);
 
