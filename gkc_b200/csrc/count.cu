@@ -324,6 +324,8 @@ struct CoarseSmem {
   uint32_t stk[kSliceStack];
   uint64_t tot_n, tot_d;     // keys and distinct keys of this CTA's slices so far
   int sort_mode;
+  int dirty;                 // the table memory was reused by a sort
+  uint32_t occ[(TSO + 31) / 32];  // occupied table slots
   uint32_t nbig;             // long clusters: (first slot << 10) | length
   uint32_t bigl[CW_LIST];
 };
@@ -562,6 +564,7 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
   if (tid == 0) {
     S.tot_n = 0;
     S.tot_d = 0;
+    S.dirty = 1;  // the table starts uncleared
   }
   while (true) {
     if (tid == 0) {
@@ -687,9 +690,20 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
       // directly; larger ones (one heavy sub-bucket) still use the table
       const bool direct_sort = sort_mode && ns <= (uint32_t)SortCap<K>::value;
       if (!direct_sort) {  // aggregate in the table
-      for (int s = tid; s < TSO; s += SC_NT) {
-        S.u.t.key[s] = empty_key<K>();
-        S.u.t.cnt[s] = 0;
+      // The occupancy bitmap (a bit per slot, set when an insert claims the
+      // slot) lets the cluster walk, the output and the clearing touch only
+      // occupied slots; the whole table is cleared only after a sort reused
+      // its memory.
+      constexpr int NW = (TSO + 31) / 32;
+      static_assert(NW <= SC_NT, "one bitmap word per thread");
+      if (S.dirty) {
+        for (int s = tid; s < TSO; s += SC_NT) {
+          S.u.t.key[s] = empty_key<K>();
+          S.u.t.cnt[s] = 0;
+        }
+        for (int w = tid; w < NW; w += SC_NT) S.occ[w] = 0;
+        __syncthreads();
+        if (tid == 0) S.dirty = 0;
       }
       __syncthreads();
       for (uint32_t i = tid; i < ns; i += SC_NT) {
@@ -712,7 +726,12 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
           }
           if (cur == empty_key<K>()) {
             K prev = smem_cas(&S.u.t.key[slot], empty_key<K>(), x);
-            if (prev == empty_key<K>() || prev == x) {
+            if (prev == empty_key<K>()) {
+              atomicOr(&S.occ[slot >> 5], 1u << (slot & 31));
+              atomicAdd(&S.u.t.cnt[slot], 1u);
+              break;
+            }
+            if (prev == x) {
               atomicAdd(&S.u.t.cnt[slot], 1u);
               break;
             }
@@ -723,16 +742,30 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
         if (get_overflow(&S.overflow)) break;
       }
       __syncthreads();
-      constexpr int PER = (TSO + SC_NT - 1) / SC_NT;
-      const int s0 = tid * PER, s1 = min(s0 + PER, TSO);
-      uint32_t occ = 0;
-      if (!S.overflow) {
-        for (int s = s0; s < s1; s++) {
-          if (S.u.t.cnt[s] == 0) continue;
-          occ++;
-          if (s > 0 && S.u.t.cnt[s - 1] != 0) continue;  // not a cluster start
+      // clusters: runs of occupied slots; the owner of a cluster's first slot
+      // sorts a short one, long ones go to warps
+      const int w = tid;
+      const uint32_t wbits = w < NW ? S.occ[w] : 0u;
+      uint32_t occ = __popc(wbits);
+      if (!S.overflow && wbits) {
+        uint32_t bits = wbits;
+        while (bits) {
+          const int q = __ffs(bits) - 1;
+          bits &= bits - 1;
+          const int s = w * 32 + q;
+          const bool prev_occ = q > 0 ? ((wbits >> (q - 1)) & 1u) != 0 : (w > 0 && (S.occ[w - 1] >> 31) != 0);
+          if (prev_occ) continue;  // not a cluster start
           int e = s + 1;
-          while (e < TSO && S.u.t.cnt[e] != 0) e++;
+          for (int ww = e >> 5; ww < NW; ww++) {  // first free slot after s
+            const uint32_t inv = ~S.occ[ww] & (0xFFFFFFFFu << (ww == (e >> 5) ? (e & 31) : 0));
+            if (inv) {
+              e = ww * 32 + __ffs(inv) - 1;
+              break;
+            }
+            e = (ww + 1) * 32;
+            if (e - s > SL_CLUSTER_LIMIT) break;
+          }
+          e = min(e, TSO);
           if (e - s > SL_CLUSTER_LIMIT) {
             set_overflow(&S.overflow);
             break;
@@ -744,10 +777,10 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
               continue;
             }
           }
-          for (int q = s + 1; q < e; q++) {  // insertion sort of (key, count)
-            K x = S.u.t.key[q];
-            uint32_t c = S.u.t.cnt[q];
-            int r = q;
+          for (int qq = s + 1; qq < e; qq++) {  // insertion sort of (key, count)
+            K x = S.u.t.key[qq];
+            uint32_t c = S.u.t.cnt[qq];
+            int r = qq;
             while (r > s && x < S.u.t.key[r - 1]) {
               S.u.t.key[r] = S.u.t.key[r - 1];
               S.u.t.cnt[r] = S.u.t.cnt[r - 1];
@@ -765,13 +798,15 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
           warp_sort_pairs<K>(S.u.t.key + (S.bigl[t] >> 10), S.u.t.cnt + (S.bigl[t] >> 10), S.bigl[t] & 1023u);
       }
       __syncthreads();
-      if (!S.overflow) {
+      const bool ok = !S.overflow;
+      if (ok) {
         uint32_t D;
         const uint32_t pos = block_exclusive_scan<SC_NT>(occ, S.tmp, &D);
         const uint64_t base = start + S.run + pos;
-        uint32_t o = 0;
-        for (int s = s0; s < s1; s++) {
-          if (S.u.t.cnt[s] == 0) continue;
+        uint32_t o = 0, bits = wbits;
+        while (bits) {
+          const int s = w * 32 + __ffs(bits) - 1;
+          bits &= bits - 1;
           if (!in_bounds(a, 8, base + o, a.tmp_cap)) break;
           tkeys[base + o] = S.u.t.key[s];
           a.tmp_counts[base + o] = S.u.t.cnt[s];
@@ -783,9 +818,21 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
           S.tot_n += ns;
           S.tot_d += D;
         }
-        __syncthreads();
-        continue;
       }
+      // empty the occupied slots and the bitmap (after an overflow too: the
+      // bitmap marks exactly the slots inserts claimed)
+      {
+        uint32_t bits = wbits;
+        while (bits) {
+          const int s = w * 32 + __ffs(bits) - 1;
+          bits &= bits - 1;
+          S.u.t.key[s] = empty_key<K>();
+          S.u.t.cnt[s] = 0;
+        }
+        if (w < NW) S.occ[w] = 0;
+      }
+      __syncthreads();
+      if (ok) continue;
       if (j_hi - j_lo > 1 && sp + 1 <= kSliceStack) {
         if (tid == 0) {  // split: smallest mid in [j_lo+1, j_hi-1] with half the keys before it
           const uint32_t half = base_cnt + ns / 2;
@@ -802,7 +849,8 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
         continue;
       }
       }  // table
-      // ---- gather the slice's keys and sort them ----
+      // ---- gather the slice's keys and sort them (this reuses the table) ----
+      if (tid == 0) S.dirty = 1;
       if (tid == 0 && a.prof) atomicAdd(a.prof + (direct_sort ? 7 : 5), 1ull);
       const uint32_t fh = j_hi - 1;
       const int skip = (j_lo == fh) ? cb + SB : cb + SB - (32 - __clz(j_lo ^ fh));
