@@ -39,6 +39,7 @@ struct PartSmem {
   uint32_t badw[PT_WORDS];         // bit i: byte i is not ACGTU
   uint32_t rsw[PT_WORDS];          // bit i: a read starts at byte i
   uint32_t validw[PT_WORDS];       // bit l: window l lies inside one read
+  uint32_t touchw[PT_WORDS];       // bit l: window l covers a byte that is not ACGTU
   union {
     uint32_t g[PT_NLOC];           // filtered p-mer minimum per position, then suffix minima
     uint32_t boff[PT_NLOC];        // per superkmer: byte offset in the tile
@@ -70,6 +71,22 @@ GKC_DEV bool any_bits(const uint32_t *w, int a, int b) {
   for (int x = wa + 1; x < wb; x++)
     if (w[x]) return true;
   return (w[wb] & (0xFFFFFFFFu >> (31 - (b & 31)))) != 0u;
+}
+
+// Bit i (0..31) of the result = OR of bits i .. i+n-1 of the 96-bit value
+// (x2:x1:x0), for 1 <= n <= 64: a sliding OR built by doubling shifts.
+GKC_DEV uint32_t span_or(uint32_t x0, uint32_t x1, uint32_t x2, int n) {
+  uint64_t lo = (uint64_t)x0 | ((uint64_t)x1 << 32);
+  uint64_t hi = x2;
+  int m = 1;
+  while (2 * m <= n) {  // lo:hi now holds the OR over m consecutive bits
+    lo |= (lo >> m) | (hi << (64 - m));
+    hi |= hi >> m;
+    m *= 2;
+  }
+  const int r = n - m;  // 0 <= r < m: cover the remaining bits with an overlapping shift
+  if (r > 0) lo |= (lo >> r) | (hi << (64 - r));
+  return (uint32_t)lo;
 }
 
 __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
@@ -123,6 +140,29 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
         for (int u = 0; u < 4; u++) m |= (((x >> (8 * u)) & 0xFFu) == 255u ? 1u : 0u) << (t * 4 + u);
       }
       S.badw[w] = m;
+    }
+    __syncthreads();
+    // Windows are valid when no read starts inside them (after their first
+    // byte) and they lie inside the data; they touch a bad byte when one of
+    // their k bytes is not ACGTU.  32 windows per word, by sliding ORs.
+    for (int w = tid; w < PT_WORDS; w += PT_NT) {
+      const uint32_t r0 = S.rsw[w], r1 = w + 1 < PT_WORDS ? S.rsw[w + 1] : 0u,
+                     r2 = w + 2 < PT_WORDS ? S.rsw[w + 2] : 0u;
+      // read starts at window bytes 1 .. k-1: shift the span right by one
+      const uint32_t hit = k > 1 ? span_or((r0 >> 1) | (r1 << 31), (r1 >> 1) | (r2 << 31), r2 >> 1, k - 1) : 0u;
+      const uint32_t b0 = S.badw[w], b1 = w + 1 < PT_WORDS ? S.badw[w + 1] : 0u,
+                     b2 = w + 2 < PT_WORDS ? S.badw[w + 2] : 0u;
+      S.touchw[w] = span_or(b0, b1, b2, k);
+      // windows inside the data: G0 + l >= 0 and G0 + l + k <= nbytes
+      const int64_t s0 = G0 + 32 * (int64_t)w;
+      const int64_t ilo = s0 < 0 ? -s0 : 0;
+      const int64_t ihi = (int64_t)a.nbytes - k - s0;
+      uint32_t range = 0u;
+      if (ihi >= 0 && ilo <= 31) {
+        const int lo_i = (int)ilo, hi_i = (int)(ihi > 31 ? 31 : ihi);
+        if (hi_i >= lo_i) range = (0xFFFFFFFFu >> (31 - hi_i)) & (0xFFFFFFFFu << lo_i);
+      }
+      S.validw[w] = ~hit & range;
     }
 
     // ---- filtered p-mer minimum per position (rolling, 16 positions a task) ----
@@ -178,19 +218,13 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
       for (int j = 0; j <= PT_PER_THREAD; j++) {
         int l = PT_PRE - 1 + tid + j * PT_NT;
         mmv[j] = 0xFFFFFFFFu;
-        if (l < PT_PRE + PT_NW) {
-          int64_t s = G0 + l;
-          bool valid = s >= 0 && !any_bits(S.rsw, l + 1, l + k - 1) && (uint64_t)(s + k) <= a.nbytes;
-          if (valid) {
-            if (!any_bits(S.badw, l, l + k - 1)) {
-              mmv[j] = min(S.a.g[l], S.b.pre[l + omega - 1]);
-            } else {
-              const uint8_t *cw = S.cd + l;
-              mmv[j] = exact_window_minimizer([&](int i) { return (uint32_t)cw[i]; }, k, p);
-            }
+        if (l < PT_PRE + PT_NW && bit_at(S.validw, l)) {
+          if (!bit_at(S.touchw, l)) {
+            mmv[j] = min(S.a.g[l], S.b.pre[l + omega - 1]);
+          } else {
+            const uint8_t *cw = S.cd + l;
+            mmv[j] = exact_window_minimizer([&](int i) { return (uint32_t)cw[i]; }, k, p);
           }
-          // validity bit (atomicOr: several threads share a word)
-          if (valid) atomicOr(&S.validw[l >> 5], 1u << (l & 31));
         }
       }
     }
@@ -322,16 +356,20 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
       uint32_t *dst = reinterpret_cast<uint32_t *>(a.packed + base_byte);
       for (uint32_t w = tid; w < nwords; w += PT_NT) {
         uint32_t word = 0;
+        // superkmer holding the word's first byte: last i with boff[i] <= 4w
+        int lo = 0;
+        {
+          int hi = (int)n_skm - 1;
+          while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (S.a.boff[mid] <= w * 4) lo = mid; else hi = mid - 1;
+          }
+        }
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           uint32_t q = w * 4 + u;
           if (q >= tile_bytes) break;
-          // superkmer holding byte q: last i with boff[i] <= q
-          int lo = 0, hi = (int)n_skm - 1;
-          while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if (S.a.boff[mid] <= q) lo = mid; else hi = mid - 1;
-          }
+          while (lo + 1 < (int)n_skm && S.a.boff[lo + 1] <= q) lo++;
           uint32_t j = S.skm[lo];
           int l = S.brk[j];
           int e = (j + 1 < n_brk) ? S.brk[j + 1] : S.ext_end;
