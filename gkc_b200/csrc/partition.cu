@@ -31,6 +31,7 @@ constexpr int PT_NLOC = PT_PRE + PT_T + PT_H + 64;  // bytes held per tile (k <=
 constexpr int PT_NW = PT_T + PT_H;               // windows with break flags
 constexpr int PT_WORDS = PT_NLOC / 32;
 constexpr int PT_PER_THREAD = PT_NW / PT_NT;     // 9 contiguous windows per thread
+constexpr int PT_PT = 9;                         // positions per rolling p-mer task
 static_assert(PT_NW % PT_NT == 0, "windows per thread");
 static_assert(PT_NLOC % 64 == 0, "tile alignment");
 
@@ -110,36 +111,34 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
     const int64_t ts = (int64_t)tile * PT_T;
     const int64_t G0 = ts - PT_PRE;  // global position of local 0 (64-aligned)
 
-    // ---- load bytes -> codes, bad-code bitmap, read-start bitmap ----
-    for (int q = tid * 16; q < PT_NLOC; q += PT_NT * 16) {
-      int64_t g = G0 + q;
-      uint8_t bytes[16];
-      if (g >= 0 && (uint64_t)(g + 16) <= a.nbytes && a.aligned16) {
-        uint4 v = __ldg(reinterpret_cast<const uint4 *>(a.reads + g));
-        *reinterpret_cast<uint4 *>(bytes) = v;
+    // ---- load bytes -> codes (16 per thread, one 16-byte store), bad-code
+    //      bitmap (lane pairs combine their 16-bit halves), read-start bitmap ----
+    static_assert(PT_NLOC % 16 == 0 && PT_NLOC / 16 <= PT_NT, "one 16-byte group per thread");
+    if ((tid & ~31) * 16 < PT_NLOC) {  // warps with at least one group
+      const int q = tid * 16;
+      const bool act = q < PT_NLOC;
+      uint32_t cw[4] = {0u, 0u, 0u, 0u};
+      uint32_t bad16 = 0;
+      if (act) {
+        const int64_t g = G0 + q;
+        uint8_t bytes[16];
+        const bool fast = g >= 0 && (uint64_t)(g + 16) <= a.nbytes && a.aligned16;
+        if (fast) *reinterpret_cast<uint4 *>(bytes) = __ldg(reinterpret_cast<const uint4 *>(a.reads + g));
 #pragma unroll
-        for (int t = 0; t < 16; t++) S.cd[q + t] = (uint8_t)code_of_byte(bytes[t]);
-      } else {
-#pragma unroll
-        for (int t = 0; t < 16; t++) S.cd[q + t] = (uint8_t)global_code(a.reads, a.nbytes, g + t);
+        for (int t = 0; t < 16; t++) {
+          const uint32_t c = fast ? code_of_byte(bytes[t]) : global_code(a.reads, a.nbytes, g + t);
+          cw[t >> 2] |= c << (8 * (t & 3));
+          bad16 |= (c == 255u ? 1u : 0u) << t;
+        }
+        *reinterpret_cast<uint4 *>(S.cd + q) = make_uint4(cw[0], cw[1], cw[2], cw[3]);
       }
+      const uint32_t other = __shfl_xor_sync(0xffffffffu, bad16, 1);
+      if (act && (tid & 1) == 0) S.badw[q >> 5] = bad16 | (other << 16);
     }
     for (int w = tid; w < PT_WORDS; w += PT_NT) {
       int64_t gw = (G0 >> 5) + w;  // G0 is a multiple of 64
       S.rsw[w] = (gw >= 0 && (uint64_t)gw < a.rs_words) ? a.rs_bits[gw] : 0u;
       S.validw[w] = 0u;
-    }
-    __syncthreads();
-    for (int w = tid; w < PT_WORDS; w += PT_NT) {
-      uint32_t m = 0;
-      const uint32_t *c4 = reinterpret_cast<const uint32_t *>(S.cd + w * 32);
-#pragma unroll
-      for (int t = 0; t < 8; t++) {
-        uint32_t x = c4[t];
-#pragma unroll
-        for (int u = 0; u < 4; u++) m |= (((x >> (8 * u)) & 0xFFu) == 255u ? 1u : 0u) << (t * 4 + u);
-      }
-      S.badw[w] = m;
     }
     __syncthreads();
     // Windows are valid when no read starts inside them (after their first
@@ -167,17 +166,19 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
 
     // ---- filtered p-mer minimum per position (rolling, 16 positions a task) ----
     {
+      // tasks of PT_PT consecutive positions: an odd stride between threads
+      // keeps their shared-memory accesses in different banks
       const int npos = PT_NLOC - p + 1;
-      const int ntask = (npos + 15) / 16;
+      const int ntask = (npos + PT_PT - 1) / PT_PT;
       for (int task = tid; task < ntask; task += PT_NT) {
-        int a0 = task * 16;
+        int a0 = task * PT_PT;
         uint32_t f = 0, r = 0;
         for (int j = 0; j < p - 1; j++) {
           uint32_t c = S.cd[a0 + j] & 3u;
           f = (f << 2) | c;
           r = (r >> 2) | ((3u - c) << (2 * p - 2));
         }
-        int e = min(a0 + 16, npos);
+        int e = min(a0 + PT_PT, npos);
         for (int i = a0; i < e; i++) {
           uint32_t c = S.cd[i + p - 1] & 3u;
           f = ((f << 2) | c) & M;
