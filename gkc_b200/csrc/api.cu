@@ -696,8 +696,8 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   if (getenv("GKC_PROBE_LIMIT")) sa.probe_limit = atoi(getenv("GKC_PROBE_LIMIT"));
   sa.prof = nullptr;
   if (getenv("GKC_PROFILE_SORT")) {
-    WS(prof, unsigned long long, "sort_prof", 16);
-    CK(cudaMemsetAsync(prof, 0, 16 * 8, c->st));
+    WS(prof, unsigned long long, "sort_prof", 32);
+    CK(cudaMemsetAsync(prof, 0, 32 * 8, c->st));
     sa.prof = prof;
   }
   const size_t smem = coarse_smem_bytes<K>();
@@ -707,10 +707,13 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   LAUNCHED(c);
   stage_mark(c, 6);
   if (sa.prof && !c->capturing) {
-    unsigned long long h[16];
+    unsigned long long h[32];
     cudaMemcpyAsync(h, sa.prof, sizeof(h), cudaMemcpyDeviceToHost, c->st);
     cudaStreamSynchronize(c->st);
-    fprintf(stderr, "coarse_count profile: fallback slices=%llu split slices=%llu\n", h[5], h[6]);
+    fprintf(stderr,
+            "coarse_count profile: fallback slices=%llu split slices=%llu direct sorts=%llu | cycles of "
+            "thread 0: histogram+placement %llu, plan+insert %llu, clusters %llu, output %llu, sorts %llu\n",
+            h[5], h[6], h[7], h[16], h[17], h[18], h[19], h[20]);
   }
   scan_u64_dev(cd, cout_, max_buckets, bucket_base + nbins, stmp, c->st);
   WS(counts, uint32_t, "counts", keys_cap);

@@ -326,6 +326,7 @@ struct CoarseSmem {
   int sort_mode;
   int dirty;                 // the table memory was reused by a sort
   uint32_t occ[(TSO + 31) / 32];  // occupied table slots
+  unsigned long long ph[8];  // phase cycles (profiling only)
   uint32_t nbig;             // long clusters: (first slot << 10) | length
   uint32_t bigl[CW_LIST];
 };
@@ -566,6 +567,16 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
     S.tot_d = 0;
     S.dirty = 1;  // the table starts uncleared
   }
+  // optional phase profile (cycles of thread 0 between marks, per phase)
+  const bool prof = a.prof != nullptr;
+  if (tid < 8) S.ph[tid] = 0;
+  long long tph = 0;
+#define PHASE(i)                                       \
+  if (prof && tid == 0) {                              \
+    const long long _t = clock64();                    \
+    S.ph[i] += (unsigned long long)(_t - tph);         \
+    tph = _t;                                          \
+  }
   while (true) {
     if (tid == 0) {
       S.g = atomicAdd(a.ticket, 1ull);
@@ -590,6 +601,7 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
     const uint64_t g = S.g;
     if (g >= n_buckets) break;
     const uint64_t start = S.start, n = S.n;
+    if (prof && tid == 0) tph = clock64();
     const int cb = (int)a.bin_bits[S.b];
     const int SB = min(CC_SUB_BITS, key_bits - cb);
     const uint32_t nsub = 1u << SB;
@@ -643,6 +655,7 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
       }
     }
     __syncthreads();
+    PHASE(0)
     // slices: runs of sub-buckets whose exclusive start falls in the same
     // multiple of `target` (a slice holds < target keys plus one sub-bucket)
     {
@@ -742,6 +755,7 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
         if (get_overflow(&S.overflow)) break;
       }
       __syncthreads();
+      PHASE(1)
       // clusters: runs of occupied slots; the owner of a cluster's first slot
       // sorts a short one, long ones go to warps
       const int w = tid;
@@ -798,6 +812,7 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
           warp_sort_pairs<K>(S.u.t.key + (S.bigl[t] >> 10), S.u.t.cnt + (S.bigl[t] >> 10), S.bigl[t] & 1023u);
       }
       __syncthreads();
+      PHASE(2)
       const bool ok = !S.overflow;
       if (ok) {
         uint32_t D;
@@ -832,6 +847,7 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
         if (w < NW) S.occ[w] = 0;
       }
       __syncthreads();
+      PHASE(3)
       if (ok) continue;
       if (j_hi - j_lo > 1 && sp + 1 <= kSliceStack) {
         if (tid == 0) {  // split: smallest mid in [j_lo+1, j_hi-1] with half the keys before it
@@ -903,6 +919,7 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
         if (tid == 0) atomicExch(a.scratch_lock, 0ull);
       }
       __syncthreads();
+      PHASE(4)
      }
     }
     if (tid == 0) {
@@ -911,6 +928,9 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
     }
     __syncthreads();
   }
+  if (prof && tid == 0)
+    for (int i = 0; i < 8; i++) atomicAdd(a.prof + 16 + i, S.ph[i]);
+#undef PHASE
 }
 
 // Moves each coarse bucket's sorted runs to its final offset.

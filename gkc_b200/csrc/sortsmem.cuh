@@ -12,6 +12,7 @@ constexpr int SC_NT = kSortThreads;  // 1024: one CTA per SM
 constexpr int SC_DMAX = 12;           // bits per MSD counting pass
 constexpr int SC_SMAX = 32;           // leaves up to this size: insertion sort
 constexpr int SC_BIGMAX = 256;        // larger leaves recorded per pass
+constexpr int SC_WARPMAX = 1024;      // leaves up to this size: sorted by one warp
 
 template <typename K> struct SortCap;
 template <> struct SortCap<uint64_t> { static constexpr int value = 5632; };
@@ -98,6 +99,44 @@ GKC_DEV void bitonic_sort(K *A, uint32_t m) {
   }
 }
 
+// In-place ascending sort of A[0, m) by one warp (the same comparator form as
+// bitonic_sort, with warp barriers between stages).
+template <typename K>
+GKC_DEV void warp_bitonic_keys(K *A, uint32_t m) {
+  uint32_t P = 1;
+  while (P < m) P <<= 1;
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t size = 2; size <= P; size <<= 1) {
+    const uint32_t half = size >> 1;
+    for (uint32_t i = lane; i < P / 2; i += 32) {
+      const uint32_t blk = i / half, off = i % half;
+      const uint32_t lo = blk * size + off, hi = blk * size + size - 1 - off;
+      if (hi < m) {
+        const K x = A[lo], y = A[hi];
+        if (y < x) {
+          A[lo] = y;
+          A[hi] = x;
+        }
+      }
+    }
+    __syncwarp();
+    for (uint32_t stride = size >> 2; stride >= 1; stride >>= 1) {
+      for (uint32_t i = lane; i < P / 2; i += 32) {
+        const uint32_t blk = i / stride, off = i % stride;
+        const uint32_t lo = blk * 2 * stride + off, hi = lo + stride;
+        if (hi < m) {
+          const K x = A[lo], y = A[hi];
+          if (y < x) {
+            A[lo] = y;
+            A[hi] = x;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
 // Sorts S.A[0, n) ascending; keys agree on their top `skip` bits.
 template <typename K>
 GKC_DEV void smem_sort(SortSmem<K> &S, uint32_t n, int key_bits, int skip) {
@@ -141,8 +180,19 @@ GKC_DEV void smem_sort(SortSmem<K> &S, uint32_t n, int key_bits, int skip) {
   }
   __syncthreads();
   const uint32_t nbig = min(S.n_big, (uint32_t)SC_BIGMAX);
+  // leaves up to SC_WARPMAX keys: one warp each, all at once
+  for (uint32_t t = threadIdx.x >> 5; t < nbig; t += SC_NT / 32) {
+    const uint32_t s = S.big_s[t], m = S.big_m[t];
+    if (m > (uint32_t)SC_WARPMAX) continue;
+    for (uint32_t i = threadIdx.x & 31u; i < m; i += 32) S.A[s + i] = S.B[s + i];
+    __syncwarp();
+    warp_bitonic_keys<K>(S.A + s, m);
+  }
+  __syncthreads();
+  // larger leaves: the whole block, one after another
   for (uint32_t t = 0; t < nbig; t++) {
     const uint32_t s = S.big_s[t], m = S.big_m[t];
+    if (m <= (uint32_t)SC_WARPMAX) continue;
     for (uint32_t i = threadIdx.x; i < m; i += SC_NT) S.A[s + i] = S.B[s + i];
     __syncthreads();
     bitonic_sort<K>(S.A + s, m);
