@@ -103,6 +103,8 @@ SIGNATURES = [
     ("gkc_subsample_positions_device", C.c_int, [vp, P(Params), u32, vp, u64, vp, u64,
                                                  P(PoslistView)]),
     ("gkc_hpc_device", C.c_int, [vp, vp, u64, vp, u64, vp, vp, vp]),
+    ("gkc_fastx_load", C.c_int, [C.c_char_p, C.c_int, C.c_int, P(vp), P(vp), P(u64)]),
+    ("gkc_fastx_free", None, [vp, vp, C.c_int]),
     ("gkc_server_create", C.c_int, [C.c_int, u64, C.c_int, P(vp)]),
     ("gkc_server_destroy", None, [vp]),
     ("gkc_server_submit", C.c_int, [vp, P(Params), vp, vp, u64, P(u64)]),
@@ -377,3 +379,21 @@ class Server:
 
 def job_hbm_estimate(prm, n_bases, n_reads):
     return int(lib().gkc_job_hbm_estimate(C.byref(prm), int(n_bases), int(n_reads)))
+
+
+def load_fastx(path, threads=0):
+    """(reads uint8, offs uint64) of a FASTA / FASTQ file (gkc_fastx_load)."""
+    L = lib()
+    r, o, n = C.c_void_p(), C.c_void_p(), C.c_uint64()
+    st = L.gkc_fastx_load(os.fsencode(path), int(threads), 0, C.byref(r), C.byref(o), C.byref(n))
+    if st != 0:
+        raise GkcError(st, f"gkc_fastx_load {path}")
+    try:
+        nr = int(n.value)
+        offs = np.ctypeslib.as_array(C.cast(o, C.POINTER(C.c_uint64)), shape=(nr + 1,)).copy()
+        nb = int(offs[-1])
+        reads = (np.ctypeslib.as_array(C.cast(r, C.POINTER(C.c_uint8)), shape=(nb,)).copy()
+                 if nb else np.zeros(0, np.uint8))
+    finally:
+        L.gkc_fastx_free(r, o, 0)
+    return reads, offs

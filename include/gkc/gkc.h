@@ -202,6 +202,20 @@ gkc_status gkc_hpc_device(gkc_ctx *ctx, const char *d_reads, uint64_t n_bytes,
                           const uint64_t *d_offs, uint64_t n_reads, char *d_out_reads,
                           uint64_t *d_out_offs, int32_t *d_orig_pos);
 
+/* ---- FASTA / FASTQ ingest (reference: ReadLoader, read_loader.hpp:44-196,
+ *      :276-321, :470-520).  Reads the file (format from its first byte, '>'
+ *      or '@') on n_threads threads (0: all cores) into one read CSR, in file
+ *      order: *reads holds the sequences back to back, *offs their n_reads+1
+ *      offsets.  FASTQ: the second line of each 4-line record; FASTA: the
+ *      lines after a header up to the next header, joined (the reference
+ *      keeps only the first).  A '\r' before a line end is dropped.  With
+ *      pinned != 0 the arrays are page-locked (fast host-to-device copies).
+ *      Free them with gkc_fastx_free and the same `pinned`.  No GPU is
+ *      needed unless pinned != 0. ---- */
+gkc_status gkc_fastx_load(const char *path, int n_threads, int pinned, char **reads, uint64_t **offs,
+                          uint64_t *n_reads);
+void gkc_fastx_free(char *reads, uint64_t *offs, int pinned);
+
 /* ---- serving: continuous batching of counting jobs against an HBM budget ---- */
 typedef struct gkc_server gkc_server;
 typedef enum gkc_job_state {
