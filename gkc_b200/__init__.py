@@ -95,6 +95,7 @@ SIGNATURES = [
     ("gkc_count_device", C.c_int, [vp, P(Params), C.c_int, P(CountView)]),
     ("gkc_count_superkmers_host", C.c_int, [vp, C.c_int, vp, vp, u64, C.c_int, P(u64)]),
     ("gkc_count_copy_out", C.c_int, [vp, vp, vp, vp]),
+    ("gkc_count_output", C.c_int, [vp, u32, u32, C.c_int, P(u64), vp, vp, vp]),
     ("gkc_count_superkmers_device_noalloc", C.c_int, [C.c_int, vp, vp, u64, u64, vp, vp, P(u64), vp]),
     ("gkc_pipeline_device", C.c_int, [vp, P(Params), C.c_int, vp, u64, vp, u64, P(PartitionView),
                                       P(CountView)]),
@@ -253,6 +254,22 @@ class Context:
         self._check(self._L.gkc_count_copy_out(self.h, _ptr(bin_off), _ptr(keys), _ptr(counts)),
                     "count_copy_out")
         return bin_off, keys[:nd * kw].reshape(nd, kw), counts[:nd]
+
+    def count_output(self, min_count=1, max_count=0xFFFFFFFF, merged=False, key_words=1, nbins=None):
+        """-> (bin_off, keys (n, key_words), counts): the last count result
+        filtered to min_count <= count <= max_count, per bin or merged."""
+        n = C.c_uint64()
+        self._check(self._L.gkc_count_output(self.h, int(min_count), int(max_count), int(bool(merged)),
+                                             C.byref(n), None, None, None), "count_output")
+        nn = int(n.value)
+        nb = 1 if merged else int(nbins)
+        bin_off = np.zeros(nb + 1, np.uint64)
+        keys = np.zeros(max(nn * key_words, 1), np.uint64)
+        counts = np.zeros(max(nn, 1), np.uint32)
+        self._check(self._L.gkc_count_output(self.h, int(min_count), int(max_count), int(bool(merged)),
+                                             C.byref(n), _ptr(bin_off), _ptr(keys), _ptr(counts)),
+                    "count_output")
+        return bin_off, keys[:nn * key_words].reshape(nn, key_words), counts[:nn]
 
     # ---- pipeline ----
     def pipeline_device(self, d_reads, n_bytes, d_offs, n_reads, prm, mode=MODE_BATCHED):

@@ -748,6 +748,7 @@ static void fill_count_view(gkc_ctx *c, const gkc_params *prm) {
   v.counts = (const uint32_t *)c->bufs["counts"].p;
   c->ck = prm->k;
   c->have_count = true;
+  c->count_gen++;
 }
 
 gkc_status count_device_impl(gkc_ctx *c, const gkc_params *prm, gkc_mode mode) {

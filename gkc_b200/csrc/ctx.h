@@ -56,6 +56,12 @@ struct gkc_ctx {
   const int32_t *part_hpc_orig = nullptr;
   // count state
   bool have_count = false;
+  uint64_t count_gen = 0;  // bumped by every new count result
+  // gkc_count_output cache
+  bool have_out = false;
+  uint32_t out_min = 0, out_max = 0, out_nbins = 0;
+  int out_merged = 0;
+  uint64_t out_n = 0, out_gen = 0;
   int ck = 0;
   gkc_count_view cv{};
   uint64_t count_keys_cap = 0;

@@ -411,6 +411,7 @@ static gkc_status count_plain_t(gkc_ctx *c, const gkc_params *prm) {
   v.counts = counts;
   c->ck = k;
   c->have_count = true;
+  c->count_gen++;
   return GKC_OK;
 }
 

@@ -163,6 +163,19 @@ gkc_status gkc_count_superkmers_device_noalloc(int k, const uint32_t *d_skm_len,
                                                uint32_t *d_counts_out, uint64_t *n_distinct,
                                                void *cuda_stream);
 
+/* Output options over the last count result (reference: the min/max
+ * frequency filter of kmc_counting_GPU, kmer_counting.cu:188-190, defaults
+ * utilities.hpp:109, commented out there; the merged global list,
+ * README.md:17,31-33).  merged = 0: per bin, the (k-mer, count) pairs with
+ * min_count <= count <= max_count; merged = 1: one sorted list over all bins,
+ * the counts of a k-mer found in several bins added up (clamped to
+ * UINT32_MAX), then the same filter.  *n_out receives the number of pairs;
+ * when bin_off (nbins+1 entries, or 2 when merged), keys (n_out * key_words)
+ * and counts (n_out) are not NULL they receive the list.  Calling first with
+ * NULL arrays to size them and again to copy computes the list once. */
+gkc_status gkc_count_output(gkc_ctx *ctx, uint32_t min_count, uint32_t max_count, int merged,
+                            uint64_t *n_out, uint64_t *bin_off, uint64_t *keys, uint32_t *counts);
+
 /* ---- whole pipeline: reads -> superkmer partitions -> sorted (k-mer, count)
  *      (reference: process_reads_count + gen_skm_and_count_with_TP,
  *      experiment.cpp:76-89,156-219) ---- */
