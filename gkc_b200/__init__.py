@@ -18,6 +18,8 @@ LIB_PATH = os.path.join(HERE, "libgkc_b200.so")
 MODE_BATCHED = 0
 MODE_PLAIN = 1
 
+FILTER_NEW2, FILTER_ALL, FILTER_NEW, FILTER_SIGNATURE = 0, 1, 2, 3
+
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no CUDA device",
           4: "out of device memory", 5: "HBM budget exceeded", 6: "capacity exceeded",
           7: "device-side wait timed out", 8: "not ready", 9: "cancelled", 10: "not found",
@@ -85,6 +87,7 @@ SIGNATURES = [
     ("gkc_ctx_destroy", None, [vp]),
     ("gkc_ctx_last_error", C.c_char_p, [vp]),
     ("gkc_ctx_set_stream", C.c_int, [vp, vp]),
+    ("gkc_ctx_set_filter", C.c_int, [vp, C.c_int]),
     ("gkc_ctx_synchronize", C.c_int, [vp]),
     ("gkc_ctx_device_bytes", u64, [vp]),
     ("gkc_ctx_release_workspace", C.c_int, [vp]),
@@ -197,6 +200,10 @@ class Context:
 
     def device_bytes(self):
         return int(self._L.gkc_ctx_device_bytes(self.h))
+
+    def set_filter(self, filter_id):
+        """Minimizer filter for later calls (FILTER_*)."""
+        self._check(self._L.gkc_ctx_set_filter(self.h, int(filter_id)), "set_filter")
 
     def set_stream(self, stream_ptr):
         self._check(self._L.gkc_ctx_set_stream(self.h, C.c_void_p(stream_ptr)), "set_stream")

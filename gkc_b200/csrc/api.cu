@@ -264,6 +264,18 @@ void gkc_ctx_destroy(gkc_ctx *c) {
 
 const char *gkc_ctx_last_error(const gkc_ctx *c) { return c ? c->err.c_str() : "no context"; }
 
+gkc_status gkc_ctx_set_filter(gkc_ctx *c, int filter) {
+  if (!c) return GKC_ERR_INVALID_ARG;
+  if (filter < GKC_FILTER_NEW2 || filter > GKC_FILTER_SIGNATURE)
+    return ctx_fail(c, GKC_ERR_INVALID_ARG, "unknown minimizer filter");
+  if (filter != c->filter) {
+    c->filter = filter;
+    c->graph_valid = false;
+    c->have_part = c->have_count = false;
+  }
+  return GKC_OK;
+}
+
 gkc_status gkc_ctx_set_stream(gkc_ctx *c, void *stream) {
   if (!c) return GKC_ERR_INVALID_ARG;
   cudaSetDevice(c->dev);
@@ -417,6 +429,7 @@ static gkc_status enqueue_partition(gkc_ctx *c, const gkc_params *prm, const cha
 
   PartArgs a;
   memset(&a, 0, sizeof(a));
+  a.filter = c->filter;
   a.reads = src;
   a.nbytes = n_bytes;
   a.nbytes_dev = nbytes_dev;
@@ -807,7 +820,7 @@ gkc_status gkc_count_device(gkc_ctx *c, const gkc_params *prm, gkc_mode mode, gk
 // unchanged.  All sizes the kernels need are read on the device.
 static gkc_status pipeline_batched(gkc_ctx *c, const gkc_params *prm, const char *d_reads,
                                    uint64_t n_bytes, const uint64_t *d_offs, uint64_t n_reads) {
-  GraphKey key{d_reads, d_offs, n_bytes, n_reads, prm->k, prm->p, prm->hpc, prm->nbins};
+  GraphKey key{d_reads, d_offs, n_bytes, n_reads, prm->k, prm->p, prm->hpc, prm->nbins, c->filter};
   uint64_t cap_skm, cap_bytes;
   partition_caps(prm, n_bytes, n_reads, &cap_skm, &cap_bytes);
   if (c->graph_valid && c->gkey == key && c->gexec) {

@@ -33,11 +33,36 @@ GKC_DEV uint32_t code_of_byte(uint32_t c) {
   return 255u;
 }
 
-// The minimizer filter the reference selects (new_filter2): the top three
-// bases of the p-mer value (taken unmasked) are not AAA, ACA or AGA.
-GKC_DEV bool mm_filter(uint32_t v, int p) {
-  uint32_t t = v >> (2 * (p - 3));
-  return (t != 0u) & (t != 4u) & (t != 8u);
+// Which p-mers may be minimizers (the reference selects one at compile time,
+// FILTER_KERNEL, gkc_cuda.cu:6, from the variants at :196-227):
+//   0 new_filter2 (the reference's choice): the top three bases of the p-mer
+//     value are not AAA, ACA or AGA;
+//   1 every p-mer (its mm_filter);
+//   2 new_filter: the second and third bases from the top are not both A;
+//   3 sign_filter (KMC2 signatures): no AA in the lowest p-1 bases, and the
+//     top three bases are not AAA or ACA.
+// Values are taken unmasked, as the reference does.
+enum : int { FILTER_NEW2 = 0, FILTER_ALL = 1, FILTER_NEW = 2, FILTER_SIGNATURE = 3 };
+
+GKC_DEV bool mm_filter(uint32_t v, int p, int filter = FILTER_NEW2) {
+  const uint32_t t = v >> (2 * (p - 3));
+  switch (filter) {
+    case FILTER_ALL:
+      return true;
+    case FILTER_NEW:
+      return (((v >> (2 * (p - 2))) & 3u) + ((v >> (2 * (p - 3))) & 3u)) != 0u;
+    case FILTER_SIGNATURE: {
+      uint32_t x = v;
+      bool ok = true;
+      for (int i = 0; i < p - 2; i++) {
+        ok &= (x & 0xFu) != 0u;
+        x >>= 2;
+      }
+      return ok & (t != 0u) & (t != 4u);
+    }
+    default:
+      return (t != 0u) & (t != 4u) & (t != 8u);
+  }
 }
 
 // Reverse complement of a 2k-bit k-mer held in the low bits of x.

@@ -23,15 +23,16 @@ struct DevTotals {
 struct GraphKey {
   const void *reads, *offs;
   uint64_t n_bytes, n_reads;
-  int k, p, hpc, nbins;
+  int k, p, hpc, nbins, filter;
   bool operator==(const GraphKey &o) const {
     return reads == o.reads && offs == o.offs && n_bytes == o.n_bytes && n_reads == o.n_reads &&
-           k == o.k && p == o.p && hpc == o.hpc && nbins == o.nbins;
+           k == o.k && p == o.p && hpc == o.hpc && nbins == o.nbins && filter == o.filter;
   }
 };
 
 struct gkc_ctx {
   int dev = 0;
+  int filter = 0;  // minimizer filter (gkc_filter)
   int n_sms = 148;
   int max_smem_optin = 0;
   cudaStream_t st = nullptr;

@@ -7,6 +7,7 @@
 namespace gkc {
 
 struct PartArgs {
+  int filter;            // minimizer filter (FILTER_*)
   const uint8_t *reads;  // concatenated read bytes (CSR), offsets rebased to 0
   uint64_t nbytes;       // byte count (an upper bound when nbytes_dev is set)
   const uint64_t *nbytes_dev;  // optional: device-side byte count

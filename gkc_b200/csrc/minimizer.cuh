@@ -7,24 +7,24 @@ namespace gkc {
 // Exact reference update rule for one window (gkc_cuda.cu:256-286), on codes
 // that may be 255.  `code(i)` returns the code of window base i.
 template <typename CodeFn>
-GKC_DEV uint32_t exact_window_minimizer(CodeFn code, int k, int p) {
+GKC_DEV uint32_t exact_window_minimizer(CodeFn code, int k, int p, int filter = FILTER_NEW2) {
   const uint32_t M = 0xFFFFFFFFu >> (32 - 2 * p);
   uint32_t f = 0, r = 0, m, mr, best;
   for (int j = 0; j < p; j++) f = (f << 2) | code(j);
-  m = mm_filter(f, p) ? f : M;
+  m = mm_filter(f, p, filter) ? f : M;
   for (int j = p - 1; j >= 0; j--) {
     uint32_t c = code(j);
     r = (r << 2) | (c == 255u ? 255u : 3u - c);
   }
-  mr = mm_filter(r, p) ? r : M;
+  mr = mm_filter(r, p, filter) ? r : M;
   best = (mr < m) ? mr : m;
   for (int j = p; j < k; j++) {
     uint32_t c = code(j);
     uint32_t cc = (c == 255u) ? 255u : 3u - c;
     f = ((f << 2) | c) & M;
     r = (r >> 2) | (cc << (2 * p - 2));
-    if (mm_filter(f, p)) m = f;
-    if (mm_filter(r, p)) mr = r;
+    if (mm_filter(f, p, filter)) m = f;
+    if (mm_filter(r, p, filter)) mr = r;
     best = (best < m) ? best : m;
     best = (best < mr) ? best : mr;
   }

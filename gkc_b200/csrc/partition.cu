@@ -58,6 +58,35 @@ struct PartSmem {
   unsigned long long base_skm, base_byte;
 };
 
+// Filtered p-mer minimum of every tile position (forward and reverse
+// complement), rolling over tasks of PT_PT consecutive positions; an odd
+// stride between threads keeps their shared-memory accesses in different
+// banks.  The filter is fixed per instantiation so the inner loop holds no
+// branch on it.
+template <int FILT>
+GKC_DEV void pmer_minima(PartSmem &S, int p, uint32_t M, int tid) {
+  const int npos = PT_NLOC - p + 1;
+  const int ntask = (npos + PT_PT - 1) / PT_PT;
+  for (int task = tid; task < ntask; task += PT_NT) {
+    int a0 = task * PT_PT;
+    uint32_t f = 0, r = 0;
+    for (int j = 0; j < p - 1; j++) {
+      uint32_t c = S.cd[a0 + j] & 3u;
+      f = (f << 2) | c;
+      r = (r >> 2) | ((3u - c) << (2 * p - 2));
+    }
+    int e = min(a0 + PT_PT, npos);
+    for (int i = a0; i < e; i++) {
+      uint32_t c = S.cd[i + p - 1] & 3u;
+      f = ((f << 2) | c) & M;
+      r = (r >> 2) | ((3u - c) << (2 * p - 2));
+      uint32_t vf = mm_filter(f, p, FILT) ? f : M;
+      uint32_t vr = mm_filter(r, p, FILT) ? r : M;
+      S.a.g[i] = vf < vr ? vf : vr;
+    }
+  }
+}
+
 GKC_DEV bool bit_at(const uint32_t *w, int i) { return (w[i >> 5] >> (i & 31)) & 1u; }
 
 // Any bit set in [a, b] (inclusive), b - a < 96.
@@ -164,30 +193,12 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
       S.validw[w] = ~hit & range;
     }
 
-    // ---- filtered p-mer minimum per position (rolling, 16 positions a task) ----
-    {
-      // tasks of PT_PT consecutive positions: an odd stride between threads
-      // keeps their shared-memory accesses in different banks
-      const int npos = PT_NLOC - p + 1;
-      const int ntask = (npos + PT_PT - 1) / PT_PT;
-      for (int task = tid; task < ntask; task += PT_NT) {
-        int a0 = task * PT_PT;
-        uint32_t f = 0, r = 0;
-        for (int j = 0; j < p - 1; j++) {
-          uint32_t c = S.cd[a0 + j] & 3u;
-          f = (f << 2) | c;
-          r = (r >> 2) | ((3u - c) << (2 * p - 2));
-        }
-        int e = min(a0 + PT_PT, npos);
-        for (int i = a0; i < e; i++) {
-          uint32_t c = S.cd[i + p - 1] & 3u;
-          f = ((f << 2) | c) & M;
-          r = (r >> 2) | ((3u - c) << (2 * p - 2));
-          uint32_t vf = mm_filter(f, p) ? f : M;
-          uint32_t vr = mm_filter(r, p) ? r : M;
-          S.a.g[i] = vf < vr ? vf : vr;
-        }
-      }
+    // ---- filtered p-mer minimum per position ----
+    switch (a.filter) {
+      case FILTER_ALL: pmer_minima<FILTER_ALL>(S, p, M, tid); break;
+      case FILTER_NEW: pmer_minima<FILTER_NEW>(S, p, M, tid); break;
+      case FILTER_SIGNATURE: pmer_minima<FILTER_SIGNATURE>(S, p, M, tid); break;
+      default: pmer_minima<FILTER_NEW2>(S, p, M, tid); break;
     }
     __syncthreads();
 
@@ -224,7 +235,7 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
             mmv[j] = min(S.a.g[l], S.b.pre[l + omega - 1]);
           } else {
             const uint8_t *cw = S.cd + l;
-            mmv[j] = exact_window_minimizer([&](int i) { return (uint32_t)cw[i]; }, k, p);
+            mmv[j] = exact_window_minimizer([&](int i) { return (uint32_t)cw[i]; }, k, p, a.filter);
           }
         }
       }
@@ -284,7 +295,7 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
         while (w < a.nbytes) {
           if (global_rs(a.rs_bits, w) || !global_window_valid(a.rs_bits, a.nbytes, w, k)) break;
           uint32_t v = exact_window_minimizer(
-              [&](int i) { return global_code(a.reads, a.nbytes, (int64_t)w + i); }, k, p);
+              [&](int i) { return global_code(a.reads, a.nbytes, (int64_t)w + i); }, k, p, a.filter);
           if (v != mv) break;
           w++;
         }

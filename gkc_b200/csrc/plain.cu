@@ -26,12 +26,12 @@ using namespace gkc;
 namespace gkc {
 
 __global__ void k_plain_minimizer(const uint8_t *reads, const uint64_t *nbytes_dev, uint64_t nb_max,
-                                  const uint32_t *rs_bits, int k, int p, uint32_t *mm) {
+                                  const uint32_t *rs_bits, int k, int p, int filter, uint32_t *mm) {
   const uint64_t nbytes = nbytes_dev ? *nbytes_dev : nb_max;
   for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nbytes;
        s += (uint64_t)gridDim.x * blockDim.x) {
     if (!global_window_valid(rs_bits, nbytes, s, k)) continue;
-    mm[s] = exact_window_minimizer([&](int i) { return global_code(reads, nbytes, (int64_t)s + i); }, k, p);
+    mm[s] = exact_window_minimizer([&](int i) { return global_code(reads, nbytes, (int64_t)s + i); }, k, p, filter);
   }
 }
 
@@ -257,7 +257,7 @@ gkc_status partition_plain_impl(gkc_ctx *c, const gkc_params *prm, const char *d
   CK(cudaMemsetAsync(rs, 0, rs_words * 4, c->st));
   k_read_start_bits<<<(unsigned)std::min<uint64_t>((n_reads + 256) / 256, 65535), 256, 0, c->st>>>(offs, n_reads, rs);
   WS(mm, uint32_t, "plain_mm", n_bytes + 1);
-  k_plain_minimizer<<<grid, 256, 0, c->st>>>(src, nbytes_dev, n_bytes, rs, prm->k, prm->p, mm);
+  k_plain_minimizer<<<grid, 256, 0, c->st>>>(src, nbytes_dev, n_bytes, rs, prm->k, prm->p, c->filter, mm);
   WS(nskm, unsigned long long, "plain_nskm", n_reads + 1);
   WS(nbyt, unsigned long long, "plain_nbytes", n_reads + 1);
   WS(skm_off, uint64_t, "plain_skm_off", n_reads + 2);

@@ -61,9 +61,9 @@ struct WinMin {
 };
 
 // Minimizer, position and strand of the window at i (inside a read).
-GKC_DEV WinMin window_min_pos(const uint8_t *reads, uint64_t i, int k, int p) {
+GKC_DEV WinMin window_min_pos(const uint8_t *reads, uint64_t i, int k, int p, int filter) {
   WinMin w;
-  w.mm = exact_window_minimizer([&](int j) { return code_of_byte(reads[i + j]); }, k, p);
+  w.mm = exact_window_minimizer([&](int j) { return code_of_byte(reads[i + j]); }, k, p, filter);
   const uint32_t M = 0xFFFFFFFFu >> (32 - 2 * p);
   uint32_t f = 0, r = 0;
   int bpos = 255, bstr = 0;
@@ -74,8 +74,8 @@ GKC_DEV WinMin window_min_pos(const uint8_t *reads, uint64_t i, int k, int p) {
     f = ((f << 2) | c) & M;
     r = (r >> 2) | (cc << (2 * p - 2));
     if (j + 1 >= p) {
-      const bool mf = mm_filter(f, p) && f == w.mm;
-      const bool mr = mm_filter(r, p) && r == w.mm;
+      const bool mf = mm_filter(f, p, filter) && f == w.mm;
+      const bool mr = mm_filter(r, p, filter) && r == w.mm;
       if (mf || mr) {
         bpos = j + 1 - p;
         bstr = (f == r) ? -1 : (mr ? 1 : 0);
@@ -88,13 +88,13 @@ GKC_DEV WinMin window_min_pos(const uint8_t *reads, uint64_t i, int k, int p) {
 }
 
 __global__ void k_window_minimizers(const uint8_t *reads, uint64_t n_bytes, const uint64_t *offs,
-                                    uint64_t n_reads, const uint32_t *bits, int k, int p,
+                                    uint64_t n_reads, const uint32_t *bits, int k, int p, int filter,
                                     uint32_t *mm, uint8_t *pos, int8_t *strand) {
   const uint64_t lo = offs[0], hi = offs[n_reads];
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_bytes;
        i += (uint64_t)gridDim.x * blockDim.x) {
     WinMin w{0xFFFFFFFFu, 255, 0};
-    if (hi <= n_bytes && window_inside(bits, i, k, lo, hi)) w = window_min_pos(reads, i, k, p);
+    if (hi <= n_bytes && window_inside(bits, i, k, lo, hi)) w = window_min_pos(reads, i, k, p, filter);
     mm[i] = w.mm;
     if (pos) pos[i] = w.pos;
     if (strand) strand[i] = w.strand;
@@ -109,8 +109,8 @@ constexpr int SUB_TILE = SUB_NT * SUB_ITEMS;  // windows per tile = 128 bitmap w
 
 // Tile t covers windows [t*SUB_TILE, (t+1)*SUB_TILE): selection bitmap and count.
 __global__ void k_sub_flags(const uint8_t *reads, uint64_t n_bytes, const uint64_t *offs,
-                            uint64_t n_reads, const uint32_t *bits, int k, int p, uint32_t mod,
-                            uint32_t *sel, unsigned long long *tile_cnt) {
+                            uint64_t n_reads, const uint32_t *bits, int k, int p, int filter,
+                            uint32_t mod, uint32_t *sel, unsigned long long *tile_cnt) {
   __shared__ uint64_t tmp[32];
   const uint64_t lo = offs[0], hi = offs[n_reads];
   const uint64_t t = blockIdx.x;
@@ -122,7 +122,7 @@ __global__ void k_sub_flags(const uint8_t *reads, uint64_t n_bytes, const uint64
     const uint64_t i = word * 32 + lane;
     bool f = false;
     if (i < n_bytes && hi <= n_bytes && window_inside(bits, i, k, lo, hi)) {
-      const uint32_t m = exact_window_minimizer([&](int j) { return code_of_byte(reads[i + j]); }, k, p);
+      const uint32_t m = exact_window_minimizer([&](int j) { return code_of_byte(reads[i + j]); }, k, p, filter);
       f = (m % mod) == 0u;
     }
     const uint32_t b = __ballot_sync(0xffffffffu, f);
@@ -231,7 +231,7 @@ gkc_status gkc_minimizers_device(gkc_ctx *c, const gkc_params *prm, const char *
   s = mark_starts(c, d_offs, n_reads, n_bytes, &bits, &err);
   if (s != GKC_OK) return s;
   k_window_minimizers<<<c->n_sms * 16, 256, 0, c->st>>>(reinterpret_cast<const uint8_t *>(d_reads), n_bytes,
-                                                         d_offs, n_reads, bits, prm->k, prm->p, d_minimizer,
+                                                         d_offs, n_reads, bits, prm->k, prm->p, c->filter, d_minimizer,
                                                          d_pos, d_strand);
   CK(cudaPeekAtLastError());
   return read_err(c, err);
@@ -250,7 +250,7 @@ static gkc_status subsample_t(gkc_ctx *c, const gkc_params *prm, uint32_t mod, c
   WS(toff, uint64_t, "win_tile_off", tiles + 2);
   WS(stmp, uint64_t, "win_scan_tmp", scan_u64_tmp_words(tiles + 1) + 8);
   k_sub_flags<<<(unsigned)tiles, SUB_NT, 0, c->st>>>(reads, n_bytes, d_offs, n_reads, bits, prm->k, prm->p,
-                                                     mod, sel, tcnt);
+                                                     c->filter, mod, sel, tcnt);
   scan_u64(tcnt, toff, tiles, stmp, c->st);
   CK(cudaPeekAtLastError());
   uint64_t n = 0;

@@ -102,6 +102,17 @@ void gkc_ctx_destroy(gkc_ctx *ctx);
 const char *gkc_ctx_last_error(const gkc_ctx *ctx);
 const char *gkc_status_string(gkc_status s);
 gkc_status gkc_ctx_set_stream(gkc_ctx *ctx, void *cuda_stream);
+/* Which p-mers may be minimizers (the reference chooses one at compile time,
+ * FILTER_KERNEL at gkc_cuda.cu:6, among the variants at :196-227).  The
+ * setting applies to every later call on the context. */
+typedef enum gkc_filter {
+  GKC_FILTER_NEW2 = 0,      /* new_filter2, the reference's choice (default):
+                               the top three bases are not AAA, ACA or AGA */
+  GKC_FILTER_ALL = 1,       /* mm_filter: every p-mer */
+  GKC_FILTER_NEW = 2,       /* new_filter: 2nd and 3rd bases not both A */
+  GKC_FILTER_SIGNATURE = 3  /* sign_filter: KMC2 signatures */
+} gkc_filter;
+gkc_status gkc_ctx_set_filter(gkc_ctx *ctx, int filter);
 gkc_status gkc_ctx_synchronize(gkc_ctx *ctx);
 uint64_t gkc_ctx_device_bytes(const gkc_ctx *ctx);
 gkc_status gkc_ctx_release_workspace(gkc_ctx *ctx);

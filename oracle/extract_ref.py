@@ -18,7 +18,9 @@ RANGES = [
     (25, 93, "d_basemap[256]"),                 # code tables
     (146, 339, "struct T_d_data"),              # HPC, filters, minimizer, GenSKM, MoveOffset
 ]
+FILTER_LINE = 6  # "#define FILTER_KERNEL new_filter2"
 ANCHORS = {
+    FILTER_LINE: "#define FILTER_KERNEL",
     164: "GPU_HPCEncoding",
     234: "GPU_GenMinimizer",
     298: "GPU_GenSKM",
@@ -37,7 +39,14 @@ def main():
         f.write("// generated by oracle/extract_ref.py -- not source\n")
         for a, b, _ in RANGES:
             f.write(f'#line {a} "{path}"\n')
-            f.write("\n".join(lines[a - 1:b]) + "\n")
+            for ln in range(a, b + 1):
+                text = lines[ln - 1]
+                if ln == FILTER_LINE:
+                    # the filter stays selectable: -DFILTER_KERNEL=<variant>
+                    f.write("#ifndef FILTER_KERNEL\n" + text + "\n#endif\n")
+                    f.write(f'#line {ln + 1} "{path}"\n')
+                else:
+                    f.write(text + "\n")
 
 
 if __name__ == "__main__":

@@ -35,12 +35,35 @@ static inline uint32_t ccode_of(uint8_t c) {
   return 3 - x;
 }
 
-/* new_filter2, the filter selected at gkc_cuda.cu:6 (definition :214-216):
- * the top three bases of the p-mer are not AAA, ACA or AGA.  Applied to the
- * unmasked value exactly as the reference does. */
+/* The minimizer filter (FILTER_KERNEL, gkc_cuda.cu:6; variants :196-227),
+ * applied to the unmasked p-mer value as the reference does:
+ *   0 new_filter2 (:214-216, the reference's choice): top three bases not
+ *     AAA, ACA or AGA;  1 mm_filter (:196-209): every p-mer;
+ *   2 new_filter (:211-213): 2nd and 3rd bases not both A;
+ *   3 sign_filter (:218-227): no AA among the lowest p-1 bases, top three
+ *     bases not AAA or ACA. */
+static int g_filter = 0;
+void orc_set_filter(int f) { g_filter = f; }
+
 static inline int filt(uint32_t v, int p) {
   uint32_t t = v >> (2 * (p - 3));
-  return (t != 0) & (t != 4u) & (t != 8u);
+  switch (g_filter) {
+    case 1:
+      return 1;
+    case 2:
+      return (((v >> (2 * (p - 2))) & 3u) + ((v >> (2 * (p - 3))) & 3u)) != 0;
+    case 3: {
+      uint32_t x = v;
+      int ok = 1;
+      for (int i = 0; i < p - 2; i++) {
+        ok &= (x & 0xFu) != 0;
+        x >>= 2;
+      }
+      return ok & (t != 0) & (t != 4u);
+    }
+    default:
+      return (t != 0) & (t != 4u) & (t != 8u);
+  }
 }
 
 /* GPU_HPCEncoding with the per-read start index (gkc_cuda.cu:178-190; the

@@ -54,6 +54,9 @@ typedef struct {
 } orc_poslists;
 
 int orc_version(void);
+/* Minimizer filter for later calls: 0 new_filter2 (default), 1 every p-mer,
+ * 2 new_filter, 3 sign_filter (the reference's FILTER_KERNEL variants). */
+void orc_set_filter(int filter);
 
 /* Run-collapse of each read (HPC).  out_reads uses the input CSR layout;
  * out_len[r] = number of runs; orig_pos[offs[r] + j] = in-read index of the

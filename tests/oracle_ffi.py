@@ -80,14 +80,30 @@ def oracle():
     return _orc
 
 
-def ref_available():
-    return os.path.exists(REF_SO)
+# the reference built as shipped (new_filter2) and with its other FILTER_KERNEL variants
+REF_FILTER_SO = {0: REF_SO, 1: REF_SO.replace("libgkcref", "libgkcref_mm_filter"),
+                 2: REF_SO.replace("libgkcref", "libgkcref_new_filter"),
+                 3: REF_SO.replace("libgkcref", "libgkcref_sign_filter")}
+_refs = {}
 
 
-def reference():
+def ref_available(filter_id=0):
+    return os.path.exists(REF_FILTER_SO[filter_id])
+
+
+def set_filter(filter_id):
+    """Minimizer filter of the C restatement for later calls (0 = new_filter2)."""
+    lib = oracle()
+    lib.orc_set_filter.argtypes = [C.c_int]
+    lib.orc_set_filter(int(filter_id))
+
+
+def reference(filter_id=0):
     global _ref
-    if _ref is None:
-        lib = C.CDLL(REF_SO)
+    if filter_id in _refs:
+        return _refs[filter_id]
+    if filter_id != 0 or _ref is None:
+        lib = C.CDLL(REF_FILTER_SO[filter_id])
         lib.ref_partition.argtypes = [C.c_char_p, u64p, C.c_int64, C.c_int, C.c_int, C.c_int,
                                       C.c_int, C.c_int, C.c_int, C.POINTER(RefSkms)]
         lib.ref_count_bins.argtypes = [C.POINTER(RefSkms), C.c_int, C.c_int, C.c_int,
@@ -96,8 +112,10 @@ def reference():
                                      C.c_int, C.c_int, C.c_int, u64p, u64p]
         lib.ref_skms_free.argtypes = [C.POINTER(RefSkms)]
         lib.ref_counts_free.argtypes = [C.POINTER(RefCounts)]
-        _ref = lib
-    return _ref
+        _refs[filter_id] = lib
+        if filter_id == 0:
+            _ref = lib
+    return _refs.get(filter_id, _ref)
 
 
 class Skms:
@@ -213,8 +231,8 @@ def oracle_subsample(reads, offs, k, p, mod):
     return res
 
 
-def ref_partition(reads, offs, k, p, hpc, nbins, batch_reads=2048, n_threads=4):
-    lib = reference()
+def ref_partition(reads, offs, k, p, hpc, nbins, batch_reads=2048, n_threads=4, filter_id=0):
+    lib = reference(filter_id)
     reads = np.ascontiguousarray(reads, dtype=np.uint8)
     offs = np.ascontiguousarray(offs, dtype=np.uint64)
     s = RefSkms()

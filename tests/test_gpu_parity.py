@@ -242,3 +242,40 @@ def test_sort_fallback_forced(ctx, seed, n, lo, hi, k, p, hpc, nb, monkeypatch):
     lib_partition(ctx, reads, offs, k, p, hpc, nb)
     got, _ = lib_counts(ctx, k, nb)
     assert_counts_equal(got, F.oracle_count_bins(o, k, nb))
+
+
+@pytest.mark.parametrize("filter_id", [G.FILTER_ALL, G.FILTER_NEW, G.FILTER_SIGNATURE, G.FILTER_NEW2])
+def test_minimizer_filters_vs_oracle(filter_id):
+    """Each minimizer filter the reference can be built with (FILTER_KERNEL),
+    chosen at run time: batched and plain partitions, counts and per-window
+    minimizers against the oracle with the same filter."""
+    import torch
+    reads, offs = random_reads(60 + filter_id, 300, 40, 800)
+    k, p, hpc, nb = 31, 11, 0, 64
+    try:
+        F.set_filter(filter_id)
+        o = F.oracle_partition(reads, offs, k, p, hpc, nb)
+        want = F.oracle_count_bins(o, k, nb)
+        with G.Context(0) as c:
+            c.set_filter(filter_id)
+            skm, _ = lib_partition(c, reads, offs, k, p, hpc, nb)
+            assert skm.multisets(nb) == o.multisets(nb)
+            got, _ = lib_counts(c, k, nb)
+            assert_counts_equal(got, want)
+            d_reads = torch.from_numpy(reads).cuda()
+            d_offs = torch.from_numpy(offs.view(np.int64)).cuda()
+            pv, cv = c.pipeline_device(d_reads, len(reads), d_offs, len(offs) - 1, G.params(k, p, nb, hpc),
+                                       mode=G.MODE_PLAIN)
+            bin_off, keys, counts = c.count_copy_out(cv)
+            assert np.array_equal(keys[:, 0], want["keys_lo"]) and np.array_equal(counts, want["counts"])
+            nbt = len(reads)
+            d_mm = torch.zeros(nbt, dtype=torch.int32, device="cuda")
+            c.minimizers_device(d_reads.data_ptr(), nbt, d_offs.data_ptr(), len(offs) - 1, G.params(k, p, 1),
+                                d_mm.data_ptr(), None, None)
+            mm = d_mm.cpu().numpy().view(np.uint32)
+            for i in range(0, len(offs) - 1, 7):
+                b, e = int(offs[i]), int(offs[i + 1])
+                want_mm = F.oracle_minimizers(reads[b:e], k, p)
+                assert np.array_equal(mm[b:b + len(want_mm)], want_mm)
+    finally:
+        F.set_filter(G.FILTER_NEW2)

@@ -125,3 +125,23 @@ def test_oracle_short_reads_produce_nothing():
     offs = np.array([0, 5, 30], np.uint64)
     s = F.oracle_partition(reads, offs, 31, 11, 0, 16)
     assert len(s.bin) == 0
+
+
+@pytest.mark.parametrize("filter_id", [1, 2, 3])
+def test_oracle_filters_match_reference(filter_id):
+    """Every FILTER_KERNEL variant of the reference, built from its sources,
+    against the restatement with the same filter."""
+    if not F.ref_available(filter_id):
+        pytest.skip("reference tree absent: the per-filter builds were not made")
+    reads, offs = _random_reads(40 + filter_id, 300, 31, 600)  # reads of at least k bases
+    try:
+        F.set_filter(filter_id)
+        for k, p, hpc in [(31, 11, 0), (21, 9, 1)]:
+            o = F.oracle_partition(reads, offs, k, p, hpc, 16)
+            r = F.ref_partition(reads, offs, k, p, hpc, 16, batch_reads=41, filter_id=filter_id)
+            assert o.multisets(16) == r.multisets(16)
+            F.set_filter(0)
+            assert o.multisets(16) != F.oracle_partition(reads, offs, k, p, hpc, 16).multisets(16)
+            F.set_filter(filter_id)
+    finally:
+        F.set_filter(0)
