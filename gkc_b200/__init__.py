@@ -44,6 +44,11 @@ class PartitionView(C.Structure):
                 ("hpc_offs", C.c_void_p), ("hpc_orig_pos", C.c_void_p)]
 
 
+class BalanceStats(C.Structure):
+    _fields_ = [("total", C.c_uint64), ("mean", C.c_uint64), ("max", C.c_uint64), ("min", C.c_uint64),
+                ("variance", C.c_double), ("stdev", C.c_double), ("cv", C.c_double)]
+
+
 class CountView(C.Structure):
     _fields_ = [("n_distinct", C.c_uint64), ("n_kmers", C.c_uint64), ("nbins", C.c_uint32),
                 ("key_words", C.c_int), ("bin_off", C.c_void_p), ("keys", C.c_void_p),
@@ -95,6 +100,7 @@ SIGNATURES = [
     ("gkc_partition_device", C.c_int, [vp, P(Params), vp, u64, vp, u64, P(PartitionView)]),
     ("gkc_partition_host", C.c_int, [vp, P(Params), vp, vp, u64, P(PartitionView)]),
     ("gkc_partition_copy_out", C.c_int, [vp, vp, vp, vp, vp, vp]),
+    ("gkc_partition_balance", C.c_int, [vp, vp, u32, P(BalanceStats)]),
     ("gkc_count_device", C.c_int, [vp, P(Params), C.c_int, P(CountView)]),
     ("gkc_count_superkmers_host", C.c_int, [vp, C.c_int, vp, vp, u64, C.c_int, P(u64)]),
     ("gkc_count_copy_out", C.c_int, [vp, vp, vp, vp]),
@@ -235,6 +241,17 @@ class Context:
         self._check(self._L.gkc_partition_copy_out(self.h, _ptr(bin_off), _ptr(lens), _ptr(boff),
                                                    _ptr(packed), _ptr(mm)), "partition_copy_out")
         return bin_off, lens[:n], boff[:n], packed[:int(view.n_packed_bytes)], mm[:n]
+
+    def partition_balance(self, view):
+        """-> (bases per bin, summary dict) of the context's partition (the
+        view its partition call returned): the per-bin superkmer bases and the
+        avg / max / min / var / std / cv summary of the reference's
+        partition-size report."""
+        nbins = int(view.nbins)
+        sizes = np.zeros(max(nbins, 1), np.uint64)
+        st = BalanceStats()
+        self._check(self._L.gkc_partition_balance(self.h, _ptr(sizes), len(sizes), C.byref(st)), "partition_balance")
+        return sizes[:nbins], {f: getattr(st, f) for f, _ in BalanceStats._fields_}
 
     # ---- count ----
     def count_device(self, prm, mode=MODE_BATCHED):

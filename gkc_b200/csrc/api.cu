@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -1015,6 +1016,47 @@ gkc_status gkc_partition_copy_out(gkc_ctx *c, uint64_t *bin_skm_off, uint32_t *s
     }
   }
   CK(cudaStreamSynchronize(c->st));
+  return GKC_OK;
+}
+
+// The partition kernels already hold, per bin, the superkmer prefix and the
+// k-mer prefix; a superkmer of w k-mers has w + k - 1 bases, so the bases of
+// bin b are its k-mers plus (k - 1) per superkmer.  Only the two prefix
+// arrays (nbins + 1 words each) cross to the host.
+gkc_status gkc_partition_balance(gkc_ctx *c, uint64_t *bin_bases, uint32_t capacity,
+                                 gkc_balance_stats *st) {
+  if (!c || !c->have_part) return GKC_ERR_INVALID_ARG;
+  cudaSetDevice(c->dev);
+  const gkc_partition_view &v = c->pv;
+  const uint32_t nb = v.nbins;
+  if (bin_bases && capacity < nb)
+    return ctx_fail(c, GKC_ERR_CAPACITY, "bin_bases holds " + std::to_string(capacity) + " entries, the partition has " +
+                                             std::to_string(nb) + " bins");
+  std::vector<uint64_t> so(nb + 1), ko(nb + 1);
+  CK(cudaMemcpyAsync(so.data(), v.bin_skm_off, (nb + 1) * 8, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(ko.data(), v.bin_kmer_off, (nb + 1) * 8, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  const uint64_t km1 = (uint64_t)(c->pp.k - 1);
+  gkc_balance_stats s{};
+  s.min = ~0ull;
+  std::vector<uint64_t> sz(nb);
+  for (uint32_t b = 0; b < nb; b++) {
+    sz[b] = (ko[b + 1] - ko[b]) + km1 * (so[b + 1] - so[b]);
+    s.total += sz[b];
+    s.max = std::max(s.max, sz[b]);
+    s.min = std::min(s.min, sz[b]);
+  }
+  s.mean = nb ? s.total / nb : 0;
+  double acc = 0.0;
+  for (uint32_t b = 0; b < nb; b++) {
+    const uint64_t d = sz[b] - s.mean;  // wraps below the mean; the square is the same mod 2^64
+    acc += (double)(d * d);
+  }
+  s.variance = nb ? acc / nb : 0.0;
+  s.stdev = std::sqrt(s.variance);
+  s.cv = s.stdev / (double)s.mean;
+  if (bin_bases) std::copy(sz.begin(), sz.end(), bin_bases);
+  if (st) *st = s;
   return GKC_OK;
 }
 

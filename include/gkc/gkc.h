@@ -132,6 +132,23 @@ gkc_status gkc_partition_host(gkc_ctx *ctx, const gkc_params *prm, const char *r
 gkc_status gkc_partition_copy_out(gkc_ctx *ctx, uint64_t *bin_skm_off, uint32_t *skm_len,
                                   uint64_t *skm_byte_off, uint8_t *packed, uint32_t *minimizer);
 
+/* Balance of the context's partition.  bin_bases[b] (room for `capacity`
+ * entries, at least nbins, or NULL) = the bases of the superkmers of bin b,
+ * each superkmer counted with its k-1 overlap (reference: the part_sizes
+ * that CalcSKMPartSize_instream, gkc_cuda.cu:350-365, adds up over all
+ * batches).  The summary is the one
+ * calVarStdev (experiment.cpp:18-37) logs: mean is the integer quotient,
+ * variance the mean of (size - mean)^2 with each square taken in 64-bit
+ * unsigned arithmetic and summed in double, in bin order.  `total` is the
+ * exact 64-bit sum; the reference accumulates it in an int, so its figures
+ * agree only while the total is below 2^31. */
+typedef struct gkc_balance_stats {
+  uint64_t total, mean, max, min;
+  double variance, stdev, cv; /* cv = stdev / mean */
+} gkc_balance_stats;
+gkc_status gkc_partition_balance(gkc_ctx *ctx, uint64_t *bin_bases, uint32_t capacity,
+                                 gkc_balance_stats *stats);
+
 /* ---- counting (reference: kmc_counting_GPU kmer_counting.cu:59-199, per bin) ---- */
 /* Counts the context's current partition, all bins. */
 gkc_status gkc_count_device(gkc_ctx *ctx, const gkc_params *prm, gkc_mode mode,

@@ -6,6 +6,7 @@
  */
 #include "gkc_oracle.h"
 
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -470,4 +471,42 @@ int orc_subsample_positions(const uint8_t *reads, const uint64_t *offs, int64_t 
 void orc_poslists_free(orc_poslists *p) {
   free(p->keys_lo); free(p->keys_hi); free(p->pos_off); free(p->pos);
   memset(p, 0, sizeof(*p));
+}
+
+/* ---- partition balance ------------------------------------------------ */
+
+/* CalcSKMPartSize_instream (gkc_cuda.cu:350-365): a superkmer between
+ * boundaries s and e adds e - s + k - 1 bases, i.e. its length, to the bin
+ * of its first minimizer. */
+void orc_partition_sizes(const orc_skms *s, int nbins, uint64_t *sizes) {
+  for (int b = 0; b < nbins; b++) sizes[b] = 0;
+  for (uint64_t i = 0; i < s->n_skm; i++) sizes[s->bin[i]] += s->len[i];
+}
+
+/* calVarStdev (experiment.cpp:18-37): integer mean, then the squares of
+ * size - mean in unsigned 64-bit arithmetic (a size below the mean wraps,
+ * its square does not change mod 2^64), each converted to double and summed
+ * in bin order; variance = sum / n, cv = stdev / mean.  The reference's
+ * std::accumulate starts from an int, so its total wraps at 2^31; here the
+ * total is the exact sum. */
+void orc_balance_stats(const uint64_t *sizes, int n, orc_balance *out) {
+  uint64_t sum = 0, mx = 0, mn = UINT64_MAX;
+  for (int i = 0; i < n; i++) {
+    sum += sizes[i];
+    if (sizes[i] > mx) mx = sizes[i];
+    if (sizes[i] < mn) mn = sizes[i];
+  }
+  const uint64_t mean = n ? sum / (uint64_t)n : 0;
+  double acc = 0.0;
+  for (int i = 0; i < n; i++) {
+    uint64_t d = sizes[i] - mean;
+    acc += (double)(d * d);
+  }
+  out->total = sum;
+  out->mean = mean;
+  out->max = mx;
+  out->min = mn;
+  out->variance = n ? acc / n : 0.0;
+  out->stdev = sqrt(out->variance);
+  out->cv = out->stdev / (double)mean;
 }

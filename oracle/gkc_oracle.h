@@ -92,6 +92,17 @@ int orc_subsample_positions(const uint8_t *reads, const uint64_t *offs, int64_t 
                             int k, int p, uint32_t mod, orc_poslists *out);
 void orc_poslists_free(orc_poslists *p);
 
+/* Partition balance.  sizes[b] = bases of the superkmers of bin b, each
+ * superkmer with its k-1 overlap (the part_sizes of CalcSKMPartSize_instream,
+ * gkc_cuda.cu:350-365); the summary calVarStdev logs (experiment.cpp:18-37)
+ * with the total kept in 64 bits. */
+typedef struct {
+  uint64_t total, mean, max, min;
+  double variance, stdev, cv;
+} orc_balance;
+void orc_partition_sizes(const orc_skms *s, int nbins, uint64_t *sizes);
+void orc_balance_stats(const uint64_t *sizes, int n, orc_balance *out);
+
 void orc_free(void *p);
 
 #ifdef __cplusplus

@@ -35,6 +35,15 @@ int ref_partition(const char *reads, const uint64_t *offs, int64_t n_reads, int 
                   int hpc, int nbins, int batch_reads, int n_threads, ref_skms *out);
 void ref_skms_free(ref_skms *s);
 
+// Bases of the superkmers of each bin as CalcSKMPartSize_instream
+// (gkc_cuda.cu:350-365) adds them up over the batches; nbins <= 512.
+int ref_partition_sizes(const char *reads, const uint64_t *offs, int64_t n_reads, int k, int p,
+                        int hpc, int nbins, int batch_reads, int n_threads, uint64_t *sizes);
+
+// The report calVarStdev (experiment.cpp:18-37) logs for the sizes, as text
+// (its two log lines); returns the text length.
+int ref_cal_var_stdev(const uint64_t *sizes, int n, char *buf, int cap);
+
 // Per-bin counting through kmc_counting_GPU; the sorted keys and run lengths
 // it computes (and discards) are captured.  k <= 32.
 int ref_count_bins(const ref_skms *s, int k, int nbins, int n_threads, ref_counts *out);

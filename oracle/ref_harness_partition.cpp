@@ -4,6 +4,7 @@
 // as process_reads_count does (experiment.cpp:85-88).
 #include "ref_shim.h"
 
+using std::atomic;  // CalcSKMPartSize_instream's signature names atomic<size_t>
 #include "ref_kernels.inc"  // generated from the reference by extract_ref.py
 
 #include <cassert>
@@ -17,8 +18,12 @@
 
 namespace {
 
+// One batch through the reference kernels; the superkmers go to the stores,
+// or, with part_sizes set, only their bases per bin to CalcSKMPartSize_instream
+// (the process_func of process_reads_v2, experiment.cpp:51).
 void run_batch(const char *reads, const uint64_t *offs, int64_t beg, int64_t end, int k, int p,
-               bool hpc, std::vector<SKMStore *> &stores) {
+               bool hpc, std::vector<SKMStore *> &stores, std::atomic<size_t> *part_sizes = nullptr,
+               int nbins = 0) {
   T_read_cnt cnt = (T_read_cnt)(end - beg);
   size_t bsize = offs[end] - offs[beg];
   std::vector<char> d_reads(reads + offs[beg], reads + offs[end]);
@@ -38,6 +43,10 @@ void run_batch(const char *reads, const uint64_t *offs, int64_t beg, int64_t end
   }
   GPU_GenMinimizer(cnt, d_len.data(), d_reads.data(), d_offs.data(), d_mm.data(), k, p);
   GPU_GenSKM(cnt, d_len.data(), d_offs.data(), d_mm.data(), d_skm.data(), k, p);
+  if (part_sizes) {
+    CalcSKMPartSize_instream(cnt, d_skm.data(), d_offs.data(), d_mm.data(), nbins, k, part_sizes);
+    return;
+  }
   SKMStore::add_skms(stores, (T_kvalue)k, cnt, d_reads.data(), d_offs.data(), d_skm.data(),
                      d_mm.data());
 }
@@ -88,6 +97,26 @@ extern "C" int ref_partition(const char *reads, const uint64_t *offs, int64_t n_
   std::copy(len.begin(), len.end(), out->len);
   std::copy(boff.begin(), boff.end(), out->byte_off);
   std::copy(bytes.begin(), bytes.end(), out->bytes);
+  return 0;
+}
+
+extern "C" int ref_partition_sizes(const char *reads, const uint64_t *offs, int64_t n_reads, int k,
+                                   int p, int hpc, int nbins, int batch_reads, int n_threads,
+                                   uint64_t *sizes) {
+  if (nbins < 1 || nbins > 512) return 1;  // experiment.cpp:57 holds 512 counters
+  std::atomic<size_t> part[512];
+  for (int i = 0; i < nbins; i++) part[i] = 0;
+  if (batch_reads < 1) batch_reads = 2048;
+  std::vector<SKMStore *> none;
+  {
+    ThreadPool<void> tp(n_threads < 1 ? 1 : n_threads);
+    for (int64_t b = 0; b < n_reads; b += batch_reads) {
+      int64_t e = std::min<int64_t>(n_reads, b + batch_reads);
+      tp.commit_task([=, &none, &part]() { run_batch(reads, offs, b, e, k, p, hpc != 0, none, part, nbins); });
+    }
+    tp.finish();
+  }
+  for (int i = 0; i < nbins; i++) sizes[i] = part[i];
   return 0;
 }
 

@@ -112,6 +112,9 @@ def reference(filter_id=0):
                                      C.c_int, C.c_int, C.c_int, u64p, u64p]
         lib.ref_skms_free.argtypes = [C.POINTER(RefSkms)]
         lib.ref_counts_free.argtypes = [C.POINTER(RefCounts)]
+        lib.ref_partition_sizes.argtypes = [C.c_char_p, u64p, C.c_int64, C.c_int, C.c_int, C.c_int,
+                                            C.c_int, C.c_int, C.c_int, u64p]
+        lib.ref_cal_var_stdev.argtypes = [u64p, C.c_int, C.c_char_p, C.c_int]
         _refs[filter_id] = lib
         if filter_id == 0:
             _ref = lib
@@ -278,3 +281,53 @@ def ref_pipeline(reads, offs, k, p, hpc, nbins, batch_reads=2048, n_threads=1):
                           int(hpc), nbins, batch_reads, n_threads, _ptr(d, u64p), _ptr(km, u64p))
     assert rc == 0
     return int(d[0]), int(km[0])
+
+
+class OrcBalance(C.Structure):
+    _fields_ = [("total", C.c_uint64), ("mean", C.c_uint64), ("max", C.c_uint64), ("min", C.c_uint64),
+                ("variance", C.c_double), ("stdev", C.c_double), ("cv", C.c_double)]
+
+
+def oracle_partition_sizes(skms, nbins):
+    """Bases per bin of an oracle (or any) partition: the sum of its superkmer lengths."""
+    sizes = np.zeros(nbins, np.uint64)
+    np.add.at(sizes, np.asarray(skms.bin, np.int64), np.asarray(skms.len, np.uint64))
+    return sizes
+
+
+def oracle_balance(sizes):
+    lib = oracle()
+    lib.orc_balance_stats.argtypes = [u64p, C.c_int, C.POINTER(OrcBalance)]
+    sizes = np.ascontiguousarray(sizes, np.uint64)
+    st = OrcBalance()
+    lib.orc_balance_stats(_ptr(sizes, u64p), len(sizes), C.byref(st))
+    return {f: getattr(st, f) for f, _ in OrcBalance._fields_}
+
+
+def balance_report(st):
+    """The text calVarStdev logs (experiment.cpp:30-35) for a summary:
+    integers as they are, doubles as an ostream prints them by default
+    (six significant digits, printf %g)."""
+    return ("SKM TOT_LEN=%d\n" % st["total"] +
+            "AVG=%d\tMAX=%d\tmin=%d\tvar=%g\tSTD=%g\tCV=%g\n\n"
+            % (st["mean"], st["max"], st["min"], st["variance"], st["stdev"], st["cv"]))
+
+
+def ref_partition_sizes(reads, offs, k, p, hpc, nbins, batch_reads=2048, n_threads=4, filter_id=0):
+    lib = reference(filter_id)
+    reads = np.ascontiguousarray(reads, np.uint8)
+    offs = np.ascontiguousarray(offs, np.uint64)
+    sizes = np.zeros(nbins, np.uint64)
+    rc = lib.ref_partition_sizes(reads.tobytes(), _ptr(offs, u64p), len(offs) - 1, k, p, int(hpc),
+                                 nbins, batch_reads, n_threads, _ptr(sizes, u64p))
+    assert rc == 0, rc
+    return sizes
+
+
+def ref_balance_report(sizes):
+    lib = reference()
+    sizes = np.ascontiguousarray(sizes, np.uint64)
+    buf = C.create_string_buffer(1024)
+    n = lib.ref_cal_var_stdev(_ptr(sizes, u64p), len(sizes), buf, len(buf))
+    assert n < len(buf)
+    return buf.value.decode()

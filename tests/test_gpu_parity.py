@@ -279,3 +279,35 @@ def test_minimizer_filters_vs_oracle(filter_id):
                 assert np.array_equal(mm[b:b + len(want_mm)], want_mm)
     finally:
         F.set_filter(G.FILTER_NEW2)
+
+
+@pytest.mark.parametrize("name", sorted(GC.index()["full"].keys()))
+def test_partition_balance_golden(ctx, name):
+    """Per-bin superkmer bases (CalcSKMPartSize_instream) and the calVarStdev
+    summary of the context's partition: the bases against the fixture's
+    superkmers, the summary against the oracle's, bit for bit."""
+    meta, d = GC.full_case(name)
+    k, p, hpc, nb = meta["k"], meta["p"], meta["hpc"], meta["nbins"]
+    _, v = lib_partition(ctx, d["reads"], d["offs"], k, p, hpc, nb)
+    sizes, st = ctx.partition_balance(v)
+    want = np.zeros(nb, np.uint64)
+    np.add.at(want, d["skm_bin"].astype(np.int64), d["skm_len"].astype(np.uint64))
+    assert np.array_equal(sizes, want)
+    assert st == F.oracle_balance(want)
+
+
+@pytest.mark.parametrize("mode", [G.MODE_BATCHED, G.MODE_PLAIN])
+def test_partition_balance_pipeline(ctx, mode):
+    """After the whole pipeline in either mode, with HPC, the balance figures
+    come from that run's partition."""
+    import torch
+    reads, offs = random_reads(70 + mode, 400, 30, 900)
+    k, p, hpc, nb = 25, 9, 1, 37
+    o = F.oracle_partition(reads, offs, k, p, hpc, nb)
+    want = F.oracle_partition_sizes(o, nb)
+    d_reads = torch.from_numpy(reads).cuda()
+    d_offs = torch.from_numpy(offs.view(np.int64)).cuda()
+    pv, _ = ctx.pipeline_device(d_reads, len(reads), d_offs, len(offs) - 1, G.params(k, p, nb, hpc), mode=mode)
+    sizes, st = ctx.partition_balance(pv)
+    assert np.array_equal(sizes, want)
+    assert st == F.oracle_balance(want)

@@ -145,3 +145,40 @@ def test_oracle_filters_match_reference(filter_id):
             F.set_filter(filter_id)
     finally:
         F.set_filter(0)
+
+
+@pytest.mark.skipif(not F.ref_available(), reason="reference harness not built here")
+@pytest.mark.parametrize("seed,k,p,hpc,nb", [(50, 31, 11, 0, 256), (51, 21, 9, 1, 31), (52, 17, 7, 0, 5)])
+def test_oracle_partition_sizes_match_reference(seed, k, p, hpc, nb):
+    """Bases per bin as CalcSKMPartSize_instream adds them up, against the
+    restatement's partition."""
+    reads, offs = _random_reads(seed, 200, k, 700)
+    want = F.ref_partition_sizes(reads, offs, k, p, hpc, nb, batch_reads=53)
+    got = F.oracle_partition_sizes(F.oracle_partition(reads, offs, k, p, hpc, nb), nb)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.skipif(not F.ref_available(), reason="reference harness not built here")
+def test_oracle_balance_report_matches_reference():
+    """The avg / max / min / var / std / cv report of calVarStdev, as the text
+    it logs, for size vectors below the reference's int-total limit."""
+    r = np.random.default_rng(11)
+    cases = [np.array([10, 20, 30, 45], np.uint64), np.full(64, 1000, np.uint64),
+             np.array([7], np.uint64), r.integers(0, 100000, 256).astype(np.uint64),
+             r.integers(1, 1 << 22, 500).astype(np.uint64)]
+    for sizes in cases:
+        assert int(sizes.sum()) < 2 ** 31
+        assert F.balance_report(F.oracle_balance(sizes)) == F.ref_balance_report(sizes)
+
+
+def test_oracle_partition_sizes_from_golden():
+    """Per-bin bases of the fixtures' partitions equal the superkmer lengths
+    each bin holds plus nothing else (the fixtures pin the partition)."""
+    for name in FULL:
+        meta, d = G.full_case(name)
+        nb = meta["nbins"]
+        skm = F.oracle_partition(d["reads"], d["offs"], meta["k"], meta["p"], meta["hpc"], nb)
+        sizes = F.oracle_partition_sizes(skm, nb)
+        want = np.zeros(nb, np.uint64)
+        np.add.at(want, d["skm_bin"].astype(np.int64), d["skm_len"].astype(np.uint64))
+        assert np.array_equal(sizes, want)
