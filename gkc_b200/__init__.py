@@ -101,6 +101,8 @@ SIGNATURES = [
     ("gkc_partition_host", C.c_int, [vp, P(Params), vp, vp, u64, P(PartitionView)]),
     ("gkc_partition_copy_out", C.c_int, [vp, vp, vp, vp, vp, vp]),
     ("gkc_partition_balance", C.c_int, [vp, vp, u32, P(BalanceStats)]),
+    ("gkc_exchange_pack", C.c_int, [vp, u32, vp, vp, u64, vp, u64, vp, vp, vp, vp]),
+    ("gkc_partition_import", C.c_int, [vp, P(Params), u32, vp, vp, vp, vp, vp, P(PartitionView)]),
     ("gkc_count_device", C.c_int, [vp, P(Params), C.c_int, P(CountView)]),
     ("gkc_count_superkmers_host", C.c_int, [vp, C.c_int, vp, vp, u64, C.c_int, P(u64)]),
     ("gkc_count_copy_out", C.c_int, [vp, vp, vp, vp]),
@@ -252,6 +254,32 @@ class Context:
         st = BalanceStats()
         self._check(self._L.gkc_partition_balance(self.h, _ptr(sizes), len(sizes), C.byref(st)), "partition_balance")
         return sizes[:nbins], {f: getattr(st, f) for f, _ in BalanceStats._fields_}
+
+    # ---- superkmer exchange (bin sharding over several GPUs) ----
+    def exchange_pack(self, view, bin_lo, d_send_desc, d_send_bytes):
+        """Runs of the context's partition per destination (owner r holds bins
+        [bin_lo[r], bin_lo[r+1])) written to the two device tensors;
+        -> (skm_split, byte_split, bin_skm, bin_kmers) numpy arrays."""
+        bin_lo = np.ascontiguousarray(bin_lo, np.uint32)
+        nd, nb = len(bin_lo) - 1, int(view.nbins)
+        skm_split, byte_split = np.zeros(nd, np.uint64), np.zeros(nd, np.uint64)
+        bin_skm, bin_kmers = np.zeros(max(nb, 1), np.uint64), np.zeros(max(nb, 1), np.uint64)
+        self._check(self._L.gkc_exchange_pack(self.h, nd, _ptr(bin_lo), _ptr(d_send_desc), d_send_desc.numel(),
+                                              _ptr(d_send_bytes), d_send_bytes.numel(), _ptr(skm_split),
+                                              _ptr(byte_split), _ptr(bin_skm), _ptr(bin_kmers)), "exchange_pack")
+        return skm_split, byte_split, bin_skm[:nb], bin_kmers[:nb]
+
+    def partition_import(self, prm, seg_bin_skm, seg_bin_kmers, seg_bytes, d_desc, d_bytes):
+        """The senders' runs (concatenated in sender order in the two device
+        tensors) as this context's partition of prm.nbins local bins."""
+        seg_bin_skm = np.ascontiguousarray(seg_bin_skm, np.uint64)
+        seg_bin_kmers = np.ascontiguousarray(seg_bin_kmers, np.uint64)
+        seg_bytes = np.ascontiguousarray(seg_bytes, np.uint64)
+        v = PartitionView()
+        self._check(self._L.gkc_partition_import(self.h, C.byref(prm), len(seg_bytes), _ptr(seg_bin_skm),
+                                                 _ptr(seg_bin_kmers), _ptr(seg_bytes), _ptr(d_desc),
+                                                 _ptr(d_bytes), C.byref(v)), "partition_import")
+        return v
 
     # ---- count ----
     def count_device(self, prm, mode=MODE_BATCHED):

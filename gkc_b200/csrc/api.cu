@@ -1002,8 +1002,12 @@ gkc_status gkc_partition_copy_out(gkc_ctx *c, uint64_t *bin_skm_off, uint32_t *s
   const gkc_partition_view &v = c->pv;
   if (bin_skm_off)
     CK(cudaMemcpyAsync(bin_skm_off, v.bin_skm_off, (v.nbins + 1) * 8, cudaMemcpyDeviceToHost, c->st));
-  if (minimizer && v.n_superkmers)
-    CK(cudaMemcpyAsync(minimizer, v.skm_minimizer, v.n_superkmers * 4, cudaMemcpyDeviceToHost, c->st));
+  if (minimizer && v.n_superkmers) {
+    if (v.skm_minimizer)
+      CK(cudaMemcpyAsync(minimizer, v.skm_minimizer, v.n_superkmers * 4, cudaMemcpyDeviceToHost, c->st));
+    else  // an imported partition carries no minimizers
+      memset(minimizer, 0xFF, v.n_superkmers * 4);
+  }
   if (packed && v.n_packed_bytes)
     CK(cudaMemcpyAsync(packed, v.packed, v.n_packed_bytes, cudaMemcpyDeviceToHost, c->st));
   if ((skm_len || skm_byte_off) && v.n_superkmers) {

@@ -128,7 +128,8 @@ gkc_status gkc_partition_host(gkc_ctx *ctx, const gkc_params *prm, const char *r
                               const uint64_t *offs, uint64_t n_reads, gkc_partition_view *out);
 /* Copies the context's partition to host arrays sized from the view:
  * bin_skm_off[nbins+1], skm_len[n_superkmers], skm_byte_off[n_superkmers]
- * (into `packed`), packed[n_packed_bytes], minimizer[n_superkmers] (may be NULL). */
+ * (into `packed`), packed[n_packed_bytes], minimizer[n_superkmers] (may be NULL;
+ * all 0xFFFFFFFF for an imported partition, which carries none). */
 gkc_status gkc_partition_copy_out(gkc_ctx *ctx, uint64_t *bin_skm_off, uint32_t *skm_len,
                                   uint64_t *skm_byte_off, uint8_t *packed, uint32_t *minimizer);
 
@@ -148,6 +149,35 @@ typedef struct gkc_balance_stats {
 } gkc_balance_stats;
 gkc_status gkc_partition_balance(gkc_ctx *ctx, uint64_t *bin_bases, uint32_t capacity,
                                  gkc_balance_stats *stats);
+
+/* ---- superkmer exchange for bin sharding over several GPUs (no reference
+ *      counterpart: the reference runs on one GPU).  Every GPU partitions
+ *      its own reads; owner r of n_dest holds bins [bin_lo[r], bin_lo[r+1])
+ *      and counts them after the exchange.  The transfer itself (an
+ *      all-to-all of descriptors and one of bytes, split as returned) is the
+ *      caller's. ---- */
+/* Sender side, on the context's partition: for each destination in turn,
+ * its superkmers' descriptors (bin order; byte offsets relative to that
+ * destination's run of bytes) go to d_send_desc and their packed bytes to
+ * d_send_bytes; skm_split and byte_split (n_dest entries each) receive the
+ * run sizes, bin_skm and bin_kmers (nbins entries each, may be NULL) the
+ * superkmers and k-mers of every bin.  Capacities equal to the view's
+ * n_superkmers and n_packed_bytes always suffice. */
+gkc_status gkc_exchange_pack(gkc_ctx *ctx, uint32_t n_dest, const uint32_t *bin_lo,
+                             uint64_t *d_send_desc, uint64_t desc_capacity, uint8_t *d_send_bytes,
+                             uint64_t bytes_capacity, uint64_t *skm_split, uint64_t *byte_split,
+                             uint64_t *bin_skm, uint64_t *bin_kmers);
+/* Receiver side: the runs of n_src senders, concatenated in sender order in
+ * d_desc and d_bytes, become the context's partition with prm->nbins local
+ * bins, ordered by bin and, inside a bin, by sender.  seg_bin_skm and
+ * seg_bin_kmers hold n_src rows of nbins counts (the sender's bin_skm /
+ * bin_kmers for this owner's bins), seg_bytes the n_src byte-run sizes.  The
+ * inputs are copied before the call returns.  The resulting view has no
+ * minimizers (skm_minimizer is NULL); gkc_count_device counts it. */
+gkc_status gkc_partition_import(gkc_ctx *ctx, const gkc_params *prm, uint32_t n_src,
+                                const uint64_t *seg_bin_skm, const uint64_t *seg_bin_kmers,
+                                const uint64_t *seg_bytes, const uint64_t *d_desc,
+                                const uint8_t *d_bytes, gkc_partition_view *out);
 
 /* ---- counting (reference: kmc_counting_GPU kmer_counting.cu:59-199, per bin) ---- */
 /* Counts the context's current partition, all bins. */
