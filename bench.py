@@ -7,6 +7,13 @@ substitution errors; k=31, p=11, 256 bins.  Reads are generated on the device
 from a seed.  One step = the batched, graph-captured pipeline
 (partition -> expand -> sort -> count) over all reads, inputs resident in HBM.
 
+With --gpus N > 1 (one process per GPU under torchrun) every rank generates
+its own reads of the same genome (weak scaling); by default the bins are
+sharded: each rank partitions its reads, the superkmers go to the owner of
+their bin over NCCL (gkc_b200.shard), and each rank counts the bins it owns,
+so every k-mer of the job is counted once.  --multi replicas runs N
+independent single-GPU pipelines instead.
+
 Printed: one JSON line (rank 0).  `--impl reference` times the reference's own
 CPU implementation (oracle/_ref, compiled from the reference sources) on a
 bounded sample of the same workload instead.
@@ -63,6 +70,9 @@ def parse():
                     help="only the serving mix (config 5): 1000 jobs at 50/80/95%% load")
     ap.add_argument("--serve-jobs", type=int, default=None)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--multi", default=None, choices=["shard", "replicas"],
+                    help="bins sharded by owner with a superkmer exchange (default when N > 1; "
+                         "also runs with one rank when given), or independent replicas")
     return ap.parse_args()
 
 
@@ -396,6 +406,9 @@ def config_dict(args, wl, n_reads, n_bases):
          "nbins": wl["nbins"], "hpc": bool(wl["hpc"]), "seed": args.seed,
          "l2": "inputs larger than L2 (reads + superkmers + keys >> 126 MB)",
          "mode": "batched, graph-captured", "parallelism": f"weak-replicas{args.gpus}"}
+    if args.multi == "shard" or (args.gpus > 1 and args.multi is None):
+        d.update(mode="partition; superkmer all-to-all to bin owners (NCCL); owned bins counted",
+                 parallelism=f"weak-bin-shard{args.gpus}")
     if wl["gen"] == "genome":
         d.update(genome_bp=wl["genome_len"], coverage=wl["coverage"], read_len=wl["read_len"],
                  error_rate=wl["err"])
@@ -600,6 +613,158 @@ def run_ours(args, wl):
         dist.destroy_process_group()
 
 
+# ----------------------------------------------- our arm, bins sharded
+
+def run_shard(args, wl):
+    """N > 1: every rank partitions its own reads, the superkmers go to the
+    owners of their bins (three NCCL all-to-alls), every rank counts the bins
+    it owns.  One step = partition + exchange + count; the whole-job rate
+    counts the k-mers all ranks counted over the slowest rank's time."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import gkc_b200 as G
+    from gkc_b200 import shard
+
+    for key, val in (("MASTER_ADDR", "127.0.0.1"), ("MASTER_PORT", "29511"), ("RANK", "0"), ("WORLD_SIZE", "1")):
+        os.environ.setdefault(key, val)  # one rank without a launcher
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    reads, offs, n_reads, n_bases, genome = make_workload_device(wl, args.seed, rank, torch, G)
+    torch.cuda.synchronize()
+    prm = G.params(wl["k"], wl["p"], wl["nbins"], wl["hpc"])
+    ctx = G.Context(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    stage_acc = {"partition": [], "exchange": [], "count": []}
+    state = {"launches": 0}
+
+    def step(record=False, host=None):
+        ev[0].record(stream)
+        if host is None:
+            pv = ctx.partition_device(reads, n_bases, offs, n_reads, prm)
+        else:
+            pv = ctx.partition_host(host[0], host[1], prm)
+        state["launches"] += int(ctx.timings().launches)
+        own = dict(kmers=int(pv.n_kmers), skm=int(pv.n_superkmers), bases=int(pv.n_bases),
+                   reads=int(pv.n_reads), bytes=int(pv.n_packed_bytes))
+        ev[1].record(stream)
+        eng = shard.DeviceEngine(ctx, pv, dev)
+        prm_local, bounds, _ = shard.exchange_dist(eng, prm)
+        state["launches"] += eng.launches
+        ev[2].record(stream)
+        cv = ctx.count_device(prm_local, G.MODE_BATCHED)
+        state["launches"] += int(ctx.timings().launches)
+        ev[3].record(stream)
+        if record:
+            ev[3].synchronize()
+            for name, a, b in (("partition", 0, 1), ("exchange", 1, 2), ("count", 2, 3)):
+                stage_acc[name].append(ev[a].elapsed_time(ev[b]))
+        return own, cv, prm_local, bounds
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    dist.barrier()
+    state["launches"] = 0
+    with ClockSampler(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            own, cv, prm_local, bounds = step(record=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+    ms_total = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+    clocks = clk.summary()
+    launches = state["launches"]
+
+    counted = torch.tensor([int(cv.n_kmers), own["kmers"], int(cv.n_distinct)], dtype=torch.int64, device=dev)
+    dist.all_reduce(counted)
+    total_kmers, own_total, distinct_total = (int(x) for x in counted.tolist())
+    ms_step = ms_total / args.steps
+    value = total_kmers * args.steps / (ms_total / 1000.0)
+    stages = {k: float(np.mean(v)) for k, v in stage_acc.items()}
+    # HBM roofline of the count stage (the owned bins) and the partition stage
+    N, D, S = int(cv.n_kmers), int(cv.n_distinct), own["skm"]
+    model_own = algorithmic_bytes(own["bases"], own["reads"], S, own["kmers"], D, wl["k"])
+    model_cnt = algorithmic_bytes(0, 0, 0, N, D, wl["k"])
+    kernel_bytes = {"partition": model_own["partition"],
+                    "count": model_cnt["expand"] + model_cnt["sort"] + model_cnt["count"]}
+    dom = max(kernel_bytes, key=lambda s: stages[s])
+    peak, peak_kind = peaks()
+    achieved = kernel_bytes[dom] / (stages[dom] / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                "model": "fixed algorithmic-bytes model (see DESIGN.md)",
+                "model_bytes_per_launch": kernel_bytes[dom], "ms_per_launch": stages[dom]}
+    sent = 8 * S + own["bytes"]  # descriptors + packed bytes, all destinations
+    leaves = sent * (world - 1) / world
+    exchange = {"bytes_sent_per_rank": sent, "bytes_leaving_rank_est": leaves, "ms": stages["exchange"],
+                "gbs_leaving": leaves / (stages["exchange"] / 1000.0) / 1e9,
+                "peer_copy_gbs_measured": 770.0,
+                "frac_of_peer_copy": leaves / (stages["exchange"] / 1000.0) / 1e9 / 770.0}
+    result = {
+        "metric": METRIC, "value": value, "unit": "kmers/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64" if wl["k"] <= 32 else "u128", "data": "synthetic",
+        "config": config_dict(args, wl, n_reads, n_bases), "roofline": roofline, "exchange": exchange,
+        "stages_ms": stages, "gpu_launches": launches, "clocks": clocks,
+        "check": {"kmers_counted": total_kmers, "kmers_partitioned": own_total,
+                  "distinct_over_owners": distinct_total, "owned_bins_rank0": [int(bounds[0]), int(bounds[1])]},
+    }
+
+    if not args.no_e2e:
+        h_reads = torch.empty(n_bases, dtype=torch.uint8, pin_memory=True)
+        h_offs = torch.empty(n_reads + 1, dtype=torch.int64, pin_memory=True)
+        h_reads.copy_(reads[:n_bases])
+        h_offs.copy_(offs)
+        host = (h_reads.numpy(), h_offs.numpy().view(np.uint64))
+        kw = 1 if wl["k"] <= 32 else 2
+        cap = 2 * int(cv.n_distinct) + 1024
+        h_binoff = torch.empty(wl["nbins"] + 1, dtype=torch.int64, pin_memory=True)
+        h_keys = torch.empty(cap * kw, dtype=torch.int64, pin_memory=True)
+        h_counts = torch.empty(cap, dtype=torch.int32, pin_memory=True)
+        del reads
+        torch.cuda.empty_cache()
+        L = G.lib()
+
+        def e2e_step():
+            o, c, pl, _ = step(host=host)
+            assert int(c.n_distinct) <= cap
+            assert L.gkc_count_copy_out(ctx.h, h_binoff.data_ptr(), h_keys.data_ptr(), h_counts.data_ptr()) == 0
+            return c
+
+        e2e_step()
+        torch.cuda.synchronize()
+        dist.barrier()
+        ee0 = torch.cuda.Event(enable_timing=True)
+        ee1 = torch.cuda.Event(enable_timing=True)
+        ee0.record(stream)
+        for _ in range(args.e2e_steps):
+            c = e2e_step()
+        ee1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        e_ms = max_over_ranks(ee0.elapsed_time(ee1), dist, "cuda")
+        nd = int(c.n_distinct)
+        result["e2e"] = {"value": total_kmers * args.e2e_steps / (e_ms / 1000.0), "unit": "kmers/s",
+                         "h2d_bytes_per_step": n_bases + (n_reads + 1) * 8,
+                         "d2h_bytes_per_step": (int(prm_local.nbins) + 1) * 8 + nd * 8 * kw + nd * 4,
+                         "ms_per_step": e_ms / args.e2e_steps, "steps": args.e2e_steps,
+                         "api": "gkc_partition_host + exchange + gkc_count_device + gkc_count_copy_out"}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(result))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def main():
     args = parse()
     wl = WORKLOADS[args.workload]
@@ -607,6 +772,8 @@ def main():
         run_reference(args, wl)
     elif args.serve:
         run_serve(args)
+    elif args.multi == "shard" or (dist_env()[1] > 1 and args.multi is None):
+        run_shard(args, wl)
     else:
         run_ours(args, wl)
 

@@ -108,6 +108,7 @@ gkc_status gkc_exchange_pack(gkc_ctx *c, uint32_t n_dest, const uint32_t *bin_lo
   for (uint32_t r = 0; r < n_dest; r++)
     if (bin_lo[r] > bin_lo[r + 1]) return ctx_fail(c, GKC_ERR_INVALID_ARG, "bin ranges must not decrease");
   const uint64_t n = v.n_superkmers;
+  c->launches = 0;
   if (n > desc_capacity || (n && !d_send_desc))
     return ctx_fail(c, GKC_ERR_CAPACITY, "send descriptors hold " + std::to_string(desc_capacity) +
                                              " entries, the partition has " + std::to_string(n) + " superkmers");
@@ -126,6 +127,7 @@ gkc_status gkc_exchange_pack(gkc_ctx *c, uint32_t n_dest, const uint32_t *bin_lo
     k_xchg_nbytes<<<grid_for(c, n), 256, 0, c->st>>>(v.skm_desc, n, nbytes);
     scan_u64(nbytes, off, n, stmp, c->st);
     CK(cudaPeekAtLastError());
+    c->launches += 5;  // the byte-length kernel and the scan's four
     // byte offset of every destination's first superkmer (and the total)
     for (uint32_t r = 0; r <= n_dest; r++)
       CK(cudaMemcpyAsync(&hoff[r], off + seg[r], 8, cudaMemcpyDeviceToHost, c->st));
@@ -139,6 +141,7 @@ gkc_status gkc_exchange_pack(gkc_ctx *c, uint32_t n_dest, const uint32_t *bin_lo
     k_xchg_pack<<<grid_for(c, n), 256, 0, c->st>>>(v.skm_desc, v.packed, n, off, dseg, n_dest, d_send_desc,
                                                    d_send_bytes);
     CK(cudaPeekAtLastError());
+    c->launches++;
   }
   for (uint32_t r = 0; r < n_dest; r++) {
     skm_split[r] = seg[r + 1] - seg[r];
@@ -149,6 +152,8 @@ gkc_status gkc_exchange_pack(gkc_ctx *c, uint32_t n_dest, const uint32_t *bin_lo
     if (bin_kmers) bin_kmers[b] = ko[b + 1] - ko[b];
   }
   CK(cudaStreamSynchronize(c->st));
+  c->tm = gkc_timings{};
+  c->tm.launches = c->launches;
   return GKC_OK;
 }
 
@@ -212,6 +217,8 @@ gkc_status gkc_partition_import(gkc_ctx *c, const gkc_params *prm, uint32_t n_sr
     k_xchg_import<<<grid_for(c, n), 256, 0, c->st>>>(d_desc, n, pe, n_src, pd, pq, pp, nbl, dd);
     CK(cudaPeekAtLastError());
   }
+  c->tm = gkc_timings{};
+  c->tm.launches = n ? 1 : 0;
   CK(cudaStreamSynchronize(c->st));  // the host plan arrays end with this call
   gkc_partition_view &v = c->pv;
   v = gkc_partition_view{};

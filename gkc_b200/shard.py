@@ -70,6 +70,7 @@ class DeviceEngine:
     def __init__(self, ctx, view, device="cuda"):
         import torch
         self.torch, self.ctx, self.view, self.device = torch, ctx, view, device
+        self.launches = 0  # kernels the pack and the import launched
 
     def _settle(self):
         # torch's stream and the library's are different: buffers pass
@@ -82,6 +83,7 @@ class DeviceEngine:
         data = t.empty(int(self.view.n_packed_bytes), dtype=t.uint8, device=self.device)
         self._settle()  # memory torch hands out may still be read by its stream
         skm_split, byte_split, bin_skm, bin_kmers = self.ctx.exchange_pack(self.view, bounds, desc, data)
+        self.launches += int(self.ctx.timings().launches)
         data = data[:int(byte_split.sum())]
         return make_plan(t, self.device, bounds, desc, data, skm_split, byte_split, bin_skm, bin_kmers)
 
@@ -89,6 +91,7 @@ class DeviceEngine:
         self._settle()  # the received runs were written on torch's side
         self.view = self.ctx.partition_import(prm_local, seg_bin_skm, seg_bin_kmers, seg_bytes, recv_desc,
                                               recv_bytes)
+        self.launches += int(self.ctx.timings().launches)
         return self.view
 
 
