@@ -49,6 +49,12 @@ class BalanceStats(C.Structure):
                 ("variance", C.c_double), ("stdev", C.c_double), ("cv", C.c_double)]
 
 
+class DbInfo(C.Structure):
+    _fields_ = [("k", C.c_uint32), ("lut_prefix_len", C.c_uint32), ("suffix_bytes", C.c_uint32),
+                ("counter_bytes", C.c_uint32), ("min_count", C.c_uint32), ("max_count", C.c_uint32),
+                ("n_kmers", C.c_uint64), ("total_count", C.c_uint64)]
+
+
 class CountView(C.Structure):
     _fields_ = [("n_distinct", C.c_uint64), ("n_kmers", C.c_uint64), ("nbins", C.c_uint32),
                 ("key_words", C.c_int), ("bin_off", C.c_void_p), ("keys", C.c_void_p),
@@ -117,6 +123,12 @@ SIGNATURES = [
     ("gkc_hpc_device", C.c_int, [vp, vp, u64, vp, u64, vp, vp, vp]),
     ("gkc_fastx_load", C.c_int, [C.c_char_p, C.c_int, C.c_int, P(vp), P(vp), P(u64)]),
     ("gkc_fastx_free", None, [vp, vp, C.c_int]),
+    ("gkc_db_write", C.c_int, [vp, C.c_char_p, u32, u32, C.c_int]),
+    ("gkc_db_open", C.c_int, [C.c_char_p, P(vp)]),
+    ("gkc_db_close", None, [vp]),
+    ("gkc_db_get_info", C.c_int, [vp, P(DbInfo)]),
+    ("gkc_db_lookup", C.c_int, [vp, vp, u64, vp]),
+    ("gkc_db_read", C.c_int, [vp, u64, u64, vp, vp]),
     ("gkc_server_create", C.c_int, [C.c_int, u64, C.c_int, P(vp)]),
     ("gkc_server_destroy", None, [vp]),
     ("gkc_server_submit", C.c_int, [vp, P(Params), vp, vp, u64, P(u64)]),
@@ -254,6 +266,12 @@ class Context:
         st = BalanceStats()
         self._check(self._L.gkc_partition_balance(self.h, _ptr(sizes), len(sizes), C.byref(st)), "partition_balance")
         return sizes[:nbins], {f: getattr(st, f) for f, _ in BalanceStats._fields_}
+
+    def db_write(self, path, min_count=1, max_count=0xFFFFFFFF, lut_prefix_len=0):
+        """The merged count list (within [min_count, max_count]) as an on-disk
+        database <path>.gkc_pre / <path>.gkc_suf; read it with Database."""
+        self._check(self._L.gkc_db_write(self.h, os.fsencode(path), int(min_count), int(max_count),
+                                         int(lut_prefix_len)), "db_write")
 
     # ---- superkmer exchange (bin sharding over several GPUs) ----
     def exchange_pack(self, view, bin_lo, d_send_desc, d_send_bytes):
@@ -448,6 +466,53 @@ class Server:
 
 def job_hbm_estimate(prm, n_bases, n_reads):
     return int(lib().gkc_job_hbm_estimate(C.byref(prm), int(n_bases), int(n_reads)))
+
+
+class Database:
+    """Reader of an on-disk k-mer database (gkc_db_open; no GPU needed)."""
+
+    def __init__(self, path):
+        self._L = lib()
+        self.h = C.c_void_p()
+        st = self._L.gkc_db_open(os.fsencode(path), C.byref(self.h))
+        if st != 0:
+            raise GkcError(st, f"gkc_db_open {path}")
+        i = DbInfo()
+        self._L.gkc_db_get_info(self.h, C.byref(i))
+        self.info = {f: int(getattr(i, f)) for f, _ in DbInfo._fields_}
+        self.key_words = 1 if self.info["k"] <= 32 else 2
+
+    def close(self):
+        if self.h:
+            self._L.gkc_db_close(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def lookup(self, keys):
+        """Counts of keys (n x key_words uint64, or n uint64 for k <= 32); 0 if absent."""
+        keys = np.ascontiguousarray(keys, np.uint64)
+        n = keys.shape[0]
+        out = np.zeros(max(n, 1), np.uint32)
+        st = self._L.gkc_db_lookup(self.h, _ptr(keys), n, _ptr(out))
+        if st != 0:
+            raise GkcError(st, "gkc_db_lookup")
+        return out[:n]
+
+    def read(self, first=0, n=None):
+        """(keys n x key_words, counts) of records first .. first+n-1."""
+        if n is None:
+            n = self.info["n_kmers"] - first
+        keys = np.zeros((max(n, 1), self.key_words), np.uint64)
+        counts = np.zeros(max(n, 1), np.uint32)
+        st = self._L.gkc_db_read(self.h, int(first), int(n), _ptr(keys), _ptr(counts))
+        if st != 0:
+            raise GkcError(st, "gkc_db_read")
+        return keys[:n], counts[:n]
 
 
 def load_fastx(path, threads=0):

@@ -234,6 +234,37 @@ gkc_status gkc_count_superkmers_device_noalloc(int k, const uint32_t *d_skm_len,
 gkc_status gkc_count_output(gkc_ctx *ctx, uint32_t min_count, uint32_t max_count, int merged,
                             uint64_t *n_out, uint64_t *bin_off, uint64_t *keys, uint32_t *counts);
 
+/* ---- on-disk k-mer database, KMC-style: a prefix lookup table and
+ *      fixed-width (suffix, counter) records in key order (no reference
+ *      code; README.md:17 names KMC3's counting as the use case).  Files
+ *      <path>.gkc_pre and <path>.gkc_suf:
+ *        gkc_pre  "GKCP", u32 version 1, u32 k, lut_prefix_len l, suffix_bytes,
+ *                 counter_bytes, min_count, max_count, u64 n_kmers,
+ *                 total_count, u64 lut[4^l + 1] (first record of each
+ *                 prefix = key >> 2(k-l)), "GKCP"
+ *        gkc_suf  "GKCS", n_kmers x (the key's low 2(k-l) bits big-endian in
+ *                 suffix_bytes, count little-endian in counter_bytes), "GKCS"
+ *      Integers little-endian.  counter_bytes is the fewest (1..4) that hold
+ *      the largest count. ---- */
+typedef struct gkc_db gkc_db;
+typedef struct gkc_db_info {
+  uint32_t k, lut_prefix_len, suffix_bytes, counter_bytes, min_count, max_count;
+  uint64_t n_kmers, total_count;
+} gkc_db_info;
+/* Writes the merged list of the last count result (gkc_count_output with
+ * merged = 1 and the given bounds).  lut_prefix_len 0 picks about eight
+ * records per table entry; otherwise 1..13 and below k. */
+gkc_status gkc_db_write(gkc_ctx *ctx, const char *path, uint32_t min_count, uint32_t max_count,
+                        int lut_prefix_len);
+/* Host reader (maps the records; needs no GPU). */
+gkc_status gkc_db_open(const char *path, gkc_db **out);
+void gkc_db_close(gkc_db *db);
+gkc_status gkc_db_get_info(const gkc_db *db, gkc_db_info *out);
+/* counts[i] = count of keys[i] (key_words per key as in the count view), 0 if absent. */
+gkc_status gkc_db_lookup(const gkc_db *db, const uint64_t *keys, uint64_t n, uint32_t *counts);
+/* Records first .. first+n-1 as keys and counts (either may be NULL). */
+gkc_status gkc_db_read(const gkc_db *db, uint64_t first, uint64_t n, uint64_t *keys, uint32_t *counts);
+
 /* ---- whole pipeline: reads -> superkmer partitions -> sorted (k-mer, count)
  *      (reference: process_reads_count + gen_skm_and_count_with_TP,
  *      experiment.cpp:76-89,156-219) ---- */
