@@ -1,7 +1,7 @@
-"""The multi-GPU host logic of bench.py (weak replicas, no data-path
-collective) on CPU: two gloo ranks sample disjoint reads of one genome, the
-job time is the slowest rank's, and the whole-job rate counts every rank's
-units.  The reference arm runs on rank 0 only."""
+"""The multi-GPU host logic on CPU with gloo ranks: bench.py's per-rank read
+ranges, slowest-rank time and whole-job rate, the reference arm on rank 0
+only, and the bin-sharded exchange of gkc_b200.shard (every k-mer counted
+once, by the owner of its bin)."""
 import json
 import os
 import subprocess
