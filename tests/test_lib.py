@@ -87,3 +87,26 @@ def test_host_long_reads_are_deterministic():
         assert G.lib().gkc_synth_long_reads(0, 4, g.ctypes.data, Gl, n, offs.ctypes.data, buf.ctypes.data) == 0
     assert np.array_equal(a, b)
     assert set(np.unique(a).tolist()) <= set(b"ACGT")
+
+
+def test_c_consumer_of_the_header(tmp_path):
+    """The header compiles as C11 with warnings as errors, and a C program
+    linked against the library calls its host-side entry points."""
+    import shutil
+    import subprocess
+    import db_format as D
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    exe = tmp_path / "consumer"
+    libdir = os.path.join(ROOT, "gkc_b200")
+    subprocess.run([cc, "-std=c11", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c_consumer", "consumer.c"), "-o", str(exe), "-L", libdir,
+                    "-lgkc_b200", f"-Wl,-rpath,{libdir}"], check=True)
+    fa = tmp_path / "r.fa"
+    fa.write_text(">a\nACGTACGT\n>b two lines\nGGGGCCCC\nAAAA\n")
+    D.write(str(tmp_path / "db"), 31, np.array([[5], [77], [1 << 40]], np.uint64),
+            np.array([2, 9, 300], np.uint32), 1, 1000)
+    r = subprocess.run([str(exe), str(fa), str(tmp_path / "db")], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.count("ok ") == 11
