@@ -259,8 +259,14 @@ def run_reference(args, wl):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference tree absent at build time)"}))
         return
     threads = os.cpu_count() or 1
-    n = sample_reads(args, wl)
-    reads, offs = host_sample(wl, args.seed, n)
+    # each step about min(10 s, 100 s / (steps + warm-up)) of CPU work, sized
+    # from a calibration run on the first sample_reads(...) reads
+    reads, offs = host_sample(wl, args.seed, sample_reads(args, wl))
+    rate, _, kmers, _ = cpu_reference_rate(reads, offs, wl, threads)
+    per_step = min(10.0, 100.0 / max(1, args.steps + args.warmup))
+    n = scaled_sample(wl, len(offs) - 1, kmers, rate, per_step)
+    if n > len(offs) - 1:
+        reads, offs = host_sample(wl, args.seed, n)
     for _ in range(args.warmup):
         cpu_reference_rate(reads, offs, wl, threads)
     rates, secs, km = [], [], 0
@@ -390,6 +396,18 @@ def wl_name(args):
     return {"ns": "ns-100Mbp-30x-150bp-k31", "config2": "config2-10Mbp-30x-150bp-k31",
             "config1": "config1-iid-20000x150bp-k31", "config4": "config4-100Mbp-30x-250bp-k63",
             "config3": "config3-100Mbp-20x-long-hpc-k25"}[args.workload]
+
+
+def scaled_sample(wl, n_cal, kmers_cal, rate, seconds):
+    """Reads whose reference CPU run takes about `seconds`, from a
+    calibration run of n_cal reads (kmers_cal k-mers at `rate` k-mers/s)."""
+    per_read = max(kmers_cal / max(n_cal, 1), 1.0)
+    n = int(seconds * rate / per_read)
+    if wl["gen"] == "iid":
+        return min(max(n, n_cal), wl["n_reads"])
+    if wl["gen"] == "genome":
+        return min(max(n, n_cal), wl["coverage"] * wl["genome_len"] // wl["read_len"])
+    return max(n, n_cal)
 
 
 def sample_reads(args, wl):
@@ -543,6 +561,14 @@ def run_ours(args, wl):
         # restore the batched result in the context
         step()
 
+    # the CPU baseline's reads: the workload's first reads, copied from the
+    # device (at most 10 M reads, enough for about 10 s of reference CPU work)
+    cpu_sample = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        n_max = min(n_reads, 10_000_000)
+        so = offs[:n_max + 1].cpu().numpy().view(np.uint64).copy()
+        cpu_sample = (reads[:int(so[-1])].cpu().numpy(), so)
+
     # end to end through the host API: pinned host reads in, full sorted list out
     if not args.no_e2e:
         h_reads = torch.empty(n_bases, dtype=torch.uint8, pin_memory=True)
@@ -587,9 +613,12 @@ def run_ours(args, wl):
         import oracle_ffi as F
         if F.ref_available():
             threads = os.cpu_count() or 1
-            n = sample_reads(args, wl)
-            gh = genome.cpu().numpy() if genome is not None else None
-            sr, so = host_sample(wl, args.seed, n, gh)
+            n_cal = min(sample_reads(args, wl), cpu_sample[1].size - 1)
+            cal_o = cpu_sample[1][:n_cal + 1]
+            rate, _, kmers, _ = cpu_reference_rate(cpu_sample[0][:int(cal_o[-1])], cal_o, wl, threads)
+            n = min(scaled_sample(wl, n_cal, kmers, rate, 10.0), cpu_sample[1].size - 1)
+            so = cpu_sample[1][:n + 1]
+            sr = cpu_sample[0][:int(so[-1])]
             rate, dt, km, _ = cpu_reference_rate(sr, so, wl, threads)
             result["cpu_baseline"] = {
                 "value": rate, "unit": "kmers/s", "cores": threads, "kind": "reference",
