@@ -189,8 +189,8 @@ gkc_status gkc_partition_import(gkc_ctx *c, const gkc_params *prm, uint32_t n_sr
   }
   const uint64_t n = e[n_src], nbytes = dby[n_src];
   if ((n && !d_desc) || (nbytes && !d_bytes)) return GKC_ERR_INVALID_ARG;
-  for (uint32_t s = 0; s < n_src; s++)
-    if (seg_bytes[s] >> 40) return ctx_fail(c, GKC_ERR_INVALID_ARG, "a sender's byte run exceeds 2^40");
+  // descriptors keep the byte offset in 40 bits, rebased over all runs
+  if (nbytes >> 40) return ctx_fail(c, GKC_ERR_INVALID_ARG, "received bytes exceed 2^40");
   WS(dd, uint64_t, "skm_desc_bin", n + 1);
   WS(dp, uint8_t, "packed", nbytes + 16);
   WS(dbs, uint64_t, "bin_start", nbl + 1);
