@@ -118,7 +118,7 @@ struct DbHeader {
 int auto_lut(uint64_t n, int k) {
   int l = 1;
   while (l < kDbMaxLut && (1ull << (2 * (l + 1))) * 8 <= n) l++;  // about 8 records per table entry
-  return std::min(l, k - 1 > 0 ? k - 1 : 1);
+  return std::min(l, k - 1);  // 0 for k = 1: a two-entry table
 }
 
 bool put(FILE *f, const void *p, size_t n) { return fwrite(p, 1, n, f) == n; }

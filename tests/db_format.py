@@ -15,7 +15,7 @@ def auto_lut(n, k):
     l = 1
     while l < 13 and (4 ** (l + 1)) * 8 <= n:
         l += 1
-    return min(l, max(k - 1, 1))
+    return min(l, k - 1)
 
 
 def key_ints(keys):
@@ -31,7 +31,7 @@ def layout(k, keys, counts, min_count, max_count, lut_len=0):
     ks = key_ints(keys)
     counts = [int(c) for c in counts]
     n = len(ks)
-    l = lut_len or auto_lut(n, k)
+    l = lut_len if lut_len else auto_lut(n, k)
     shift = 2 * (k - l)
     sb = (shift + 7) // 8
     cmax = max(counts, default=0)

@@ -60,3 +60,14 @@ def test_reader_rejects_damaged_files(tmp_path):
         G.Database(path)
     with pytest.raises(G.GkcError):
         G.Database(str(tmp_path / "missing"))
+
+
+def test_reader_single_base_kmers(tmp_path):
+    """k = 1: the table has no prefix bits (two entries)."""
+    keys = np.array([[0], [2], [3]], np.uint64)
+    counts = np.array([4, 1, 7], np.uint32)
+    path = str(tmp_path / "db")
+    D.write(path, 1, keys, counts, 1, 9, 0)
+    with G.Database(path) as db:
+        assert db.info["lut_prefix_len"] == 0
+        assert np.array_equal(db.lookup(np.array([0, 1, 2, 3], np.uint64)), [4, 0, 1, 7])
