@@ -182,3 +182,30 @@ def test_oracle_partition_sizes_from_golden():
         want = np.zeros(nb, np.uint64)
         np.add.at(want, d["skm_bin"].astype(np.int64), d["skm_len"].astype(np.uint64))
         assert np.array_equal(sizes, want)
+
+
+@pytest.mark.skipif(not F.ref_available(), reason="reference harness not built here")
+def test_oracle_matches_reference_parameter_sweep():
+    """Random (k, p, nbins, hpc, filter) combinations, each on its own random
+    read set (reads of at least k bases, N and lower case included):
+    partition multisets and per-bin counts equal the reference's."""
+    r = np.random.default_rng(2024)
+    try:
+        for case in range(24):
+            k = int(r.integers(5, 33))
+            p = int(r.integers(3, min(16, k) + 1))
+            nb = int(r.integers(1, 300))
+            hpc = int(r.integers(0, 2))
+            filt = int(r.integers(0, 4))
+            if filt and not F.ref_available(filt):
+                filt = 0
+            reads, offs = _random_reads(1000 + case, 60, k, 400)
+            F.set_filter(filt)
+            o = F.oracle_partition(reads, offs, k, p, hpc, nb)
+            ref = F.ref_partition(reads, offs, k, p, hpc, nb, batch_reads=17, filter_id=filt)
+            assert o.multisets(nb) == ref.multisets(nb), (k, p, nb, hpc, filt)
+            co, cr = F.oracle_count_bins(o, k, nb), F.ref_count_bins(ref, k, nb)
+            for key in ("bin_off", "keys_lo", "counts"):
+                assert np.array_equal(co[key], cr[key]), (k, p, nb, hpc, filt, key)
+    finally:
+        F.set_filter(0)
