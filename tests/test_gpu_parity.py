@@ -311,3 +311,38 @@ def test_partition_balance_pipeline(ctx, mode):
     sizes, st = ctx.partition_balance(pv)
     assert np.array_equal(sizes, want)
     assert st == F.oracle_balance(want)
+
+
+def test_random_parameter_sweep_vs_oracle(ctx):
+    """Random (k, p, nbins, hpc, filter) combinations, k up to 64 and up to
+    3000 bins (beyond the shared-memory bin placement): batched partition
+    and counts, and plain-mode counts, against the oracle."""
+    import torch
+    r = np.random.default_rng(77)
+    try:
+        for case in range(16):
+            k = int(r.integers(5, 65))
+            p = int(r.integers(3, min(16, k) + 1))
+            nb = int(r.choice([int(r.integers(1, 300)), int(r.integers(2049, 3001))]))
+            hpc = int(r.integers(0, 2))
+            filt = int(r.integers(0, 4))
+            reads, offs = random_reads(500 + case, 150, k, 600)
+            F.set_filter(filt)
+            ctx.set_filter(filt)
+            o = F.oracle_partition(reads, offs, k, p, hpc, nb)
+            want = F.oracle_count_bins(o, k, nb)
+            skm, _ = lib_partition(ctx, reads, offs, k, p, hpc, nb)
+            assert skm.multisets(nb) == o.multisets(nb), (k, p, nb, hpc, filt)
+            got, _ = lib_counts(ctx, k, nb)
+            assert_counts_equal(got, want)
+            d_reads = torch.from_numpy(reads).cuda()
+            d_offs = torch.from_numpy(offs.view(np.int64)).cuda()
+            _, cv = ctx.pipeline_device(d_reads, len(reads), d_offs, len(offs) - 1, G.params(k, p, nb, hpc),
+                                        mode=G.MODE_PLAIN)
+            bin_off, keys, counts = ctx.count_copy_out(cv)
+            got = dict(bin_off=bin_off, keys_lo=keys[:, 0].copy(), counts=counts,
+                       keys_hi=keys[:, 1].copy() if keys.shape[1] > 1 else None)
+            assert_counts_equal(got, want)
+    finally:
+        F.set_filter(0)
+        ctx.set_filter(0)
