@@ -110,3 +110,19 @@ def test_c_consumer_of_the_header(tmp_path):
     r = subprocess.run([str(exe), str(fa), str(tmp_path / "db")], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.count("ok ") == 11
+
+
+def test_cpp_nccl_sharding_example_compiles(tmp_path):
+    """The C++ driver of the bin-sharded count over NCCL
+    (tests/c_consumer/shard_nccl.cpp) compiles against the header."""
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++")
+    cuda_inc = "/usr/local/cuda/include"
+    nccl_dirs = [d for d in ("/usr/include",) if os.path.exists(os.path.join(d, "nccl.h"))]
+    if cxx is None or not nccl_dirs or not os.path.exists(os.path.join(cuda_inc, "cuda_runtime.h")):
+        pytest.skip("no C++ compiler, CUDA headers or NCCL header")
+    subprocess.run([cxx, "-std=c++17", "-Wall", "-Wextra", "-Werror", "-c", "-I", os.path.join(ROOT, "include"),
+                    "-I", cuda_inc, "-I", nccl_dirs[0],
+                    os.path.join(ROOT, "tests", "c_consumer", "shard_nccl.cpp"), "-o", str(tmp_path / "s.o")],
+                   check=True)
