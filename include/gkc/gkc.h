@@ -306,7 +306,8 @@ gkc_status gkc_hpc_device(gkc_ctx *ctx, const char *d_reads, uint64_t n_bytes,
 
 /* ---- FASTA / FASTQ ingest (reference: ReadLoader, read_loader.hpp:44-196,
  *      :276-321, :470-520).  Reads the file (format from its first byte, '>'
- *      or '@') on n_threads threads (0: all cores) into one read CSR, in file
+ *      or '@'; the reference goes by the file name's last letter, :285) on
+ *      n_threads threads (0: all cores) into one read CSR, in file
  *      order: *reads holds the sequences back to back, *offs their n_reads+1
  *      offsets.  FASTQ: the second line of each 4-line record; FASTA: the
  *      lines after a header up to the next header, joined (the reference

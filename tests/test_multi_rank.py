@@ -89,11 +89,13 @@ def _shard_rank_main(rank, world, port, out_dir):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     reads, offs = _random_reads(5, 240, 30, 400)
     n = len(offs) - 1
-    # uneven shares, the last rank's possibly empty
-    cuts = [0, n // 5, n][:world] + [n] if world == 2 else [0, n // 2, n // 2, n]
+    # uneven shares: two ranks 1:4; three ranks with the middle one empty;
+    # four ranks with every read on rank 2
+    cuts = {2: [0, n // 5, n], 3: [0, n // 2, n // 2, n], 4: [0, 0, 0, n, n]}[world]
     r, o = _slice_reads(reads, offs, cuts[rank], cuts[rank + 1])
-    eng = OracleEngine(r, o, SHARD_K, SHARD_P, 0, SHARD_NB)
-    prm_local, bounds, _ = shard.exchange_dist(eng, G.params(SHARD_K, SHARD_P, SHARD_NB))
+    nb = SHARD_NB if world < 4 else 4  # one bin per rank
+    eng = OracleEngine(r, o, SHARD_K, SHARD_P, 0, nb)
+    prm_local, bounds, _ = shard.exchange_dist(eng, G.params(SHARD_K, SHARD_P, nb))
     c = eng.count(prm_local.nbins)
     np.savez(os.path.join(out_dir, f"s{rank}.npz"), bounds=bounds, bin_off=c["bin_off"], keys=c["keys_lo"],
              counts=c["counts"], kmers=eng.local_kmers)
@@ -101,7 +103,7 @@ def _shard_rank_main(rank, world, port, out_dir):
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("world", [2, 3, 4])
 def test_bin_sharded_count_gloo(tmp_path, world):
     """Over gloo ranks, the owners' counts put together equal the counts of
     all reads on one rank: every k-mer counted once, by its bin's owner."""
@@ -110,7 +112,8 @@ def test_bin_sharded_count_gloo(tmp_path, world):
     port = 31500 + (os.getpid() % 2000) + world
     mp.spawn(_shard_rank_main, args=(world, port, str(tmp_path)), nprocs=world, join=True)
     reads, offs = _random_reads(5, 240, 30, 400)
-    want = F.oracle_count_bins(F.oracle_partition(reads, offs, SHARD_K, SHARD_P, 0, SHARD_NB), SHARD_K, SHARD_NB)
+    nb = SHARD_NB if world < 4 else 4
+    want = F.oracle_count_bins(F.oracle_partition(reads, offs, SHARD_K, SHARD_P, 0, nb), SHARD_K, nb)
     total_kmers = 0
     for rank in range(world):
         d = np.load(tmp_path / f"s{rank}.npz")
