@@ -1,6 +1,6 @@
 """Benchmark: canonical k-mers counted per second on one B200 (or N, weak).
 
-Default workload (the north-star shape): a 100 Mbp synthetic genome with 5%
+Default workload: a 100 Mbp synthetic genome with 5%
 of its length as 1-5 kbp segment copies (1% divergence), sampled as 150 bp
 reads on both strands to 30x coverage (20 M reads, 3.0 G bases) with 0.5%
 substitution errors; k=31, p=11, 256 bins.  Reads are generated on the device

@@ -1,7 +1,7 @@
 /* CPU restatement of GKC's partition-and-count path -- TEST INFRASTRUCTURE.
  *
  * Only tests/, the smoke check and bench.py's CPU-baseline leg may use this
- * file, and only as the checker.  Each function cites the reference lines it
+ * file, and only to check results.  Each function cites the reference lines it
  * restates (paths relative to the GKC project root).
  */
 #include "gkc_oracle.h"

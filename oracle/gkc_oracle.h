@@ -2,7 +2,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the shipped library calls, links or
  * loads this code; only the tests, the smoke check and the benchmark's CPU
- * baseline leg use it, and only as the checker.
+ * baseline leg use it, and only to check results.
  *
  * Parity of the k <= 32 partition and count semantics (including the
  * N-smear of the minimizer kernel and the run-collapse of HPC) is pinned

@@ -13,7 +13,7 @@ def pytest_configure(config):
 
 
 @pytest.fixture(scope="session", autouse=True)
-def _built_checkers():
+def _built_oracle():
     """The oracle library is built by __graft_entry__.build(); build it here
     if a test session starts without it."""
     so = os.path.join(ROOT, "oracle", "liboracle.so")

@@ -1,4 +1,4 @@
-"""ctypes bindings to the checkers under oracle/ (test infrastructure only).
+"""ctypes bindings to the oracle libraries under oracle/ (test infrastructure only).
 
 liboracle.so is the plain-C restatement; oracle/_ref/libgkcref.so is the
 reference's own code compiled from its sources (present only where it was
