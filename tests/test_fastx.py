@@ -83,3 +83,11 @@ def test_rejects_other_formats(tmp_path):
         G.load_fastx(str(p))
     with pytest.raises(G.GkcError):
         G.load_fastx(str(tmp_path / "missing.fq"))
+
+
+def test_empty_file_has_no_reads(tmp_path):
+    for name, data in (("e.fq", b""), ("nl.fa", b"\n\n")):
+        p = tmp_path / name
+        p.write_bytes(data)
+        reads, offs = G.load_fastx(str(p))
+        assert len(reads) == 0 and list(offs) == [0]
