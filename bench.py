@@ -248,6 +248,23 @@ def cpu_reference_rate(reads, offs, wl, threads):
     return kmers / dt, dt, kmers, distinct
 
 
+def reference_parity(ctx, G, prm, reads, offs, wl, threads):
+    """The CPU-baseline sample counted by the reference's own CPU path and by
+    this library (through the host API), their per-bin sorted (k-mer, count)
+    lists compared by digest (untimed)."""
+    import oracle_ffi as F
+    ref, _ = F.ref_pipeline_counts(reads, offs, wl["k"], wl["p"], wl["hpc"], wl["nbins"], batch_reads=2048,
+                                   n_threads=threads)
+    rd, _ = F.counts_digest64(ref["bin_off"], ref["keys_lo"], ref["counts"])
+    cv = ctx.pipeline_host(reads, offs, prm, G.MODE_BATCHED)
+    bo, keys, counts = ctx.count_copy_out(cv)
+    gd, _ = F.counts_digest64(bo, keys[:, 0], counts)
+    return {"reads": len(offs) - 1, "kmers": int(cv.n_kmers), "distinct": int(cv.n_distinct),
+            "reference_distinct": int(len(ref["keys_lo"])), "digest": "%016x" % gd,
+            "reference_digest": "%016x" % rd, "match": bool(gd == rd and np.array_equal(bo, ref["bin_off"])),
+            "compared": "per-bin sorted (k-mer, count) lists of the CPU-baseline sample"}
+
+
 # ------------------------------------------------------------ reference arm
 
 def run_reference(args, wl):
@@ -517,7 +534,7 @@ def run_ours(args, wl):
             traffic = None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                "model": "fixed algorithmic-bytes model (see DESIGN.md)",
+                "model": "fixed algorithmic-bytes model: partition B+8(R+1)+L/4+8S, expand L/4+8S+wN, sort wN+2PwN, count wN+(w+4)D",
                 "model_bytes_per_launch": kernel_bytes[dom], "ms_per_launch": dom_ms}
     if traffic:
         roofline["frac_dram_traffic"] = traffic / (dom_ms / 1000.0) / 1e9 / peak
@@ -535,12 +552,16 @@ def run_ours(args, wl):
         "pipeline": pipeline, "stages_ms": stages, "gpu_launches": launches, "clocks": clocks,
     }
 
-    # plain per-stage form on the same input (bit-exact check against batched)
+    # plain per-stage form on the same input, its whole output compared with
+    # the batched one on the device (bin offsets, every key and count)
     if not args.no_plain and rank == 0:
-        bin_off_b, keys_b, counts_b = None, None, None
-        h_bo = np.zeros(wl["nbins"] + 1, np.uint64)
-        G.lib().gkc_count_copy_out(ctx.h, h_bo.ctypes.data, None, None)
-        ref_digest = (int(cv.n_distinct), h_bo.tobytes())
+        kw = 1 if wl["k"] <= 32 else 2
+        nd_b = int(cv.n_distinct)
+        batched_out = (torch.empty(wl["nbins"] + 1, dtype=torch.int64, device="cuda"),
+                       torch.empty(max(nd_b * kw, 1), dtype=torch.int64, device="cuda"),
+                       torch.empty(max(nd_b, 1), dtype=torch.int32, device="cuda"))
+        assert G.lib().gkc_count_copy_out(ctx.h, *(t.data_ptr() for t in batched_out)) == 0
+        torch.cuda.synchronize()
         # the plain form allocates its own buffers: with 16-byte keys the
         # batched ones are given back first (both key sets do not fit)
         wide = wl["k"] > 32
@@ -556,12 +577,19 @@ def run_ours(args, wl):
         pe1.record(stream)
         torch.cuda.synchronize()
         p_ms = pe0.elapsed_time(pe1) / args.plain_steps
-        h_bo2 = np.zeros(wl["nbins"] + 1, np.uint64)
-        G.lib().gkc_count_copy_out(ctx.h, h_bo2.ctypes.data, None, None)
-        same = (int(pcv.n_distinct), h_bo2.tobytes()) == ref_digest
+        same = int(pcv.n_distinct) == nd_b
+        if same:
+            plain_out = tuple(torch.empty_like(t) for t in batched_out)
+            assert G.lib().gkc_count_copy_out(ctx.h, *(t.data_ptr() for t in plain_out)) == 0
+            torch.cuda.synchronize()
+            same = all(torch.equal(a, b) for a, b in zip(batched_out, plain_out))
+            del plain_out
+        del batched_out
+        torch.cuda.empty_cache()
         result["plain"] = {"value": N / (p_ms / 1000.0), "unit": "kmers/s", "ms_per_step": p_ms,
                            "steps": args.plain_steps, "batched_over_plain": p_ms / ms_step,
-                           "same_counts_as_batched": bool(same),
+                           "same_output_as_batched": bool(same),
+                           "compared": "bin offsets, every key and every count, on the device",
                            "launches_per_step": int(ctx.timings().launches)}
         # restore the batched result in the context
         if wide:
@@ -633,6 +661,10 @@ def run_ours(args, wl):
             if wl["k"] > 32:
                 result["cpu_baseline"]["note"] = ("the reference keeps k-mers in 64-bit words (k <= 32): "
                                                   "at this k its CPU path is a timing figure only")
+                result["parity"] = {"reads": len(so) - 1, "match": None,
+                                    "note": "the reference's keys are 64-bit: no comparison at k > 32"}
+            else:
+                result["parity"] = reference_parity(ctx, G, prm, sr, so, wl, threads)
         else:
             result["cpu_baseline"] = {"value": None, "unit": "kmers/s", "cores": 0, "kind": "reference",
                                       "sample": "oracle/_ref not built"}
@@ -740,7 +772,7 @@ def run_shard(args, wl):
     achieved = kernel_bytes[dom] / (stages[dom] / 1000.0) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                "model": "fixed algorithmic-bytes model (see DESIGN.md)",
+                "model": "fixed algorithmic-bytes model: partition B+8(R+1)+L/4+8S, expand L/4+8S+wN, sort wN+2PwN, count wN+(w+4)D",
                 "model_bytes_per_launch": kernel_bytes[dom], "ms_per_launch": stages[dom]}
     sent = 8 * S + own["bytes"]  # descriptors + packed bytes, all destinations
     leaves = sent * (world - 1) / world

@@ -1069,12 +1069,13 @@ gkc_status gkc_count_copy_out(gkc_ctx *c, uint64_t *bin_off, uint64_t *keys, uin
   cudaSetDevice(c->dev);
   const gkc_count_view &v = c->cv;
   CK(cudaEventRecord(c->ev[2], c->st));
+  // cudaMemcpyDefault: each destination may be host or device memory
   if (bin_off)
-    CK(cudaMemcpyAsync(bin_off, v.bin_off, (v.nbins + 1) * 8, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(bin_off, v.bin_off, (v.nbins + 1) * 8, cudaMemcpyDefault, c->st));
   if (keys && v.n_distinct)
-    CK(cudaMemcpyAsync(keys, v.keys, v.n_distinct * 8 * v.key_words, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(keys, v.keys, v.n_distinct * 8 * v.key_words, cudaMemcpyDefault, c->st));
   if (counts && v.n_distinct)
-    CK(cudaMemcpyAsync(counts, v.counts, v.n_distinct * 4, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(counts, v.counts, v.n_distinct * 4, cudaMemcpyDefault, c->st));
   CK(cudaEventRecord(c->ev[3], c->st));
   CK(cudaStreamSynchronize(c->st));
   float ms = 0;

@@ -887,14 +887,8 @@ __global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
       }
       K *dst = fits ? T.A : reinterpret_cast<K *>(a.scratch);
       for (uint32_t i = tid; i < ns; i += SC_NT) dst[i] = placed[base_cnt + i];
-      if (tid == 0) S.cursor = ns;
-      __syncthreads();
       if (tid == 0) T.out = start + S.run;
       __syncthreads();
-      if (!in_bounds(a, 9, S.cursor, (uint64_t)ns + 1)) {
-        __syncthreads();
-        continue;
-      }
       if (fits) {
         smem_sort<K>(T, ns, key_bits, skip);
         const uint32_t D = smem_runs<K>(T, ns);

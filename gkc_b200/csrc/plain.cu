@@ -498,7 +498,10 @@ static std::mutex g_mu;
 static Dev g_dev[kMaxDevices];
 
 // Set-up for the current device, once: the array's device address and the
-// SM count.
+// SM count.  With lazy module loading (the CUDA default) the library's
+// kernels and the array itself are loaded onto the device by this first
+// lookup, so the first call does take device memory for them.  The address is
+// kept for the life of the process: after cudaDeviceReset it would be stale.
 static gkc_status setup(int dev, Dev *out) {
   if (dev < 0 || dev >= kMaxDevices) return GKC_ERR_NO_DEVICE;
   std::lock_guard<std::mutex> lock(g_mu);
@@ -549,10 +552,16 @@ extern "C" gkc_status gkc_count_superkmers_device_noalloc(int k, const uint32_t 
   if (n_skm == 0) return GKC_OK;
   int dev = 0;
   NA_CK(cudaGetDevice(&dev));
+  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+  // the call waits on its stream twice (to read the sizes, then the result):
+  // on a stream that is being captured that would end the caller's capture,
+  // so such a call is refused before any work is queued
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  NA_CK(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return GKC_ERR_INVALID_ARG;
   Dev d;
   gkc_status s = setup(dev, &d);
   if (s != GKC_OK) return s;
-  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
   unsigned long long *w = d.base;
   auto u64p = [&](uint64_t off) { return reinterpret_cast<uint64_t *>(w + off); };
   uint32_t *err = reinterpret_cast<uint32_t *>(w + W_ERR);

@@ -191,7 +191,8 @@ gkc_status gkc_count_superkmers_host(gkc_ctx *ctx, int k, const uint32_t *skm_le
                                      const uint8_t *packed, uint64_t n_skm, gkc_mode mode,
                                      uint64_t *n_distinct);
 /* Copies the last count result: bin_off[nbins+1], keys[n_distinct*key_words],
- * counts[n_distinct]; any pointer may be NULL. */
+ * counts[n_distinct]; any pointer may be NULL, and each may point to host or
+ * to device memory. */
 gkc_status gkc_count_copy_out(gkc_ctx *ctx, uint64_t *bin_off, uint64_t *keys, uint32_t *counts);
 /* Counts one group of packed superkmers already in device memory without
  * allocating anything.  No counterpart in the reference: it exists for callers
@@ -210,11 +211,17 @@ gkc_status gkc_count_copy_out(gkc_ctx *ctx, uint64_t *bin_off, uint64_t *keys, u
  * the library, held by every GPU that loads it until the process exits.  It
  * bounds a call to 131,072 superkmers and 1,048,576 k-mers: larger groups are
  * rejected with GKC_ERR_CAPACITY (GKC_ERR_INVALID_ARG for k > 32).  The first
- * call on a device looks up the array's device address; make that first call
- * before any stream capture.  All calls share the one array and each leaves
- * its contents behind (the next call clears what must start at zero), so
- * calls that overlap on the GPU, from different streams or threads, race and
- * must not be made. */
+ * call on a device looks up the array's device address, and with CUDA's lazy
+ * module loading (the default) that lookup is what loads the library's
+ * kernels and the array onto the device: make the first call at start-up,
+ * before a memory pool claims the rest of HBM and before any stream capture.
+ * The address is kept for the process's life, so the entry point must not be
+ * used after cudaDeviceReset.  Every call waits on its stream (to read the
+ * group's size, then the result); on a stream that is capturing it returns
+ * GKC_ERR_INVALID_ARG without queuing work.  All calls share the one array
+ * and each leaves its contents behind (the next call clears what must start
+ * at zero), so calls that overlap on the GPU, from different streams or
+ * threads, race and must not be made. */
 gkc_status gkc_count_superkmers_device_noalloc(int k, const uint32_t *d_skm_len,
                                                const uint8_t *d_packed, uint64_t n_skm,
                                                uint64_t out_capacity, uint64_t *d_keys_out,

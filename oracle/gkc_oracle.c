@@ -510,3 +510,63 @@ void orc_balance_stats(const uint64_t *sizes, int n, orc_balance *out) {
   out->stdev = sqrt(out->variance);
   out->cv = out->stdev / (double)mean;
 }
+
+/* --- digests for comparing large outputs without moving them twice (test
+ *     infrastructure; not a reference algorithm).  Both are sums of mixed
+ *     64-bit words, so they are fast and need one pass. --- */
+
+static inline uint64_t dg_mix(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+/* Per bin: the sum over the bin's list of mix(key, count, index in bin); the
+ * list's order enters through the index.  Returns the digest of all bins
+ * (each bin's sum mixed with its number and length). */
+uint64_t orc_counts_digest(const uint64_t *bin_off, uint32_t nbins, const uint64_t *keys_lo,
+                           const uint64_t *keys_hi, const uint32_t *counts, uint64_t *bin_digest) {
+  uint64_t total = 0;
+  for (uint32_t b = 0; b < nbins; b++) {
+    uint64_t h = 0;
+    for (uint64_t i = bin_off[b]; i < bin_off[b + 1]; i++) {
+      uint64_t j = i - bin_off[b] + 1;
+      uint64_t e = dg_mix(keys_lo[i] ^ (0x9E3779B97F4A7C15ull * j));
+      e += (keys_hi ? keys_hi[i] : 0) * 0xD1B54A32D192ED03ull + (uint64_t)counts[i] * 0x632BE59BD9B4E019ull;
+      h += dg_mix(e);
+    }
+    if (bin_digest) bin_digest[b] = h;
+    total += dg_mix(h + 0xA24BAED4963EE407ull * (b + 1) + (bin_off[b + 1] - bin_off[b]) * 0x9FB21C651E98DF25ull);
+  }
+  return total;
+}
+
+/* Multiset digest of a partition: per superkmer a hash of (length, packed
+ * bytes), summed per bin, so the order of superkmers does not matter. */
+uint64_t orc_skm_multiset_digest(const uint32_t *bin, const uint32_t *len, const uint64_t *byte_off,
+                                 const uint8_t *bytes, uint64_t n_skm, uint32_t nbins,
+                                 uint64_t *bin_digest, uint64_t *bin_count) {
+  uint64_t *h = (uint64_t *)calloc(nbins, sizeof(uint64_t));
+  uint64_t *n = (uint64_t *)calloc(nbins, sizeof(uint64_t));
+  for (uint64_t i = 0; i < n_skm; i++) {
+    const uint8_t *p = bytes + byte_off[i];
+    const uint64_t nb = (len[i] + 3) / 4;
+    uint64_t x = dg_mix(0x51AF0DE5ull + len[i]);
+    for (uint64_t j = 0; j < nb; j += 8) {
+      uint64_t w = 0;
+      for (uint64_t t = 0; t < 8 && j + t < nb; t++) w |= (uint64_t)p[j + t] << (8 * t);
+      x = dg_mix(x ^ w ^ (j << 56));
+    }
+    h[bin[i]] += x;
+    n[bin[i]]++;
+  }
+  uint64_t total = 0;
+  for (uint32_t b = 0; b < nbins; b++) {
+    if (bin_digest) bin_digest[b] = h[b];
+    if (bin_count) bin_count[b] = n[b];
+    total += dg_mix(h[b] + 0xA24BAED4963EE407ull * (b + 1) + n[b] * 0x9FB21C651E98DF25ull);
+  }
+  free(h);
+  free(n);
+  return total;
+}

@@ -105,6 +105,17 @@ void orc_balance_stats(const uint64_t *sizes, int n, orc_balance *out);
 
 void orc_free(void *p);
 
+/* Digests of large outputs (test infrastructure): per bin, a sum of mixed
+ * words over the bin's sorted (key, count) list, the index in the bin
+ * included; and a multiset digest of a partition's (length, packed bytes)
+ * per bin.  Each returns the digest over all bins; the per-bin arrays may be
+ * NULL.  keys_hi is NULL for 64-bit keys. */
+uint64_t orc_counts_digest(const uint64_t *bin_off, uint32_t nbins, const uint64_t *keys_lo,
+                           const uint64_t *keys_hi, const uint32_t *counts, uint64_t *bin_digest);
+uint64_t orc_skm_multiset_digest(const uint32_t *bin, const uint32_t *len, const uint64_t *byte_off,
+                                 const uint8_t *bytes, uint64_t n_skm, uint32_t nbins,
+                                 uint64_t *bin_digest, uint64_t *bin_count);
+
 #ifdef __cplusplus
 }
 #endif

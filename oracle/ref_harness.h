@@ -55,6 +55,11 @@ int ref_pipeline(const char *reads, const uint64_t *offs, int64_t n_reads, int k
                  int nbins, int batch_reads, int n_threads, uint64_t *distinct_out,
                  uint64_t *kmers_out);
 
+// The same with the per-bin sorted (k-mer, count) lists returned (k <= 32).
+int ref_pipeline_counts(const char *reads, const uint64_t *offs, int64_t n_reads, int k, int p,
+                        int hpc, int nbins, int batch_reads, int n_threads, uint64_t *kmers_out,
+                        ref_counts *out);
+
 #ifdef __cplusplus
 }
 #endif

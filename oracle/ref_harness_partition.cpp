@@ -153,3 +153,53 @@ extern "C" int ref_pipeline(const char *reads, const uint64_t *offs, int64_t n_r
   *kmers_out = kmers;
   return 0;
 }
+
+// The same CPU path with the sorted (k-mer, count) lists kept: per bin, the
+// sorted keys and run lengths kmc_counting_GPU computes (captured as in
+// ref_count_bins), for comparing a GPU run on the same reads.
+extern "C" int ref_pipeline_counts(const char *reads, const uint64_t *offs, int64_t n_reads, int k,
+                                   int p, int hpc, int nbins, int batch_reads, int n_threads,
+                                   uint64_t *kmers_out, ref_counts *out) {
+  std::memset(out, 0, sizeof(*out));
+  if (k < 1 || k > 32) return -1;
+  std::vector<SKMStore *> stores;
+  for (int i = 0; i < nbins; i++) stores.push_back(new SKMStore());
+  partition_into(reads, offs, n_reads, k, p, hpc, batch_reads, n_threads, stores);
+  uint64_t kmers = 0;
+  for (int b = 0; b < nbins; b++)
+    kmers += stores[b]->tot_size - stores[b]->skms.size_approx() * (uint64_t)(k - 1);
+  std::vector<std::vector<uint64_t>> keys(nbins), runs(nbins);
+  std::vector<size_t> ret(nbins, 0);
+  {
+    ThreadPool<size_t> tp(n_threads < 1 ? 1 : n_threads);
+    std::vector<std::future<size_t>> fut(nbins);
+    for (int b = 0; b < nbins; b++)
+      fut[b] = tp.commit_task([=, &stores, &keys, &runs]() { return ref_count_store(k, stores[b], &keys[b], &runs[b]); });
+    tp.finish();
+    for (int b = 0; b < nbins; b++) ret[b] = fut[b].get();
+  }
+  uint64_t total = 0;
+  for (int b = 0; b < nbins; b++) total += ret[b];
+  out->nbins = (uint32_t)nbins;
+  out->n_distinct = total;
+  out->bin_off = (uint64_t *)malloc(sizeof(uint64_t) * (nbins + 1));
+  out->keys = (uint64_t *)malloc(sizeof(uint64_t) * (total + 1));
+  out->counts = (uint32_t *)malloc(sizeof(uint32_t) * (total + 1));
+  out->returned = (uint64_t *)malloc(sizeof(uint64_t) * (nbins + 1));
+  uint64_t w = 0;
+  for (int b = 0; b < nbins; b++) {
+    out->bin_off[b] = w;
+    out->returned[b] = ret[b];
+    for (size_t i = 0; i < ret[b]; i++) {
+      out->keys[w] = keys[b][i];
+      const uint64_t r = runs[b][i];
+      out->counts[w] = r > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)r;
+      w++;
+    }
+    std::vector<uint64_t>().swap(keys[b]);
+    std::vector<uint64_t>().swap(runs[b]);
+  }
+  out->bin_off[nbins] = w;
+  *kmers_out = kmers;
+  return 0;
+}

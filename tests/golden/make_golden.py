@@ -5,7 +5,10 @@ library was built:  python tests/golden/make_golden.py
 
 Small cases store inputs and full outputs (case_<name>.npz); larger cases
 store the generator parameters plus SHA-256 digests (golden.json), their
-reads being regenerated by gkc_b200.synth.
+reads being regenerated by gkc_b200.synth.  The "large" cases (config 2 at its
+stated size: 2 M reads, 240 M k-mers) store 64-bit digests instead
+(oracle_ffi.counts_digest64 / skm_digest64), which the GPU tests recompute
+on the library's output; `--large` regenerates only those.
 """
 import json
 import os
@@ -79,6 +82,30 @@ def gen_digest_case(c):
     return synth.short_reads(c["seed"], g, n, c["read_len"], c["err"])
 
 
+LARGE_CASES = {
+    # config 2 at its stated size: 10 Mbp genome, 30x of 150 bp reads (2 M reads)
+    "config2": dict(gen="genome", seed=2026, genome_len=10_000_000, coverage=30, read_len=150,
+                    err=0.005, k=31, p=11, hpc=0, nbins=256),
+}
+
+
+def make_large(index):
+    index.setdefault("large", {})
+    for name, c in LARGE_CASES.items():
+        reads, offs = gen_digest_case(c)
+        skm = F.ref_partition(reads, offs, c["k"], c["p"], c["hpc"], c["nbins"], n_threads=os.cpu_count())
+        sd, _, _ = F.skm_digest64(skm.bin, skm.len, skm.byte_off, skm.bytes, c["nbins"])
+        cnt = F.ref_count_bins(skm, c["k"], c["nbins"], n_threads=os.cpu_count())
+        cd, _ = F.counts_digest64(cnt["bin_off"], cnt["keys_lo"], cnt["counts"])
+        d = dict(c)
+        d.update(reads_sha256=P.bytes_digest(reads), n_reads=len(offs) - 1, n_skm=int(len(skm.bin)),
+                 skm_bases=int(skm.len.astype(np.uint64).sum()), n_distinct=int(len(cnt["keys_lo"])),
+                 n_kmers=int(cnt["counts"].astype(np.uint64).sum()),
+                 skm_digest64="%016x" % sd, counts_digest64="%016x" % cd)
+        index["large"][name] = d
+        print(name, d["n_skm"], d["n_distinct"], d["n_kmers"], d["skm_digest64"], d["counts_digest64"])
+
+
 def run_ref(reads, offs, k, p, hpc, nbins):
     skm = F.ref_partition(reads, offs, k, p, hpc, nbins)
     ms = skm.multisets(nbins)
@@ -88,6 +115,13 @@ def run_ref(reads, offs, k, p, hpc, nbins):
 
 def main():
     assert F.ref_available(), "build oracle/_ref first (make -C oracle)"
+    if "--large" in sys.argv:
+        with open(os.path.join(HERE, "golden.json")) as f:
+            index = json.load(f)
+        make_large(index)
+        with open(os.path.join(HERE, "golden.json"), "w") as f:
+            json.dump(index, f, indent=1, sort_keys=True)
+        return
     index = {"full": {}, "digest": {}}
     for name, (gen, k, p, hpc, nbins) in FULL_CASES.items():
         reads, offs = gen()
@@ -116,6 +150,7 @@ def main():
                  counts_sha256=P.counts_digest(cnt["bin_off"], cnt["keys_lo"], cnt["counts"]))
         index["digest"][name] = d
         print(name, n_skm, d["n_distinct"], d["n_kmers"])
+    make_large(index)
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(index, f, indent=1, sort_keys=True)
 

@@ -110,6 +110,8 @@ def reference(filter_id=0):
                                        C.POINTER(RefCounts)]
         lib.ref_pipeline.argtypes = [C.c_char_p, u64p, C.c_int64, C.c_int, C.c_int, C.c_int,
                                      C.c_int, C.c_int, C.c_int, u64p, u64p]
+        lib.ref_pipeline_counts.argtypes = [C.c_char_p, u64p, C.c_int64, C.c_int, C.c_int, C.c_int,
+                                            C.c_int, C.c_int, C.c_int, u64p, C.POINTER(RefCounts)]
         lib.ref_skms_free.argtypes = [C.POINTER(RefSkms)]
         lib.ref_counts_free.argtypes = [C.POINTER(RefCounts)]
         lib.ref_partition_sizes.argtypes = [C.c_char_p, u64p, C.c_int64, C.c_int, C.c_int, C.c_int,
@@ -281,6 +283,61 @@ def ref_pipeline(reads, offs, k, p, hpc, nbins, batch_reads=2048, n_threads=1):
                           int(hpc), nbins, batch_reads, n_threads, _ptr(d, u64p), _ptr(km, u64p))
     assert rc == 0
     return int(d[0]), int(km[0])
+
+
+def ref_pipeline_counts(reads, offs, k, p, hpc, nbins, batch_reads=2048, n_threads=1):
+    """The reference's CPU path with its per-bin sorted (k-mer, count) lists
+    kept (k <= 32); returns (counts dict as ref_count_bins, k-mers)."""
+    lib = reference()
+    reads = np.ascontiguousarray(reads, dtype=np.uint8)
+    offs = np.ascontiguousarray(offs, dtype=np.uint64)
+    km = np.zeros(1, np.uint64)
+    c = RefCounts()
+    rc = lib.ref_pipeline_counts(reads.ctypes.data_as(C.c_char_p), _ptr(offs, u64p), len(offs) - 1, k, p,
+                                 int(hpc), nbins, batch_reads, n_threads, _ptr(km, u64p), C.byref(c))
+    assert rc == 0
+    res = dict(bin_off=_arr(c.bin_off, nbins + 1, np.uint64),
+               keys_lo=_arr(c.keys, c.n_distinct, np.uint64),
+               counts=_arr(c.counts, c.n_distinct, np.uint32), keys_hi=None)
+    lib.ref_counts_free(C.byref(c))
+    return res, int(km[0])
+
+
+def counts_digest64(bin_off, keys_lo, counts, keys_hi=None):
+    """(digest over all bins, per-bin digests) of per-bin sorted (k-mer,
+    count) lists; the same function digests the GPU's and the reference's."""
+    lib = oracle()
+    lib.orc_counts_digest.restype = C.c_uint64
+    lib.orc_counts_digest.argtypes = [u64p, C.c_uint32, u64p, u64p, u32p, u64p]
+    bo = np.ascontiguousarray(bin_off, np.uint64)
+    kl = np.ascontiguousarray(keys_lo, np.uint64)
+    kh = None if keys_hi is None else np.ascontiguousarray(keys_hi, np.uint64)
+    cn = np.ascontiguousarray(counts, np.uint32)
+    nb = len(bo) - 1
+    per = np.zeros(max(nb, 1), np.uint64)
+    if len(kl) == 0:
+        kl = np.zeros(1, np.uint64)
+        cn = np.zeros(1, np.uint32)
+    tot = lib.orc_counts_digest(_ptr(bo, u64p), nb, _ptr(kl, u64p), None if kh is None else _ptr(kh, u64p),
+                                _ptr(cn, u32p), _ptr(per, u64p))
+    return int(tot), per[:nb]
+
+
+def skm_digest64(bins, lens, byte_off, data, nbins):
+    """(digest, per-bin digests, per-bin counts) of a partition as per-bin
+    multisets of (length, packed bytes)."""
+    lib = oracle()
+    lib.orc_skm_multiset_digest.restype = C.c_uint64
+    lib.orc_skm_multiset_digest.argtypes = [u32p, u32p, u64p, u8p, C.c_uint64, C.c_uint32, u64p, u64p]
+    b = np.ascontiguousarray(bins, np.uint32)
+    ln = np.ascontiguousarray(lens, np.uint32)
+    bo = np.ascontiguousarray(byte_off, np.uint64)
+    d = np.ascontiguousarray(data if len(data) else np.zeros(1, np.uint8), np.uint8)
+    per = np.zeros(nbins, np.uint64)
+    cnt = np.zeros(nbins, np.uint64)
+    tot = lib.orc_skm_multiset_digest(_ptr(b, u32p), _ptr(ln, u32p), _ptr(bo, u64p), _ptr(d, u8p), len(b),
+                                      nbins, _ptr(per, u64p), _ptr(cnt, u64p))
+    return int(tot), per, cnt
 
 
 class OrcBalance(C.Structure):

@@ -19,6 +19,7 @@ import numpy as np
 import pytest
 
 import gkc_b200 as G
+import oracle_ffi as F
 
 pytestmark = pytest.mark.gpu
 
@@ -102,6 +103,55 @@ def test_two_calls_in_a_row_match_the_allocating_entry_point(torch, ctx):
         assert np.array_equal(counts, want_counts)
         assert int(counts.astype(np.int64).sum()) == n_kmers_of(lens, k)
         assert counts.max() > 1
+        # and against the oracle's count of the same group
+        boff = np.zeros(len(lens), np.uint64)
+        boff[1:] = np.cumsum((lens.astype(np.uint64) + 3) // 4)[:-1]
+        want = F.oracle_count_bins(F.Skms(np.zeros(len(lens), np.uint32), lens, boff, packed), k, 1)
+        assert np.array_equal(keys, want["keys_lo"])
+        assert np.array_equal(counts, want["counts"])
+
+
+def test_a_call_allocates_no_device_memory(torch):
+    k = 31
+    lens, packed = superkmer_group(21, 4000, k, 20, 120)
+    d_lens = torch.from_numpy(lens.astype(np.uint32).view(np.int32)).cuda()
+    d_packed = torch.from_numpy(packed).cuda()
+    cap = n_kmers_of(lens, k)
+    d_keys = torch.zeros(cap, dtype=torch.int64, device="cuda")
+    d_counts = torch.zeros(cap, dtype=torch.int32, device="cuda")
+    nd = C.c_uint64(0)
+
+    def call():
+        return G.lib().gkc_count_superkmers_device_noalloc(
+            k, d_lens.data_ptr(), d_packed.data_ptr(), len(lens), cap, d_keys.data_ptr(),
+            d_counts.data_ptr(), C.byref(nd), None)
+
+    assert call() == GKC_OK  # first call on the device: set-up
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    assert call() == GKC_OK
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
+def test_a_capturing_stream_is_refused(torch):
+    k = 31
+    lens, packed = superkmer_group(22, 100, k, 40, 60)
+    d_lens = torch.from_numpy(lens.astype(np.uint32).view(np.int32)).cuda()
+    d_packed = torch.from_numpy(packed).cuda()
+    cap = n_kmers_of(lens, k)
+    d_keys = torch.zeros(cap, dtype=torch.int64, device="cuda")
+    d_counts = torch.zeros(cap, dtype=torch.int32, device="cuda")
+    nd = C.c_uint64(0)
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        st = G.lib().gkc_count_superkmers_device_noalloc(
+            k, d_lens.data_ptr(), d_packed.data_ptr(), len(lens), cap, d_keys.data_ptr(),
+            d_counts.data_ptr(), C.byref(nd), C.c_void_p(s.cuda_stream))
+    assert st == GKC_ERR_INVALID_ARG
+    del g
 
 
 def test_group_at_the_kmer_limit(torch, ctx):
