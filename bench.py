@@ -70,6 +70,8 @@ def parse():
                     help="only the serving mix (config 5): 1000 jobs at 50/80/95%% load")
     ap.add_argument("--serve-jobs", type=int, default=None)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default count-stage shapes instead of tuning them on a sample first")
     ap.add_argument("--multi", default=None, choices=["shard", "replicas"],
                     help="bins sharded by owner with a superkmer exchange (default when N > 1; "
                          "also runs with one rank when given), or independent replicas")
@@ -477,6 +479,16 @@ def run_ours(args, wl):
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
 
+    # launch shapes of the count stage, chosen by timing candidates on a
+    # sample of the reads (outside the timed region)
+    tune = None
+    if not args.no_tune:
+        rep = ctx.autotune_device(reads, n_bases, offs, n_reads, prm, force=True)
+        tune = {"chosen": rep.chosen.as_dict(), "defaults": rep.defaults.as_dict(),
+                "sample_bases": int(rep.sample_bases), "candidates": int(rep.candidates),
+                "count_ms_sample_default": float(rep.default_ms), "count_ms_sample_tuned": float(rep.tuned_ms),
+                "tuned_over_default": float(rep.default_ms / rep.tuned_ms) if rep.tuned_ms > 0 else None}
+
     def step():
         return ctx.pipeline_device(reads, n_bases, offs, n_reads, prm, G.MODE_BATCHED)
 
@@ -551,6 +563,8 @@ def run_ours(args, wl):
         "config": config_dict(args, wl, n_reads, n_bases), "roofline": roofline,
         "pipeline": pipeline, "stages_ms": stages, "gpu_launches": launches, "clocks": clocks,
     }
+    if tune is not None:
+        result["tune"] = tune
 
     # plain per-stage form on the same input, its whole output compared with
     # the batched one on the device (bin offsets, every key and count)

@@ -87,6 +87,21 @@ class JobInfo(C.Structure):
                 ("end_s", C.c_double), ("hbm_bytes", C.c_uint64)]
 
 
+class TuneParams(C.Structure):
+    _fields_ = [("coarse_target", C.c_uint32), ("chunk_kmers", C.c_uint32),
+                ("count_ctas_per_sm", C.c_uint32), ("reserved", C.c_uint32)]
+
+    def as_dict(self):
+        return {"coarse_target": int(self.coarse_target), "chunk_kmers": int(self.chunk_kmers),
+                "count_ctas_per_sm": int(self.count_ctas_per_sm)}
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("chosen", TuneParams), ("defaults", TuneParams), ("default_ms", C.c_float),
+                ("tuned_ms", C.c_float), ("candidates", C.c_uint32), ("from_cache", C.c_int),
+                ("sample_bases", C.c_uint64)]
+
+
 # (name, restype, argtypes) for every exported symbol of include/gkc/gkc.h
 vp, u64, u32, i32, dbl = C.c_void_p, C.c_uint64, C.c_uint32, C.c_int, C.c_double
 P = C.POINTER
@@ -114,6 +129,14 @@ SIGNATURES = [
     ("gkc_count_copy_out", C.c_int, [vp, vp, vp, vp]),
     ("gkc_count_output", C.c_int, [vp, u32, u32, C.c_int, P(u64), vp, vp, vp]),
     ("gkc_count_superkmers_device_noalloc", C.c_int, [C.c_int, vp, vp, u64, u64, vp, vp, P(u64), vp]),
+    ("gkc_tune_get", C.c_int, [vp, P(TuneParams)]),
+    ("gkc_tune_set", C.c_int, [vp, P(TuneParams)]),
+    ("gkc_autotune_device", C.c_int, [vp, P(Params), vp, u64, vp, u64, C.c_int, P(TuneReport)]),
+    ("gkc_tune_cache_lookup", C.c_int, [C.c_int, P(Params), u64, u64, P(TuneParams)]),
+    ("gkc_tune_cache_store", C.c_int, [C.c_int, P(Params), u64, u64, P(TuneParams)]),
+    ("gkc_tune_cache_clear", None, []),
+    ("gkc_tune_cache_save", C.c_int, [C.c_char_p]),
+    ("gkc_tune_cache_load", C.c_int, [C.c_char_p]),
     ("gkc_pipeline_device", C.c_int, [vp, P(Params), C.c_int, vp, u64, vp, u64, P(PartitionView),
                                       P(CountView)]),
     ("gkc_pipeline_host", C.c_int, [vp, P(Params), C.c_int, vp, vp, u64, P(CountView)]),
@@ -340,6 +363,24 @@ class Context:
                                              C.byref(n), _ptr(bin_off), _ptr(keys), _ptr(counts)),
                     "count_output")
         return bin_off, keys[:nn * key_words].reshape(nn, key_words), counts[:nn]
+
+    # ---- launch-shape tuning ----
+    def tune_get(self):
+        t = TuneParams()
+        self._check(self._L.gkc_tune_get(self.h, C.byref(t)), "tune_get")
+        return t
+
+    def tune_set(self, tp=None):
+        self._check(self._L.gkc_tune_set(self.h, C.byref(tp) if tp is not None else None), "tune_set")
+
+    def autotune_device(self, d_reads, n_bytes, d_offs, n_reads, prm, force=False):
+        """Times candidate count-stage shapes on a sample of the reads and
+        keeps the fastest on this context; -> TuneReport."""
+        r = TuneReport()
+        self._check(self._L.gkc_autotune_device(self.h, C.byref(prm), _ptr(d_reads), int(n_bytes),
+                                                _ptr(d_offs), int(n_reads), int(bool(force)), C.byref(r)),
+                    "autotune_device")
+        return r
 
     # ---- pipeline ----
     def pipeline_device(self, d_reads, n_bytes, d_offs, n_reads, prm, mode=MODE_BATCHED):

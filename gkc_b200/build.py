@@ -57,5 +57,34 @@ def build(force=False, verbose=False):
     return LIB
 
 
+COMPAT_SRC = os.path.join(HERE, "compat", "gkc_compat.cpp")
+COMPAT_DIR = os.path.join(BUILD, "compat")
+COMPAT_LIB = os.path.join(COMPAT_DIR, "libgkc_compat.so")
+COMPAT_DRIVER = os.path.join(COMPAT_DIR, "compat_driver")
+
+
+def build_compat(gkc_src_dir):
+    """Compiles the drop-in for GKC's GPU entry points (compat/gkc_compat.cpp)
+    as C++14 against the GKC source tree's own headers (gkc_cuda.hpp,
+    kmer_counting.hpp, superkmers.hpp), as a GKC build would, into
+    _build/compat/libgkc_compat.so, plus the test driver that uses it the way
+    GKC's driver does.  Returns the library path."""
+    os.makedirs(COMPAT_DIR, exist_ok=True)
+    lib = build()
+    cuda = os.path.dirname(os.path.dirname(NVCC))
+    inc = ["-I" + gkc_src_dir, "-I" + os.path.join(HERE, "..", "include"), "-I" + os.path.join(cuda, "include")]
+    link = ["-L" + HERE, "-lgkc_b200", "-L" + os.path.join(cuda, "lib64"), "-lcudart", "-lpthread",
+            "-Wl,-rpath," + HERE + ":" + COMPAT_DIR + ":" + os.path.join(cuda, "lib64")]
+    cmds = [["g++", "-std=c++14", "-O2", "-fPIC", "-shared", "-w"] + inc + [COMPAT_SRC, "-o", COMPAT_LIB] + link,
+            ["g++", "-std=c++14", "-O2", "-w"] + inc +
+            [os.path.join(HERE, "..", "tests", "c_consumer", "compat_driver.cpp"), "-o", COMPAT_DRIVER,
+             "-L" + COMPAT_DIR, "-lgkc_compat"] + link]
+    for cmd in cmds:
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("compat build failed:\n" + " ".join(cmd) + "\n" + r.stderr)
+    return COMPAT_LIB
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

@@ -41,7 +41,7 @@ int gkc_abi_version(void) { return GKC_ABI_VERSION; }
 
 // Stages of the batched pipeline, bounded by events sev[i] .. sev[i+1].
 static const char *kStageNames[] = {"prepare", "partition", "bin_scatter", "coarse_hist",
-                                    "coarse_scatter", "coarse_count", "compact"};
+                                    "coarse_scatter", "coarse_count", "finish"};
 constexpr int kNumStages = 7;
 const char *gkc_stage_name(int i) { return (i >= 0 && i < kNumStages) ? kStageNames[i] : ""; }
 
@@ -228,10 +228,11 @@ gkc_status gkc_ctx_create(int device_id, uint64_t hbm_budget_bytes, gkc_ctx **ou
   // and never per launch, where one thread could lower it between another
   // thread's setting and launch.
   if (set_dyn_smem_limit((const void *)k_partition, c->max_smem_optin) != cudaSuccess ||
-      set_dyn_smem_limit((const void *)k_coarse_count<uint64_t>, c->max_smem_optin) != cudaSuccess ||
-      set_dyn_smem_limit((const void *)k_coarse_count<u128>, c->max_smem_optin) != cudaSuccess ||
-      set_dyn_smem_limit((const void *)k_coarse_scatter<uint64_t>, c->max_smem_optin) != cudaSuccess ||
-      set_dyn_smem_limit((const void *)k_coarse_scatter<u128>, c->max_smem_optin) != cudaSuccess) {
+      set_dyn_smem_limit((const void *)k_bin_place, c->max_smem_optin) != cudaSuccess ||
+      set_dyn_smem_limit((const void *)k_bucket_count<uint64_t>, c->max_smem_optin) != cudaSuccess ||
+      set_dyn_smem_limit((const void *)k_bucket_count<u128>, c->max_smem_optin) != cudaSuccess ||
+      set_dyn_smem_limit((const void *)k_bucket_scatter<uint64_t>, c->max_smem_optin) != cudaSuccess ||
+      set_dyn_smem_limit((const void *)k_bucket_scatter<u128>, c->max_smem_optin) != cudaSuccess) {
     cudaGetLastError();
     delete c;
     return GKC_ERR_CUDA;
@@ -370,11 +371,11 @@ uint64_t gkc_job_hbm_estimate(const gkc_params *prm, uint64_t n_bases, uint64_t 
   const uint64_t kc = std::max<uint64_t>(B, 16);
   uint32_t max_bits = kCoarseMaxBits;
   while (max_bits > 0 && ((uint64_t)prm->nbins << max_bits) > (1ull << 20)) max_bits--;
-  const uint64_t hist_cap = ((kc / kChunkKmers) + prm->nbins + 1) << max_bits;
-  e += 16 * hist_cap;                                                    // chunk matrices
-  e += w * kc * 2 + 4 * kc * 2;                                          // keys, runs, counts
-  e += 2 * w * (kc / 16) + 24 * 4096 * 4;                                // sort scratch
-  e += ((uint64_t)prm->nbins << max_bits) * 8 * 4;                       // coarse buckets
+  const uint64_t chunks = kc / 32768 + prm->nbins + 1;  // the smallest chunk the tuner picks
+  e += 4 * (chunks << max_bits) + 8 * chunks;                            // chunk matrix, first superkmers
+  e += w * kc * 2 + 4 * kc;                                              // keys, output keys, counts
+  e += w * std::max<uint64_t>(kc / 16, 1 << 16);                         // oversized-bucket scratch
+  e += ((uint64_t)prm->nbins << max_bits) * 8 * 3;                       // bucket starts, sizes, look-back
   return e + (64ull << 20);
 }
 
@@ -480,7 +481,8 @@ static gkc_status enqueue_partition(gkc_ctx *c, const gkc_params *prm, const cha
     LAUNCHED(c);
     scan_u64(bmat, boff, cells, btmp, c->st);
     c->launches += 4;
-    k_bin_place<<<g, 256, nbins * 8, c->st>>>(tot, desc, mm, nbins, nch_cap, boff, bdesc, bmm, err);
+    k_bin_place<<<(unsigned)std::min<uint64_t>(nch_cap, (uint64_t)c->n_sms * 2), kBinPlaceThreads,
+                  bin_place_smem_bytes(nbins), c->st>>>(tot, desc, mm, nbins, nch_cap, boff, bdesc, bmm, err);
     LAUNCHED(c);
   } else {
     WS(bfill, unsigned long long, "bin_fill", nbins + 1);
@@ -533,12 +535,9 @@ static gkc_status read_totals(gkc_ctx *c, bool with_count, uint32_t nbins) {
 
 static gkc_status check_device_err(gkc_ctx *c) {
   uint32_t e = c->h_tot->err;
-  if (e & ERR_BOUNDS) {
-    unsigned long long d[3] = {0, 0, 0};
-    cudaMemcpy(d, c->bufs["dbg"].p, sizeof(d), cudaMemcpyDeviceToHost);
-    return ctx_fail(c, GKC_ERR_INTERNAL, "device bounds check " + std::to_string(d[0]) + " failed: index " +
-                                             std::to_string(d[1]) + " limit " + std::to_string(d[2]));
-  }
+  if (e & ERR_BIN_TOO_LARGE)
+    return ctx_fail(c, GKC_ERR_CAPACITY, "a bin holds 2^32 or more k-mers: use more bins");
+  if (e & ERR_BOUNDS) return ctx_fail(c, GKC_ERR_INTERNAL, "device bounds check failed");
   if (e & ERR_SPIN_TIMEOUT) return ctx_fail(c, GKC_ERR_DEVICE_TIMEOUT, "device look-back wait timed out");
   if (e & ERR_BAD_READ) return ctx_fail(c, GKC_ERR_INVALID_ARG, "read longer than supported");
   return GKC_OK;
@@ -598,7 +597,6 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   uint32_t max_bits = kCoarseMaxBits;
   while (max_bits > 0 && ((uint64_t)nbins << max_bits) > (1ull << 20)) max_bits--;
   const uint64_t max_buckets = (uint64_t)nbins << max_bits;
-  const int cap = sort_count_cap<K>();
   const uint64_t cap_skm = std::max<uint64_t>(c->part_cap_skm, 1);
   WS(err, uint32_t, "err", 4);
   const unsigned long long *n_skm_dev = (const unsigned long long *)c->bufs["cursors"].p;
@@ -610,7 +608,7 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   stage_mark(c, 3);
   WS(nk, unsigned long long, "skm_nk", cap_skm + 1);
   WS(koff, uint64_t, "skm_koff", cap_skm + 2);
-  WS(stmp, uint64_t, "scan_tmp2", scan_u64_tmp_words(std::max<uint64_t>(cap_skm, max_buckets) + 1) + 8);
+  WS(stmp, uint64_t, "scan_tmp2", scan_u64_tmp_words(cap_skm + 1) + 8);
   k_skm_nk<<<c->n_sms * 8, 256, 0, c->st>>>(desc, n_skm_dev, prm->k, nk);
   LAUNCHED(c);
   scan_u64_dev(nk, koff, cap_skm, (const uint64_t *)n_skm_dev, stmp, c->st);
@@ -624,10 +622,10 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   pl.nbins = nbins;
   pl.bin_start = bin_start;
   pl.bin_kstart = bin_kstart;
-  pl.coarse_target = kCoarseTarget;
-  if (getenv("GKC_COARSE_TARGET")) pl.coarse_target = (uint32_t)atoi(getenv("GKC_COARSE_TARGET"));
+  pl.coarse_target = c->tune.coarse_target ? c->tune.coarse_target : kCoarseTarget;
   pl.max_bits = max_bits;
-  pl.chunk_kmers = kChunkKmers;
+  const uint64_t chunk_kmers = c->tune.chunk_kmers ? c->tune.chunk_kmers : kChunkKmers;
+  pl.chunk_kmers = chunk_kmers;
   pl.k = prm->k;
   pl.err = err;
   pl.bin_bits = bin_bits;
@@ -637,11 +635,13 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   k_count_plan<<<1, 32, 0, c->st>>>(pl);
   LAUNCHED(c);
 
-  const uint64_t hist_cap = ((keys_cap / kChunkKmers) + nbins + 1) << max_bits;
-  WS(chunk_hist, unsigned long long, "chunk_hist", hist_cap + 1);
-  WS(chunk_off, uint64_t, "chunk_off", hist_cap + 2);
-  WS(stmp4, uint64_t, "scan_tmp4", scan_u64_tmp_words(hist_cap + 1) + 8);
+  // chunks: at most keys_cap / kChunkKmers + nbins; histogram cells: chunks << max_bits
+  const uint64_t max_chunks = keys_cap / chunk_kmers + nbins + 1;
+  WS(chunk_s0, uint64_t, "chunk_s0", max_chunks);
+  WS(hist, uint32_t, "bucket_hist", max_chunks << max_bits);
   WS(keys, K, "keys", keys_cap);
+  WS(bstart, uint64_t, "bucket_start", max_buckets + 1);
+  WS(bsize, uint64_t, "bucket_size", max_buckets + 1);
   ExpandArgs ea;
   memset(&ea, 0, sizeof(ea));
   ea.desc = desc;
@@ -652,98 +652,73 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   ea.bin_kstart = bin_kstart;
   ea.chunk_base = chunk_base;
   ea.hist_base = hist_base;
+  ea.bucket_base = bucket_base;
   ea.bin_bits = bin_bits;
-  ea.max_bits = max_bits;
-  ea.chunk_kmers = kChunkKmers;
+  ea.chunk_kmers = chunk_kmers;
   ea.k = prm->k;
-  ea.chunk_hist = chunk_hist;
-  ea.chunk_off = chunk_off;
+  ea.chunk_s0 = chunk_s0;
+  ea.hist = hist;
   ea.keys = keys;
   ea.keys_cap = keys_cap;
   ea.err = err;
-  const unsigned ex_grid = c->n_sms * 8;
-  k_coarse_hist<K><<<ex_grid, 256, (1u << max_bits) * 4, c->st>>>(ea);
+  k_chunk_first<<<(unsigned)std::min<uint64_t>((max_chunks + 255) / 256, 65535), 256, 0, c->st>>>(ea);
   LAUNCHED(c);
-  scan_u64_dev(chunk_hist, chunk_off, hist_cap, hist_base + nbins, stmp4, c->st);
-  c->launches += 4;
+  k_bucket_hist<<<c->n_sms * 8, kBucketHistThreads, 0, c->st>>>(ea);
+  LAUNCHED(c);
+  k_bucket_scan<<<std::min<uint32_t>(nbins, 65535), kBucketScanThreads, 0, c->st>>>(ea, bstart, bsize);
+  LAUNCHED(c);
   stage_mark(c, 4);
-  const size_t sct_smem = coarse_scatter_smem_bytes<K>(max_bits);
-  if ((int)sct_smem + 1024 > c->max_smem_optin) return ctx_fail(c, GKC_ERR_INTERNAL, "scatter stage exceeds shared memory");
-  k_coarse_scatter<K><<<c->n_sms, SCT_NT, sct_smem, c->st>>>(ea);
+  const size_t sct_smem = bucket_scatter_smem_bytes<K>();
+  if ((int)sct_smem > c->max_smem_optin) return ctx_fail(c, GKC_ERR_INTERNAL, "scatter stage exceeds shared memory");
+  k_bucket_scatter<K><<<c->n_sms * 2, kBucketScatterThreads, sct_smem, c->st>>>(ea);
   LAUNCHED(c);
 
-  WS(tkeys, K, "tmp_keys", keys_cap);
-  WS(tcounts, uint32_t, "tmp_counts", keys_cap);
-  WS(cstart, uint64_t, "coarse_start", max_buckets + 1);
-  WS(cd, unsigned long long, "coarse_d", max_buckets + 1);
-  WS(cout_, uint64_t, "coarse_out", max_buckets + 2);
-  WS(ticket, unsigned long long, "lb_ticket", 2);
-  scratch_keys = std::max<uint64_t>(scratch_keys, 4ull * cap);
-  WS(scratch, K, "sort_scratch", 2 * scratch_keys);
-  WS(scnt, uint32_t, "sort_scratch_cnt", 24 * 4096);
-  CK(cudaMemsetAsync(ticket, 0, 16, c->st));
+  // counting: one look-back word per bucket; oversized buckets go through the scratch area
+  WS(out_keys, K, "out_keys", keys_cap);
+  WS(out_counts, uint32_t, "counts", keys_cap);
+  WS(lookback, unsigned long long, "lookback", max_buckets + 1);
+  WS(ticket, unsigned long long, "lb_ticket", 4);
+  scratch_keys = std::max<uint64_t>(scratch_keys, 1 << 16);
+  WS(scratch, K, "sort_scratch", scratch_keys);
+  WS(bin_out, uint64_t, "bin_out", nbins + 1);
+  CK(cudaMemsetAsync(ticket, 0, 32, c->st));
+  CK(cudaMemsetAsync(lookback, 0, (max_buckets + 1) * 8, c->st));
   SortCountArgs sa;
   memset(&sa, 0, sizeof(sa));
   sa.nbins = nbins;
   sa.k = prm->k;
   sa.bucket_base = bucket_base;
-  sa.chunk_base = chunk_base;
-  sa.hist_base = hist_base;
   sa.bin_bits = bin_bits;
-  sa.chunk_off = chunk_off;
+  sa.bucket_start = bstart;
+  sa.bucket_size = bsize;
   sa.keys = keys;
-  sa.tmp_keys = tkeys;
-  sa.tmp_counts = tcounts;
-  sa.coarse_start = cstart;
-  sa.coarse_d = cd;
-  sa.ticket = ticket;
-  sa.scratch_lock = ticket + 1;
   sa.scratch = scratch;
   sa.scratch_keys = scratch_keys;
-  sa.scratch_cnt = scnt;
+  sa.scratch_cursor = ticket + 1;
+  sa.out_keys = out_keys;
+  sa.out_counts = out_counts;
+  sa.out_cap = keys_cap;
+  sa.bin_out = bin_out;
+  sa.lookback = lookback;
+  sa.ticket = ticket;
   sa.err = err;
-  sa.probe_limit = 256;
-  sa.tmp_cap = keys_cap;
-  WS(dbg, unsigned long long, "dbg", 8);
-  CK(cudaMemsetAsync(dbg, 0, 64, c->st));
-  sa.dbg = dbg;
-  if (getenv("GKC_PROBE_LIMIT")) sa.probe_limit = atoi(getenv("GKC_PROBE_LIMIT"));
-  sa.prof = nullptr;
-  if (getenv("GKC_PROFILE_SORT")) {
-    WS(prof, unsigned long long, "sort_prof", 32);
-    CK(cudaMemsetAsync(prof, 0, 32 * 8, c->st));
-    sa.prof = prof;
-  }
-  const size_t smem = coarse_smem_bytes<K>();
+  const size_t smem = bucket_count_smem_bytes<K>();
   if ((int)smem > c->max_smem_optin) return ctx_fail(c, GKC_ERR_INTERNAL, "count tables exceed shared memory");
+  int occ = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bucket_count<K>, kBucketCountThreads, smem));
   stage_mark(c, 5);
-  k_coarse_count<K><<<c->n_sms, kSortThreads, smem, c->st>>>(sa);
+  // persistent: every CTA resident at once (the look-back waits only on
+  // buckets taken earlier, by CTAs that are running)
+  const int ctas = std::max(1, std::min(occ, c->tune.count_ctas ? (int)c->tune.count_ctas : 2));
+  k_bucket_count<K><<<c->n_sms * ctas, kBucketCountThreads, smem, c->st>>>(sa);
   LAUNCHED(c);
   stage_mark(c, 6);
-  if (sa.prof && !c->capturing) {
-    unsigned long long h[32];
-    cudaMemcpyAsync(h, sa.prof, sizeof(h), cudaMemcpyDeviceToHost, c->st);
-    cudaStreamSynchronize(c->st);
-    fprintf(stderr,
-            "coarse_count profile: fallback slices=%llu split slices=%llu direct sorts=%llu | cycles of "
-            "thread 0: histogram+placement %llu, plan+insert %llu, clusters %llu, output %llu, sorts %llu\n",
-            h[5], h[6], h[7], h[16], h[17], h[18], h[19], h[20]);
-  }
-  scan_u64_dev(cd, cout_, max_buckets, bucket_base + nbins, stmp, c->st);
-  WS(counts, uint32_t, "counts", keys_cap);
-  k_compact<K><<<c->n_sms * 8, 256, 0, c->st>>>(tkeys, tcounts, cstart, cd, cout_, bucket_base, nbins,
-                                                 keys, counts);
-  LAUNCHED(c);
-  WS(bin_out, uint64_t, "bin_out", nbins + 1);
-  k_bin_out_offsets<<<(nbins + 256) / 256, 256, 0, c->st>>>(cout_, bucket_base, nbins, bin_out);
-  LAUNCHED(c);
-  c->launches += 4;
   c->count_keys_cap = keys_cap;
   return GKC_OK;
 }
 
-// Oversized buckets are sorted through a scratch area; it starts at 1/16 of
-// the keys and grows to the full key count if a bucket does not fit.
+// Oversized buckets are placed through a scratch area; it starts at 1/16 of
+// the keys and grows to the full key count if the oversized buckets need more.
 static gkc_status enqueue_count(gkc_ctx *c, const gkc_params *prm, uint64_t keys_cap) {
   uint64_t scratch = c->scratch_full ? keys_cap : keys_cap / 16;
   if (prm->k <= 32) return enqueue_count_batched<uint64_t>(c, prm, keys_cap, scratch);
@@ -758,7 +733,7 @@ static void fill_count_view(gkc_ctx *c, const gkc_params *prm) {
   v.nbins = (uint32_t)prm->nbins;
   v.key_words = prm->k <= 32 ? 1 : 2;
   v.bin_off = (const uint64_t *)c->bufs["bin_out"].p;
-  v.keys = (const uint64_t *)c->bufs["keys"].p;
+  v.keys = (const uint64_t *)c->bufs["out_keys"].p;
   v.counts = (const uint32_t *)c->bufs["counts"].p;
   c->ck = prm->k;
   c->have_count = true;

@@ -16,6 +16,7 @@ enum : uint32_t {
   ERR_OVERSIZE_SCRATCH = 1u << 2,
   ERR_BAD_READ = 1u << 3,       // a read longer than the supported superkmer length
   ERR_BOUNDS = 1u << 4,         // a device bounds check failed (access skipped)
+  ERR_BIN_TOO_LARGE = 1u << 5,  // a bin holds 2^32 or more k-mers
 };
 
 // Bounded spin limit for any wait on another CTA (~0.5-2 s with backoff).

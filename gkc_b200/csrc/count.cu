@@ -4,28 +4,69 @@
 // every superkmer of a bin, canonicalised as min(x, revcomp(x)), sorted
 // ascending, run-length counted (count clamped to 2^32-1), per bin.
 //
-// Device layout:
-//   1. k_coarse_hist    - each chunk of a bin's k-mer stream (load-balanced:
-//                         every thread expands the same number of k-mers)
-//                         histograms the top `bin_bits[b]` bits of the
-//                         canonical keys; counts go to a (bin, digit, chunk)
-//                         matrix whose exclusive scan gives every chunk its
-//                         write offset per digit -- no global atomics;
-//   2. k_coarse_scatter - re-expands and writes each key into its coarse
-//                         bucket (bin, top bits);
-//   3. k_coarse_count   - persistent, one coarse bucket per iteration: a
-//                         sub-histogram of the next bits plans slices; each
-//                         slice is aggregated in an order-preserving shared
-//                         memory hash table (duplicates meet in one slot, a
-//                         left-to-right scan is ascending once collision
-//                         clusters are sorted) and written as sorted
-//                         (k-mer, count) runs to a staging area;
-//   4. k_compact        - moves each coarse bucket's runs to its final offset.
+// The keys of a bin are split into 2^cb coarse buckets by the top bits of an
+// order-preserving map of the key (eq_map), so a bin's sorted list is the
+// concatenation of its buckets' sorted lists.  Device stages:
+//   1. k_bucket_hist    - per chunk of a bin's k-mers, a histogram of coarse
+//                         digits.  A canonical key's digit depends only on its
+//                         top 32 bits, which are min(top of x, top of
+//                         revcomp x): the first 16 bases and the reverse
+//                         complement of the last 16, two 32-bit rolling
+//                         windows (no 64-bit expansion);
+//   2. k_bucket_scan    - one CTA per bin turns the (chunk, digit) counts
+//                         into each chunk's write offset per digit and each
+//                         bucket's start and size;
+//   3. k_bucket_scatter - expands every k-mer once; each round of a chunk is
+//                         grouped by digit in shared memory and leaves as
+//                         runs of consecutive keys at the chunk's offsets;
+//   4. k_bucket_count   - persistent, one bucket per ticket: counting sort by
+//                         sub-bucket in shared memory, each thread sorting and
+//                         run-length encoding a few sub-buckets, a block scan,
+//                         and the bucket's output offset by decoupled
+//                         look-back over the buckets before it, so the runs
+//                         are written once, to their final place.  A bucket
+//                         larger than shared memory is placed by sub-bucket in
+//                         a scratch area and counted in slices; a single
+//                         sub-bucket too large for a slice is aggregated in a
+//                         shared-memory hash table over key ranges that are
+//                         halved until a range's distinct keys fit.
 #include "common.cuh"
 #include "kernels.h"
-#include "sortsmem.cuh"
 
 namespace gkc {
+
+// ------------------------------------------------------------ key digits
+
+// Top 32 bits of a 2k-bit key, left-aligned when the key is shorter.
+template <typename K>
+GKC_DEV uint32_t key_top32(K x, int key_bits) {
+  return key_bits >= 32 ? (uint32_t)(x >> (key_bits - 32)) : (uint32_t)((uint64_t)x << (32 - key_bits));
+}
+
+// Order-preserving map of a canonical key's top 32 bits t that spreads
+// canonical keys evenly: the canonical key of a uniform k-mer is the smaller
+// of two near-independent uniform values, whose distribution function is
+// 1 - (1 - u)^2; v = 2^32 (1 - (1 - t / 2^32)^2), non-decreasing in t.
+GKC_DEV uint32_t eq_map(uint32_t t) {
+  if (t == 0) return 0;
+  const uint64_t s = (1ull << 32) - t;  // 1 .. 2^32 - 1
+  return (uint32_t)((0ull - s * s) >> 32);
+}
+
+GKC_DEV uint32_t coarse_of(uint32_t v, int cb) { return cb ? v >> (32 - cb) : 0u; }
+
+template <typename K>
+GKC_DEV uint32_t coarse_digit(K x, int key_bits, int cb) {
+  return coarse_of(eq_map(key_top32<K>(x, key_bits)), cb);
+}
+
+// The sb bits of the key's map below its cb coarse bits (cb + sb <= 32).
+template <typename K>
+GKC_DEV uint32_t sub_digit(K x, int key_bits, int cb, int sb) {
+  if (sb == 0) return 0u;
+  const uint32_t v = eq_map(key_top32<K>(x, key_bits));
+  return (v >> (32 - cb - sb)) & ((1u << sb) - 1u);
+}
 
 // ------------------------------------------------------------------ planning
 
@@ -51,224 +92,14 @@ __global__ void k_count_plan(CountPlan pl) {
   pl.hist_base[pl.nbins] = hb;
 }
 
-// ----------------------------------------------------------------- expansion
-
-// The 2k bits of bases [o, o+k) of a packed superkmer starting at byte `off`
-// (2 bits per base, first base in the top bits of its byte).
-template <typename K>
-GKC_DEV K extract_kmer(const uint8_t *packed, uint64_t off, uint32_t o, int k);
-
-template <>
-GKC_DEV uint64_t extract_kmer<uint64_t>(const uint8_t *packed, uint64_t off, uint32_t o, int k) {
-  const uint8_t *p = packed + off + (o >> 2);
-  const int sh = 2 * (o & 3);
-  uint64_t hi = 0;
-#pragma unroll
-  for (int i = 0; i < 8; i++) hi = (hi << 8) | __ldg(p + i);
-  const uint32_t nx = __ldg(p + 8);
-  const uint64_t v = sh ? ((hi << sh) | (nx >> (8 - sh))) : hi;
-  return v >> (64 - 2 * k);
-}
-
-template <>
-GKC_DEV u128 extract_kmer<u128>(const uint8_t *packed, uint64_t off, uint32_t o, int k) {
-  const uint8_t *p = packed + off + (o >> 2);
-  const int sh = 2 * (o & 3);
-  u128 hi = 0;
-#pragma unroll
-  for (int i = 0; i < 16; i++) hi = (hi << 8) | (u128)__ldg(p + i);
-  const uint32_t nx = __ldg(p + 16);
-  const u128 v = sh ? ((hi << sh) | (u128)(nx >> (8 - sh))) : hi;
-  return v >> (128 - 2 * k);
-}
-
-// Calls f(canonical key) for the k-mers with global indices [q0, q1) of the
-// bin-ordered superkmer stream (superkmers [s_lo, s_hi) hold them; koff is
-// the exclusive prefix of their k-mer counts).  The first k-mer of each
-// superkmer segment is extracted whole and reverse-complemented; the rest roll
-// in one base at a time (kmer_counting.cu:99-112, canonical form :33-44).
-template <typename K, typename F>
-GKC_DEV void expand_range(const uint64_t *desc, const uint64_t *koff, const uint8_t *packed,
-                          uint64_t s_lo, uint64_t s_hi, uint64_t q0, uint64_t q1, int k, F &&f) {
-  if (q0 >= q1) return;
-  uint64_t lo = s_lo, hi = s_hi - 1;
-  while (lo < hi) {
-    uint64_t mid = (lo + hi + 1) >> 1;
-    if (koff[mid] <= q0) lo = mid; else hi = mid - 1;
-  }
-  uint64_t s = lo;
-  const K mask = kmer_mask<K>(k);
-  const int top = 2 * k - 2;
-  while (q0 < q1 && s < s_hi) {
-    const uint64_t kb = koff[s], ke = koff[s + 1];
-    if (q0 >= ke) {
-      s++;
-      continue;
-    }
-    const uint64_t off = desc[s] >> 24;
-    const uint32_t o = (uint32_t)(q0 - kb);
-    const uint32_t cnt = (uint32_t)(min(q1, ke) - q0);
-    K x = extract_kmer<K>(packed, off, o, k);
-    K r = revcomp_k<K>(x, k);
-    f(x < r ? x : r);
-    const uint8_t *src = packed + off;
-    uint32_t j = o + (uint32_t)k;
-    uint32_t byte = cnt > 1 ? __ldg(src + (j >> 2)) : 0u;
-    for (uint32_t t = 1; t < cnt; t++, j++) {
-      if ((j & 3u) == 0) byte = __ldg(src + (j >> 2));
-      const uint32_t c = (byte >> (6 - 2 * (j & 3u))) & 3u;
-      x = ((x << 2) | (K)c) & mask;
-      r = (r >> 2) | ((K)(3u - c) << top);
-      f(x < r ? x : r);
-    }
-    q0 += cnt;
-    s++;
-  }
-}
-
 GKC_DEV uint32_t find_bin(const uint64_t *base, uint32_t nbins, uint64_t c) {
   uint32_t lo = 0, hi = nbins - 1;
   while (lo < hi) {
-    uint32_t mid = (lo + hi + 1) >> 1;
+    const uint32_t mid = (lo + hi + 1) >> 1;
     if (base[mid] <= c) lo = mid; else hi = mid - 1;
   }
   return lo;
 }
-
-constexpr int EX_NT = 256;
-
-struct ChunkInfo {
-  uint32_t b, nbits;
-  uint64_t j, nch, q0, q1, s_lo, s_hi;
-};
-
-GKC_DEV ChunkInfo chunk_info(const ExpandArgs &a, uint64_t c) {
-  ChunkInfo ci;
-  ci.b = find_bin(a.chunk_base, a.nbins, c);
-  ci.j = c - a.chunk_base[ci.b];
-  ci.nch = a.chunk_base[ci.b + 1] - a.chunk_base[ci.b];
-  ci.nbits = a.bin_bits[ci.b];
-  const uint64_t k0 = a.bin_kstart[ci.b] + ci.j * a.chunk_kmers;
-  const uint64_t k1 = min(k0 + a.chunk_kmers, a.bin_kstart[ci.b + 1]);
-  const uint64_t per = (k1 - k0 + EX_NT - 1) / EX_NT;
-  ci.q0 = min(k0 + per * threadIdx.x, k1);
-  ci.q1 = min(ci.q0 + per, k1);
-  ci.s_lo = a.bin_start[ci.b];
-  ci.s_hi = a.bin_start[ci.b + 1];
-  return ci;
-}
-
-template <typename K>
-__global__ void __launch_bounds__(EX_NT) k_coarse_hist(ExpandArgs a) {
-  extern __shared__ uint32_t hist[];  // 1 << max bits
-  if (*a.err & (ERR_CAPACITY | ERR_BAD_READ)) return;
-  const uint64_t n_chunks = a.chunk_base[a.nbins];
-  const int key_bits = 2 * a.k;
-  for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
-    const ChunkInfo ci = chunk_info(a, c);
-    const uint32_t nd = 1u << ci.nbits;
-    for (uint32_t d = threadIdx.x; d < nd; d += EX_NT) hist[d] = 0;
-    __syncthreads();
-    expand_range<K>(a.desc, a.koff, a.packed, ci.s_lo, ci.s_hi, ci.q0, ci.q1, a.k, [&](K key) {
-      atomicAdd(&hist[key_digit<K>(key, key_bits, 0, (int)ci.nbits)], 1u);
-    });
-    __syncthreads();
-    unsigned long long *row = a.chunk_hist + a.hist_base[ci.b] + ci.j;
-    for (uint32_t d = threadIdx.x; d < nd; d += EX_NT) row[(uint64_t)d * ci.nch] = hist[d];
-    __syncthreads();
-  }
-}
-
-// Writes every k-mer key at its (bin, coarse digit, chunk) slot.  A chunk is
-// processed in sub-chunks of SctSub<K> k-mers: expanded into shared memory
-// (with a digit histogram), permuted there into digit order, then written out
-// linearly, so that consecutive threads store consecutive keys of one digit's
-// run and global writes come in whole sectors instead of scattered words.
-template <typename K>
-__global__ void __launch_bounds__(SCT_NT) k_coarse_scatter(ExpandArgs a) {
-  constexpr int SUB = SctSub<K>::value;
-  extern __shared__ __align__(16) uint8_t sct_raw[];
-  K *stage = reinterpret_cast<K *>(sct_raw);
-  K *sorted = stage + SUB;
-  unsigned long long *gbase = reinterpret_cast<unsigned long long *>(sorted + SUB);
-  uint32_t *cursor = reinterpret_cast<uint32_t *>(gbase + (1u << a.max_bits));
-  uint32_t *hstart = cursor + (1u << a.max_bits);
-  __shared__ uint32_t tmp[64];
-  __shared__ uint64_t s_first, s_last;
-  if (*a.err & (ERR_CAPACITY | ERR_BAD_READ)) return;
-  K *keys = reinterpret_cast<K *>(a.keys);
-  const uint64_t n_chunks = a.chunk_base[a.nbins];
-  const int key_bits = 2 * a.k;
-  const int tid = threadIdx.x;
-  for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
-    const uint32_t b = find_bin(a.chunk_base, a.nbins, c);
-    const uint64_t j = c - a.chunk_base[b];
-    const uint64_t nch = a.chunk_base[b + 1] - a.chunk_base[b];
-    const uint32_t nbits = a.bin_bits[b], nd = 1u << nbits;
-    const uint64_t k0 = a.bin_kstart[b] + j * a.chunk_kmers;
-    const uint64_t k1 = min(k0 + a.chunk_kmers, a.bin_kstart[b + 1]);
-    const uint64_t s_lo = a.bin_start[b], s_hi = a.bin_start[b + 1];
-    const uint64_t *row = a.chunk_off + a.hist_base[b] + j;
-    for (uint32_t d = tid; d < nd; d += SCT_NT) gbase[d] = row[(uint64_t)d * nch];
-    for (uint64_t q0s = k0; q0s < k1; q0s += SUB) {
-      const uint64_t q1s = min(q0s + SUB, k1);
-      const uint32_t m = (uint32_t)(q1s - q0s);
-      // the superkmers holding k-mers [q0s, q1s): last with koff <= q0s, last with koff < q1s
-      if (tid < 2) {
-        const uint64_t target = tid == 0 ? q0s : q1s - 1;
-        uint64_t lo = s_lo, hi = s_hi - 1;
-        while (lo < hi) {
-          const uint64_t mid = (lo + hi + 1) >> 1;
-          if (a.koff[mid] <= target) lo = mid; else hi = mid - 1;
-        }
-        if (tid == 0) s_first = lo; else s_last = lo;
-      }
-      for (uint32_t d = tid; d < nd; d += SCT_NT) cursor[d] = 0;
-      __syncthreads();
-      // expand into the stage in k-mer order, counting digits
-      const uint32_t per = (m + SCT_NT - 1) / SCT_NT;
-      const uint32_t p0 = min(m, (uint32_t)tid * per), p1 = min(m, p0 + per);
-      uint32_t p = p0;
-      expand_range<K>(a.desc, a.koff, a.packed, s_first, s_last + 1, q0s + p0, q0s + p1, a.k, [&](K key) {
-        stage[p++] = key;
-        atomicAdd(&cursor[key_digit<K>(key, key_bits, 0, (int)nbits)], 1u);
-      });
-      __syncthreads();
-      // digit starts inside the sub-chunk (nd <= SCT_NT: one digit per thread)
-      {
-        const uint32_t v = (uint32_t)tid < nd ? cursor[tid] : 0u;
-        uint32_t total;
-        const uint32_t ex = block_exclusive_scan<SCT_NT>(v, tmp, &total);
-        if ((uint32_t)tid < nd) {
-          hstart[tid] = ex;
-          cursor[tid] = ex;
-        }
-      }
-      __syncthreads();
-      for (uint32_t i = tid; i < m; i += SCT_NT) {
-        const K x = stage[i];
-        sorted[atomicAdd(&cursor[key_digit<K>(x, key_bits, 0, (int)nbits)], 1u)] = x;
-      }
-      __syncthreads();
-      for (uint32_t i = tid; i < m; i += SCT_NT) {
-        const K x = sorted[i];
-        const uint32_t d = key_digit<K>(x, key_bits, 0, (int)nbits);
-        const uint64_t slot = gbase[d] + (i - hstart[d]);
-        if (slot < a.keys_cap) keys[slot] = x;
-        else atomicOr(a.err, ERR_CAPACITY);
-      }
-      __syncthreads();
-      for (uint32_t d = tid; d < nd; d += SCT_NT) gbase[d] += cursor[d] - hstart[d];
-      __syncthreads();
-    }
-  }
-}
-
-template <typename K> size_t coarse_scatter_smem_bytes(uint32_t max_bits) {
-  return 2 * (size_t)SctSub<K>::value * sizeof(K) + ((size_t)1 << max_bits) * 16;
-}
-template size_t coarse_scatter_smem_bytes<uint64_t>(uint32_t);
-template size_t coarse_scatter_smem_bytes<u128>(uint32_t);
 
 // Number of k-mers of each bin-ordered superkmer (for the k-mer prefix).
 __global__ void k_skm_nk(const uint64_t *desc, const unsigned long long *n_skm_dev, int k,
@@ -281,89 +112,463 @@ __global__ void k_skm_nk(const uint64_t *desc, const unsigned long long *n_skm_d
   }
 }
 
-// ------------------------------------------- coarse bucket: hash-aggregate sort
+// First superkmer of every chunk: the last superkmer of the bin whose k-mer
+// prefix is at most the chunk's first k-mer.
+__global__ void k_chunk_first(ExpandArgs a) {
+  if (*a.err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
+  const uint64_t n_chunks = a.chunk_base[a.nbins];
+  for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < n_chunks;
+       c += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t b = find_bin(a.chunk_base, a.nbins, c);
+    const uint64_t q0 = a.bin_kstart[b] + (c - a.chunk_base[b]) * a.chunk_kmers;
+    uint64_t lo = a.bin_start[b], hi = a.bin_start[b + 1] - 1;
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi + 1) >> 1;
+      if (a.koff[mid] <= q0) lo = mid; else hi = mid - 1;
+    }
+    a.chunk_s0[c] = lo;
+  }
+}
 
-// Order-preserving shared-memory hash table: a key's home slot is a monotone
-// function of the key (piecewise linear over the slice's sub-buckets, each
-// given slots in proportion to its keys), so duplicates meet in one slot and a
-// left-to-right scan is ascending once each run of occupied slots (a
-// collision cluster) is sorted: every key of a cluster has its home inside
-// it, so clusters are mutually ordered.
-template <typename K> struct SliceTab;
-template <> struct SliceTab<uint64_t> { static constexpr int TS = 16384, OVF = 512; };
-template <> struct SliceTab<u128> { static constexpr int TS = 8192, OVF = 512; };
-constexpr int CC_SUB_BITS = 11;        // sub-histogram inside a coarse bucket
-constexpr int CC_NSUB = 1 << CC_SUB_BITS;
-constexpr int SL_PROBE_LIMIT = 256;
-constexpr int SL_CLUSTER_LIMIT = 512;
-constexpr int SL_LOW_BITS = 20;
-constexpr int kSliceStack = 32;  // > 2 * log2(CC_NSUB) + 1: splits halve a slice's keys
-// clusters longer than CW_MIN slots are sorted by a warp (up to CW_LIST a slice)
-constexpr int CW_MIN = 16;
-constexpr int CW_LIST = 128;
-static_assert(SL_CLUSTER_LIMIT < 1024, "cluster lengths are packed in 10 bits");
+// -------------------------------------------------------- superkmer rounds
 
-template <typename K>
-struct CoarseSmem {
-  static constexpr int TSO = SliceTab<K>::TS + SliceTab<K>::OVF;
-  union {
-    struct {
-      K key[TSO];
-      uint32_t cnt[TSO];
-    } t;
-    SortSmem<K> s;  // fallback sort layout
-  } u;
-  uint32_t sub[CC_NSUB + 2];        // sub-bucket counts, then first placed keys
-  uint32_t slot_base[CC_NSUB + 1];
-  uint16_t slo[CC_NSUB + 1];        // first sub-bucket of each slice
-  uint32_t tmp[64];
-  uint64_t g, start, n, run;
-  uint32_t b, nsl, cursor;
-  int overflow;
-  int sp;                    // slice stack: (first << 16) | end sub-bucket
-  uint32_t stk[kSliceStack];
-  uint64_t tot_n, tot_d;     // keys and distinct keys of this CTA's slices so far
-  int sort_mode;
-  int dirty;                 // the table memory was reused by a sort
-  uint32_t occ[(TSO + 31) / 32];  // occupied table slots
-  unsigned long long ph[8];  // phase cycles (profiling only)
-  uint32_t nbig;             // long clusters: (first slot << 10) | length
-  uint32_t bigl[CW_LIST];
+// The superkmers of one round of a chunk, staged in shared memory: k-mer
+// starts relative to the round's first k-mer (clamped above) and packed byte
+// offsets.  At most MAXS superkmers: a round ends early where they run out.
+template <int MAXS>
+struct SkmRound {
+  int32_t koff[MAXS + 1];
+  uint64_t off[MAXS];
+  uint32_t ns, m;    // staged superkmers; k-mers in the round
+  uint64_t s_first;  // first staged superkmer (global index)
+  uint64_t s_next;   // first superkmer of the next round
 };
 
-template <typename K> size_t coarse_smem_bytes() { return sizeof(CoarseSmem<K>); }
-template size_t coarse_smem_bytes<uint64_t>();
-template size_t coarse_smem_bytes<u128>();
-
-template <typename K> GKC_DEV K empty_key() { return ~(K)0; }
-
-GKC_DEV uint64_t smem_cas(uint64_t *p, uint64_t cmp, uint64_t val) {
-  return atomicCAS((unsigned long long *)p, (unsigned long long)cmp, (unsigned long long)val);
+// Stages the round that starts at k-mer r0 inside superkmer s_first and
+// sets R.m (<= rmax).  All threads call; ends with a barrier.
+template <int NT, int MAXS>
+GKC_DEV void stage_round(SkmRound<MAXS> &R, const ExpandArgs &a, uint64_t s_first, uint64_t s_hi,
+                         uint64_t r0, uint64_t q1, uint32_t rmax) {
+  const uint32_t ns = (uint32_t)min((uint64_t)(s_hi - s_first), (uint64_t)MAXS);
+  for (uint32_t i = threadIdx.x; i <= ns; i += NT) {
+    const int64_t d = (int64_t)a.koff[s_first + i] - (int64_t)r0;
+    R.koff[i] = (int32_t)min((int64_t)d, (int64_t)rmax + 1);
+    if (i < ns) R.off[i] = a.desc[s_first + i] >> 24;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    R.ns = ns;
+    R.s_first = s_first;
+    int64_t m = min((int64_t)(q1 - r0), (int64_t)rmax);
+    m = min((int64_t)m, (int64_t)R.koff[ns]);
+    R.m = (uint32_t)max(m, (int64_t)0);
+  }
+  __syncthreads();
 }
-GKC_DEV u128 smem_cas(u128 *p, u128 cmp, u128 val) {
-  // 16-byte compare-and-swap on shared memory (sm_90+)
-  uint64_t clo = (uint64_t)cmp, chi = (uint64_t)(cmp >> 64);
-  uint64_t vlo = (uint64_t)val, vhi = (uint64_t)(val >> 64);
-  uint64_t rlo, rhi;
-  unsigned addr = (unsigned)__cvta_generic_to_shared(p);
-  asm volatile(
-      "{\n\t.reg .b128 c, v, r;\n\t"
-      "mov.b128 c, {%2, %3};\n\t"
-      "mov.b128 v, {%4, %5};\n\t"
-      "atom.shared.cas.b128 r, [%6], c, v;\n\t"
-      "mov.b128 {%0, %1}, r;\n\t}"
-      : "=l"(rlo), "=l"(rhi)
-      : "l"(clo), "l"(chi), "l"(vlo), "l"(vhi), "r"(addr)
-      : "memory");
-  return ((u128)rhi << 64) | rlo;
+
+// Staged superkmer holding local k-mer q: the last with koff <= q.
+template <int MAXS>
+GKC_DEV uint32_t round_find(const SkmRound<MAXS> &R, int32_t q) {
+  uint32_t lo = 0, hi = R.ns - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (R.koff[mid] <= q) lo = mid; else hi = mid - 1;
+  }
+  return lo;
 }
+
+// Thread 0, after a round: the next round's first superkmer (the last staged
+// one starting at or before the round's end; past all staged ones when the
+// round held no k-mers, as they all were empty).
+template <int MAXS>
+GKC_DEV void round_advance(SkmRound<MAXS> &R) {
+  R.s_next = R.m == 0 ? R.s_first + R.ns : R.s_first + round_find<MAXS>(R, (int32_t)R.m);
+}
+
+// 16 bases of a packed superkmer from base index pos, first base in the top
+// bits (2 bits per base, MSB first; bytes past the end read as padding).
+GKC_DEV uint32_t bases16(const uint8_t *packed, uint64_t off, uint32_t pos) {
+  const uint8_t *p = packed + off + (pos >> 2);
+  const uint32_t sh = 2 * (pos & 3u);
+  uint32_t v = ((uint32_t)__ldg(p) << 24) | ((uint32_t)__ldg(p + 1) << 16) | ((uint32_t)__ldg(p + 2) << 8) |
+               (uint32_t)__ldg(p + 3);
+  if (sh) v = (v << sh) | ((uint32_t)__ldg(p + 4) >> (8 - sh));
+  return v;
+}
+
+// Reverse complement of the 16 bases of w.
+GKC_DEV uint32_t revcomp16(uint32_t w) {
+  const uint32_t y = __brev(~w);
+  return ((y >> 1) & 0x55555555u) | ((y & 0x55555555u) << 1);
+}
+
+// The 2k bits of bases [o, o+k) of a packed superkmer at byte `off`.
+template <typename K>
+GKC_DEV K extract_kmer(const uint8_t *packed, uint64_t off, uint32_t o, int k);
+
+template <>
+GKC_DEV uint64_t extract_kmer<uint64_t>(const uint8_t *packed, uint64_t off, uint32_t o, int k) {
+  const uint8_t *p = packed + off + (o >> 2);
+  const int sh = 2 * (o & 3);
+  uint64_t hi = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) hi = (hi << 8) | __ldg(p + i);
+  const uint64_t v = sh ? ((hi << sh) | (uint64_t)(__ldg(p + 8) >> (8 - sh))) : hi;
+  return v >> (64 - 2 * k);
+}
+
+template <>
+GKC_DEV u128 extract_kmer<u128>(const uint8_t *packed, uint64_t off, uint32_t o, int k) {
+  const uint8_t *p = packed + off + (o >> 2);
+  const int sh = 2 * (o & 3);
+  u128 hi = 0;
+#pragma unroll
+  for (int i = 0; i < 16; i++) hi = (hi << 8) | (u128)__ldg(p + i);
+  const u128 v = sh ? ((hi << sh) | (u128)(__ldg(p + 16) >> (8 - sh))) : hi;
+  return v >> (128 - 2 * k);
+}
+
+// Bases of a packed superkmer from index j on, each byte read once.
+struct BaseStream {
+  const uint8_t *p;
+  uint32_t j, byte;
+  GKC_DEV void init(const uint8_t *src, uint32_t j0) {
+    p = src;
+    j = j0;
+    byte = __ldg(p + (j >> 2));
+  }
+  GKC_DEV uint32_t next() {
+    if ((j & 3u) == 0) byte = __ldg(p + (j >> 2));
+    const uint32_t c = (byte >> (6 - 2 * (j & 3u))) & 3u;
+    j++;
+    return c;
+  }
+};
+
+// ----------------------------------------------------------- 1. histogram
+
+constexpr int HS_NT = 256;
+constexpr int HS_PER = 16;
+constexpr int HS_R = HS_NT * HS_PER;  // k-mers per round
+constexpr int HS_MAXS = 1024;
+
+__global__ void __launch_bounds__(HS_NT) k_bucket_hist(ExpandArgs a) {
+  __shared__ SkmRound<HS_MAXS> R;
+  __shared__ uint32_t hist[1 << kCoarseMaxBits];
+  if (*a.err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
+  const uint64_t n_chunks = a.chunk_base[a.nbins];
+  const int k = a.k;
+  const int h = k < 16 ? k : 16;  // bases in each 32-bit window
+  const uint32_t hmask = h == 16 ? 0xFFFFFFFFu : ((1u << (2 * h)) - 1u);
+  const int hsh = 32 - 2 * h;
+  for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
+    const uint32_t b = find_bin(a.chunk_base, a.nbins, c);
+    const uint64_t j = c - a.chunk_base[b];
+    const int cb = (int)a.bin_bits[b];
+    const uint32_t nd = 1u << cb;
+    const uint64_t q0 = a.bin_kstart[b] + j * a.chunk_kmers;
+    const uint64_t q1 = min(q0 + a.chunk_kmers, a.bin_kstart[b + 1]);
+    const uint64_t s_hi = a.bin_start[b + 1];
+    for (uint32_t d = threadIdx.x; d < nd; d += HS_NT) hist[d] = 0;
+    uint64_t s_first = a.chunk_s0[c], r0 = q0;
+    while (r0 < q1) {
+      stage_round<HS_NT, HS_MAXS>(R, a, s_first, s_hi, r0, q1, HS_R);
+      if (R.ns == 0) {  // k-mers left but no superkmer: inconsistent offsets
+        if (threadIdx.x == 0) atomicOr(a.err, ERR_BOUNDS);
+        break;
+      }
+      const uint32_t m = R.m;
+      const uint32_t q = threadIdx.x * HS_PER;
+      if (q < m) {
+        const uint32_t qe = min(q + HS_PER, m);
+        uint32_t si = round_find<HS_MAXS>(R, (int32_t)q);
+        uint32_t t = q;
+        while (t < qe) {
+          // k-mers [t, te) lie in superkmer si
+          const uint64_t off = R.off[si];
+          const uint32_t o = (uint32_t)((int32_t)t - R.koff[si]);
+          const uint32_t te = min(qe, (uint32_t)R.koff[si + 1]);
+          uint32_t fw = bases16(a.packed, off, o) >> hsh;
+          uint32_t rc = revcomp16(bases16(a.packed, off, o + k - h)) & hmask;
+          BaseStream sf, sr;
+          sf.init(a.packed + off, o + h);
+          sr.init(a.packed + off, o + k);
+          while (true) {
+            atomicAdd(&hist[coarse_of(eq_map(min(fw, rc) << hsh), cb)], 1u);
+            if (++t >= te) break;
+            fw = ((fw << 2) | sf.next()) & hmask;
+            rc = (rc >> 2) | ((3u - sr.next()) << (2 * h - 2));
+          }
+          si++;
+          while (si < R.ns && R.koff[si + 1] <= (int32_t)t) si++;  // superkmers without k-mers
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) round_advance<HS_MAXS>(R);
+      __syncthreads();
+      s_first = R.s_next;
+      r0 += m;
+    }
+    __syncthreads();
+    // the chunk's row, digits contiguous
+    uint32_t *row = a.hist + a.hist_base[b] + j * nd;
+    for (uint32_t d = threadIdx.x; d < nd; d += HS_NT) row[d] = hist[d];
+    __syncthreads();
+  }
+}
+
+// ----------------------------------------------------------------- 2. scan
+
+// One CTA per bin: column sums of the bin's (chunk, digit) counts, an
+// exclusive scan over digits (the bucket starts), then every chunk's write
+// offset per digit, written over its count; offsets are relative to the
+// bin's first key.
+constexpr int BS_NT = 1024;
+__global__ void __launch_bounds__(BS_NT) k_bucket_scan(ExpandArgs a, uint64_t *bucket_start,
+                                                       uint64_t *bucket_size) {
+  __shared__ uint32_t tmp[64];
+  constexpr int DPT = (1 << kCoarseMaxBits) / BS_NT;
+  if (*a.err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
+  for (uint32_t b = blockIdx.x; b < a.nbins; b += gridDim.x) {
+    const uint32_t nd = 1u << a.bin_bits[b];
+    const uint64_t nch = a.chunk_base[b + 1] - a.chunk_base[b];
+    if (a.bin_kstart[b + 1] - a.bin_kstart[b] >= (1ull << 32)) {  // offsets in a bin are 32-bit
+      if (threadIdx.x == 0) atomicOr(a.err, ERR_BIN_TOO_LARGE);
+      continue;
+    }
+    uint32_t *M = a.hist + a.hist_base[b];
+    // thread t holds the contiguous digits [t * DPT, t * DPT + DPT)
+    uint32_t col[DPT];
+#pragma unroll
+    for (int u = 0; u < DPT; u++) col[u] = 0;
+    for (uint64_t jj = 0; jj < nch; jj++) {
+#pragma unroll
+      for (int u = 0; u < DPT; u++) {
+        const uint32_t d = threadIdx.x * DPT + u;
+        if (d < nd) col[u] += M[jj * nd + d];
+      }
+    }
+    uint32_t s = 0;
+#pragma unroll
+    for (int u = 0; u < DPT; u++) s += col[u];
+    uint32_t tot;
+    uint32_t run = block_exclusive_scan<BS_NT>(s, tmp, &tot);
+    const uint64_t g0 = a.bucket_base[b];
+    uint32_t start[DPT];
+#pragma unroll
+    for (int u = 0; u < DPT; u++) {
+      const uint32_t d = threadIdx.x * DPT + u;
+      start[u] = run;
+      if (d < nd) {
+        bucket_start[g0 + d] = a.bin_kstart[b] + run;
+        bucket_size[g0 + d] = col[u];
+      }
+      run += col[u];
+    }
+    for (uint64_t jj = 0; jj < nch; jj++) {
+#pragma unroll
+      for (int u = 0; u < DPT; u++) {
+        const uint32_t d = threadIdx.x * DPT + u;
+        if (d < nd) {
+          const uint32_t v = M[jj * nd + d];
+          M[jj * nd + d] = start[u];
+          start[u] += v;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// -------------------------------------------------------------- 3. scatter
+
+template <typename K> struct ScatterShape;
+template <> struct ScatterShape<uint64_t> { static constexpr int NT = 512, PER = 8, MAXS = 1024; };
+template <> struct ScatterShape<u128> { static constexpr int NT = 512, PER = 4, MAXS = 512; };
 
 template <typename K>
-GKC_DEV K volatile_load(const K *p) {
-  return *(const volatile K *)p;
+struct ScatterSmem {
+  static constexpr int RR = ScatterShape<K>::NT * ScatterShape<K>::PER;  // k-mers per round
+  static constexpr int ND = 1 << kCoarseMaxBits;
+  K stage[RR];
+  K sorted[RR];
+  uint32_t cnt[ND / 2 + 1];  // two 16-bit counters per word (counts, then cursors)
+  uint16_t lstart[ND];       // digit starts inside the round
+  uint32_t gbase[ND];        // next write position per digit, from the bin's first key
+  uint32_t tmp[64];
+  SkmRound<ScatterShape<K>::MAXS> R;
+};
+
+template <typename K> size_t bucket_scatter_smem_bytes() { return sizeof(ScatterSmem<K>); }
+template size_t bucket_scatter_smem_bytes<uint64_t>();
+template size_t bucket_scatter_smem_bytes<u128>();
+
+// 16-bit counters in pairs: returns the counter's value before the increment.
+GKC_DEV uint32_t cnt16_add(uint32_t *cnt, uint32_t d) {
+  const uint32_t sh = 16 * (d & 1u);
+  return (atomicAdd(&cnt[d >> 1], 1u << sh) >> sh) & 0xFFFFu;
+}
+GKC_DEV uint32_t cnt16_get(const uint32_t *cnt, uint32_t d) { return (cnt[d >> 1] >> (16 * (d & 1u))) & 0xFFFFu; }
+
+template <typename K>
+__global__ void __launch_bounds__(ScatterShape<K>::NT, 2) k_bucket_scatter(ExpandArgs a) {
+  constexpr int NT = ScatterShape<K>::NT, PER = ScatterShape<K>::PER, MAXS = ScatterShape<K>::MAXS;
+  constexpr int RR = ScatterSmem<K>::RR;
+  static_assert(RR < 65536, "16-bit counters");
+  extern __shared__ __align__(16) uint8_t sct_raw[];
+  ScatterSmem<K> &S = *reinterpret_cast<ScatterSmem<K> *>(sct_raw);
+  SkmRound<MAXS> &R = S.R;
+  if (*a.err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
+  K *keys = reinterpret_cast<K *>(a.keys);
+  const uint64_t n_chunks = a.chunk_base[a.nbins];
+  const int k = a.k, key_bits = 2 * k, top = 2 * k - 2;
+  const K mask = kmer_mask<K>(k);
+  const int tid = threadIdx.x;
+  for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
+    const uint32_t b = find_bin(a.chunk_base, a.nbins, c);
+    const uint64_t j = c - a.chunk_base[b];
+    const int cb = (int)a.bin_bits[b];
+    const uint32_t nd = 1u << cb;
+    const uint64_t kbase = a.bin_kstart[b];
+    const uint64_t q0 = kbase + j * a.chunk_kmers;
+    const uint64_t q1 = min(q0 + a.chunk_kmers, a.bin_kstart[b + 1]);
+    const uint64_t s_hi = a.bin_start[b + 1];
+    const uint32_t *row = a.hist + a.hist_base[b] + j * nd;
+    for (uint32_t d = tid; d < nd; d += NT) S.gbase[d] = row[d];
+    uint64_t s_first = a.chunk_s0[c], r0 = q0;
+    while (r0 < q1) {
+      for (uint32_t w = tid; w <= nd / 2; w += NT) S.cnt[w] = 0;
+      stage_round<NT, MAXS>(R, a, s_first, s_hi, r0, q1, RR);
+      if (R.ns == 0) {  // k-mers left but no superkmer: inconsistent offsets
+        if (tid == 0) atomicOr(a.err, ERR_BOUNDS);
+        break;
+      }
+      const uint32_t m = R.m;
+      // expand: thread-contiguous k-mers, staged at e * NT + tid
+      const uint32_t q = tid * PER;
+      if (q < m) {
+        const uint32_t qe = min(q + PER, m);
+        uint32_t si = round_find<MAXS>(R, (int32_t)q);
+        uint32_t t = q, e = 0;
+        while (t < qe) {
+          const uint64_t off = R.off[si];
+          const uint32_t o = (uint32_t)((int32_t)t - R.koff[si]);
+          const uint32_t te = min(qe, (uint32_t)R.koff[si + 1]);
+          K x = extract_kmer<K>(a.packed, off, o, k);
+          K r = revcomp_k<K>(x, k);
+          BaseStream bs;
+          bs.init(a.packed + off, o + k);
+          while (true) {
+            const K key = x < r ? x : r;  // canonicalkmer, kmer_counting.cu:33-44
+            S.stage[e * NT + tid] = key;
+            cnt16_add(S.cnt, coarse_digit<K>(key, key_bits, cb));
+            e++;
+            if (++t >= te) break;
+            const uint32_t cc = bs.next();
+            x = ((x << 2) | (K)cc) & mask;
+            r = (r >> 2) | ((K)(3u - cc) << top);
+          }
+          si++;
+          while (si < R.ns && R.koff[si + 1] <= (int32_t)t) si++;
+        }
+      }
+      __syncthreads();
+      // digit starts inside the round
+      {
+        constexpr int DPT = (1 << kCoarseMaxBits) / NT;
+        uint32_t v[DPT], s = 0;
+#pragma unroll
+        for (int u = 0; u < DPT; u++) {
+          const uint32_t d = tid * DPT + u;
+          v[u] = d < nd ? cnt16_get(S.cnt, d) : 0u;
+          s += v[u];
+        }
+        uint32_t total;
+        uint32_t run = block_exclusive_scan<NT>(s, S.tmp, &total);
+#pragma unroll
+        for (int u = 0; u < DPT; u++) {
+          const uint32_t d = tid * DPT + u;
+          if (d < nd) S.lstart[d] = (uint16_t)run;
+          run += v[u];
+        }
+        __syncthreads();
+        // the counters become cursors, starting at the digit starts
+        for (uint32_t w = tid; w < (nd + 1) / 2; w += NT) {
+          const uint32_t lo = S.lstart[2 * w], hi = 2 * w + 1 < nd ? S.lstart[2 * w + 1] : 0u;
+          S.cnt[w] = lo | (hi << 16);
+        }
+      }
+      __syncthreads();
+      // local k-mer i sits in slot (i % PER) * NT + i / PER
+      for (uint32_t i = tid; i < m; i += NT) {
+        const K x = S.stage[(i % PER) * NT + i / PER];
+        S.sorted[cnt16_add(S.cnt, coarse_digit<K>(x, key_bits, cb))] = x;
+      }
+      __syncthreads();
+      for (uint32_t i = tid; i < m; i += NT) {
+        const K x = S.sorted[i];
+        const uint32_t d = coarse_digit<K>(x, key_bits, cb);
+        const uint64_t slot = kbase + S.gbase[d] + (i - S.lstart[d]);
+        if (slot < a.keys_cap) keys[slot] = x;
+        else atomicOr(a.err, ERR_CAPACITY);
+      }
+      __syncthreads();
+      // the cursors now hold each digit's end inside the round
+      for (uint32_t d = tid; d < nd; d += NT) S.gbase[d] += cnt16_get(S.cnt, d) - S.lstart[d];
+      if (tid == 0) round_advance<MAXS>(R);
+      __syncthreads();
+      s_first = R.s_next;
+      r0 += m;
+      __syncthreads();
+    }
+  }
 }
 
-GKC_DEV void set_overflow(int *f) { *(volatile int *)f = 1; }
+// ---------------------------------------------------------------- 4. count
+
+template <typename K> struct CountShape;
+template <> struct CountShape<uint64_t> { static constexpr int NT = 512, CAP = 8192; };
+template <> struct CountShape<u128> { static constexpr int NT = 512, CAP = 4096; };
+constexpr int CC_SB_MAX = 12;        // sub-bucket bits
+constexpr int CC_NSUB_MAX = 1 << CC_SB_MAX;
+constexpr uint32_t CC_SEG_MAX = 64;  // longer per-thread segments are sorted by warps
+constexpr int CC_BIG_LIST = 128;
+constexpr int CC_STACK = 2 * 129 + 2;  // key-range halving: at most 128 levels, two entries each
+
+// Heavy-slice hash table: keys, counts and a slot state (0 free, 1 being
+// written, 2 holds a key), inside the key area of the shared memory.
+template <typename K> struct HeavyTab {
+  static constexpr int SLOTS = (CountShape<K>::CAP * sizeof(K)) / (sizeof(K) + 8);
+  static constexpr int N = SLOTS >= 4096 ? 4096 : (SLOTS >= 2048 ? 2048 : 1024);
+  K key[N];
+  uint32_t cnt[N];
+  uint32_t state[N];
+};
+
+template <typename K>
+struct CountSmem {
+  static constexpr int CAP = CountShape<K>::CAP, NT = CountShape<K>::NT;
+  union {
+    K A[CAP];  // keys of a bucket or a slice
+    HeavyTab<K> h;
+  } u;
+  // run counts; cursors of the oversized path (as 32-bit words)
+  uint16_t C[CAP > 2 * CC_NSUB_MAX ? CAP : 2 * CC_NSUB_MAX];
+  uint32_t cnt[CC_NSUB_MAX + 1];  // sub-bucket counts, then starts
+  uint32_t seg_pos[NT];           // output position of each thread's runs (exclusive scan)
+  uint32_t seg_src[NT];           // first run of each thread's segment in A
+  uint32_t big[CC_BIG_LIST];      // threads whose segments are sorted by warps
+  uint32_t tmp[64];
+  uint32_t nbig, hfill, nsub;
+  int flag, sp;
+  uint64_t g, start, n, out_base, run, tbase;
+  uint32_t b;
+  K stk_lo[CC_STACK], stk_hi[CC_STACK];
+};
+
+template <typename K> size_t bucket_count_smem_bytes() { return sizeof(CountSmem<K>); }
+template size_t bucket_count_smem_bytes<uint64_t>();
+template size_t bucket_count_smem_bytes<u128>();
 
 GKC_DEV uint64_t globaltimer_ns() {
   uint64_t t;
@@ -371,150 +576,49 @@ GKC_DEV uint64_t globaltimer_ns() {
   return t;
 }
 
-// Bounded spin lock (thread 0 of a CTA): false if the wait ran out.
-GKC_DEV bool acquire_lock(unsigned long long *lock, uint32_t *err) {
+// Look-back words: (flag << 62) | value; flag 1: the bucket's distinct count,
+// flag 2: the inclusive prefix through the bucket.
+constexpr uint64_t LB_AGG = 1ull << 62, LB_INC = 2ull << 62, LB_VAL = (1ull << 62) - 1;
+
+GKC_DEV void lb_publish(unsigned long long *st, uint64_t g, uint64_t word) {
+  __threadfence();
+  atomicExch(st + g, (unsigned long long)word);
+}
+
+// Exclusive prefix of bucket g (one thread): walks back over the published
+// words until an inclusive prefix.  The wait is bounded (about 10 s); when it
+// runs out, ERR_SPIN_TIMEOUT is set and the sum so far returned.
+GKC_DEV uint64_t lb_exclusive(unsigned long long *st, uint64_t g, uint32_t *err) {
+  uint64_t excl = 0;
+  int64_t i = (int64_t)g - 1;
   const uint64_t t0 = globaltimer_ns();
   uint32_t it = 0;
-  while (atomicCAS(lock, 0ull, 1ull) != 0ull) {
-    if (++it > (1u << 24) || globaltimer_ns() - t0 > 10000000000ull) {
+  while (i >= 0) {
+    const uint64_t w = *(volatile unsigned long long *)(st + i);
+    const uint64_t f = w & ~LB_VAL;
+    if (f == LB_INC) {
+      excl += w & LB_VAL;
+      break;
+    }
+    if (f == LB_AGG) {
+      excl += w & LB_VAL;
+      i--;
+      continue;
+    }
+    if (++it > (1u << 26) || globaltimer_ns() - t0 > 10000000000ull) {
       atomicOr(err, ERR_SPIN_TIMEOUT);
-      return false;
+      break;
     }
     nanosleep_backoff(it);
   }
   __threadfence();
-  return true;
+  return excl;
 }
 
-// Records the first failed bounds check (code, index, limit); the caller
-// skips the access.
-GKC_DEV bool in_bounds(const SortCountArgs &a, int code, uint64_t idx, uint64_t lim) {
-  if (idx < lim) return true;
-  if (atomicCAS(a.dbg, 0ull, (unsigned long long)code) == 0ull) {
-    a.dbg[1] = idx;
-    a.dbg[2] = lim;
-  }
-  atomicOr(a.err, ERR_BOUNDS);
-  return false;
-}
-GKC_DEV int get_overflow(const int *f) { return *(const volatile int *)f; }
-
-// Oversized slice fallback: MSD passes through global scratch, depth first in
-// key order; sub-ranges that fit are finished in shared memory.  Input: n keys
-// in scratch half 0.  Output runs are appended at S.out.
+// In-place ascending sort of A[0, m) by one warp (bitonic network whose
+// comparators put the smaller key first, so indices >= m act as +infinity).
 template <typename K>
-GKC_DEV void scratch_sort(SortSmem<K> &S, const SortCountArgs &a, uint64_t n, int skip0,
-                          K *out_keys, uint32_t *out_counts) {
-  const int key_bits = 2 * a.k;
-  const int CAP = SortCap<K>::value;
-  K *half[2] = {reinterpret_cast<K *>(a.scratch), reinterpret_cast<K *>(a.scratch) + a.scratch_keys};
-  if (threadIdx.x == 0) {
-    S.depth = 0;
-    S.fr[0] = {0, n, skip0, 0, 0, 0, 0};
-  }
-  __threadfence_block();
-  __syncthreads();
-  while (S.depth >= 0) {
-    const int dep = S.depth;
-    uint32_t *gc = a.scratch_cnt + (size_t)dep * 4096;
-    if (!S.fr[dep].split) {
-      const uint64_t off = S.fr[dep].off, len = S.fr[dep].len;
-      const int skip = S.fr[dep].skip, src = S.fr[dep].src;
-      const int d = min(SC_DMAX, key_bits - skip);
-      const uint32_t nd = 1u << d;
-      for (uint32_t j = threadIdx.x; j < nd; j += SC_NT) S.cnt[j] = 0;
-      __syncthreads();
-      for (uint64_t i = threadIdx.x; i < len; i += SC_NT)
-        atomicAdd(&S.cnt[key_digit<K>(half[src][off + i], key_bits, skip, d)], 1u);
-      __syncthreads();
-      scan_counters(S.cnt, nd, S.tmp);
-      for (uint64_t i = threadIdx.x; i < len; i += SC_NT) {
-        K x = half[src][off + i];
-        uint32_t pos = atomicAdd(&S.cnt[key_digit<K>(x, key_bits, skip, d)], 1u);
-        if (in_bounds(a, 2, off + pos, a.scratch_keys)) half[1 - src][off + pos] = x;
-      }
-      __syncthreads();
-      if (!in_bounds(a, 3, dep, 24)) return;
-      for (uint32_t j = threadIdx.x; j < nd; j += SC_NT) gc[j] = S.cnt[j];  // leaf ends
-      __threadfence_block();
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        S.fr[dep].split = 1;
-        S.fr[dep].d = d;
-        S.fr[dep].cursor = 0;
-      }
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-      // next action: a run of consecutive children that fits in shared memory
-      // is sorted together (it is contiguous and in key order); a single child
-      // too large to fit is split further, or emitted whole if all its bits
-      // are consumed (all keys equal)
-      S.act = 0;
-      auto &F = S.fr[dep];
-      const uint32_t nd = 1u << F.d;
-      while (F.cursor < nd) {
-        uint32_t j = F.cursor;
-        uint64_t s0 = j ? gc[j - 1] : 0, e = gc[j];
-        if (e == s0) {
-          F.cursor++;
-          continue;
-        }
-        if (e - s0 > (uint64_t)CAP) {
-          F.cursor++;
-          S.c_off = F.off + s0;
-          S.c_len = e - s0;
-          S.c_skip = F.skip + F.d;
-          S.c_src = 1 - F.src;
-          S.act = (S.c_skip >= key_bits) ? 2 : 3;
-          break;
-        }
-        uint32_t jn = j + 1;
-        while (jn < nd && gc[jn] - s0 <= (uint64_t)CAP) jn++;
-        F.cursor = jn;
-        S.c_off = F.off + s0;
-        S.c_len = gc[jn - 1] - s0;
-        S.c_skip = F.skip;  // the run shares only the parent's prefix
-        S.c_src = 1 - F.src;
-        S.act = 1;
-        break;
-      }
-      if (S.act == 3) {
-        S.depth = dep + 1;
-        S.fr[dep + 1] = {S.c_off, S.c_len, S.c_skip, S.c_src, 0, 0, 0};
-      } else if (S.act == 0) {
-        S.depth = dep - 1;
-      }
-    }
-    __syncthreads();
-    const int act = S.act;
-    if (act == 1) {
-      const uint32_t m = (uint32_t)S.c_len;
-      if (!in_bounds(a, 4, m, (uint64_t)CAP + 1) || !in_bounds(a, 5, S.c_off + m, a.scratch_keys + 1)) return;
-      load_keys<K>(S.A, half[S.c_src] + S.c_off, m);
-      __syncthreads();
-      smem_sort<K>(S, m, key_bits, S.c_skip);
-      uint32_t D = smem_runs<K>(S, m);
-      if (!in_bounds(a, 6, S.out + D, a.tmp_cap + 1)) return;
-      write_runs<K>(S, D, out_keys, out_counts, S.out);
-      __syncthreads();
-      if (threadIdx.x == 0) S.out += D;
-    } else if (act == 2) {
-      if (threadIdx.x == 0 && in_bounds(a, 7, S.out, a.tmp_cap)) {
-        out_keys[S.out] = half[S.c_src][S.c_off];
-        out_counts[S.out] = S.c_len > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)S.c_len;
-        S.out += 1;
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// In-place ascending sort of m (key, count) pairs by one warp: a bitonic
-// network in the form where every comparator puts the smaller key at the
-// lower index, so positions >= m act as +infinity.
-template <typename K>
-GKC_DEV void warp_sort_pairs(K *key, uint32_t *cnt, uint32_t m) {
+GKC_DEV void warp_sort(K *A, uint32_t m) {
   uint32_t P = 1;
   while (P < m) P <<= 1;
   const uint32_t lane = threadIdx.x & 31u;
@@ -523,13 +627,12 @@ GKC_DEV void warp_sort_pairs(K *key, uint32_t *cnt, uint32_t m) {
     for (uint32_t i = lane; i < P / 2; i += 32) {
       const uint32_t blk = i / half, off = i % half;
       const uint32_t lo = blk * size + off, hi = blk * size + size - 1 - off;
-      if (hi < m && key[hi] < key[lo]) {
-        const K x = key[lo];
-        key[lo] = key[hi];
-        key[hi] = x;
-        const uint32_t c = cnt[lo];
-        cnt[lo] = cnt[hi];
-        cnt[hi] = c;
+      if (hi < m) {
+        const K x = A[lo], y = A[hi];
+        if (y < x) {
+          A[lo] = y;
+          A[hi] = x;
+        }
       }
     }
     __syncwarp();
@@ -537,13 +640,12 @@ GKC_DEV void warp_sort_pairs(K *key, uint32_t *cnt, uint32_t m) {
       for (uint32_t i = lane; i < P / 2; i += 32) {
         const uint32_t blk = i / stride, off = i % stride;
         const uint32_t lo = blk * 2 * stride + off, hi = lo + stride;
-        if (hi < m && key[hi] < key[lo]) {
-          const K x = key[lo];
-          key[lo] = key[hi];
-          key[hi] = x;
-          const uint32_t c = cnt[lo];
-          cnt[lo] = cnt[hi];
-          cnt[hi] = c;
+        if (hi < m) {
+          const K x = A[lo], y = A[hi];
+          if (y < x) {
+            A[lo] = y;
+            A[hi] = x;
+          }
         }
       }
       __syncwarp();
@@ -551,416 +653,430 @@ GKC_DEV void warp_sort_pairs(K *key, uint32_t *cnt, uint32_t m) {
   }
 }
 
-template <typename K>
-__global__ void __launch_bounds__(SC_NT, 1) k_coarse_count(SortCountArgs a) {
-  extern __shared__ __align__(16) uint8_t smem_raw[];
-  CoarseSmem<K> &S = *reinterpret_cast<CoarseSmem<K> *>(smem_raw);
-  constexpr int TS = SliceTab<K>::TS, TSO = CoarseSmem<K>::TSO;
-  const K *keys = reinterpret_cast<const K *>(a.keys);
-  K *tkeys = reinterpret_cast<K *>(a.tmp_keys);
-  const int key_bits = 2 * a.k;
-  const int tid = threadIdx.x;
-  if (*a.err & (ERR_CAPACITY | ERR_BAD_READ)) return;  // keys incomplete: the host re-runs
-  const uint64_t n_buckets = a.bucket_base[a.nbins];
-  if (tid == 0) {
-    S.tot_n = 0;
-    S.tot_d = 0;
-    S.dirty = 1;  // the table starts uncleared
-  }
-  // optional phase profile (cycles of thread 0 between marks, per phase)
-  const bool prof = a.prof != nullptr;
-  if (tid < 8) S.ph[tid] = 0;
-  long long tph = 0;
-#define PHASE(i)                                       \
-  if (prof && tid == 0) {                              \
-    const long long _t = clock64();                    \
-    S.ph[i] += (unsigned long long)(_t - tph);         \
-    tph = _t;                                          \
-  }
-  while (true) {
-    if (tid == 0) {
-      S.g = atomicAdd(a.ticket, 1ull);
-      if (S.g < n_buckets) {
-        const uint32_t b = find_bin(a.bucket_base, a.nbins, S.g);
-        const uint64_t d = S.g - a.bucket_base[b];
-        const uint64_t nch = a.chunk_base[b + 1] - a.chunk_base[b];
-        const uint64_t hb = a.hist_base[b];
-        S.b = b;
-        S.start = a.chunk_off[hb + d * nch];
-        S.n = a.chunk_off[hb + (d + 1) * nch] - S.start;
+// The same network over (key, count) pairs, by the whole block.
+template <typename K, int NT>
+GKC_DEV void block_sort_pairs(K *A, uint32_t *cv, uint32_t m) {
+  uint32_t P = 1;
+  while (P < m) P <<= 1;
+  for (uint32_t size = 2; size <= P; size <<= 1) {
+    const uint32_t half = size >> 1;
+    for (uint32_t i = threadIdx.x; i < P / 2; i += NT) {
+      const uint32_t blk = i / half, off = i % half;
+      const uint32_t lo = blk * size + off, hi = blk * size + size - 1 - off;
+      if (hi < m && A[hi] < A[lo]) {
+        const K x = A[lo];
+        A[lo] = A[hi];
+        A[hi] = x;
+        const uint32_t c = cv[lo];
+        cv[lo] = cv[hi];
+        cv[hi] = c;
       }
-      S.run = 0;
-      // Mostly distinct keys gain little from the table (and near-equal ones
-      // make long probe chains): when this CTA's slices so far were more
-      // than 55% distinct, the bucket's slices are sorted directly instead.
-      S.sort_mode = S.tot_n > 0 && S.tot_d * 20 > S.tot_n * 11;
     }
     __syncthreads();
-    const bool sort_mode = S.sort_mode;
-    const uint32_t target = sort_mode ? (uint32_t)SortCap<K>::value : (uint32_t)(SliceTab<K>::TS / 2);
-    const uint64_t g = S.g;
-    if (g >= n_buckets) break;
-    const uint64_t start = S.start, n = S.n;
-    if (prof && tid == 0) tph = clock64();
-    const int cb = (int)a.bin_bits[S.b];
-    const int SB = min(CC_SUB_BITS, key_bits - cb);
-    const uint32_t nsub = 1u << SB;
-    const int lbits = min(SL_LOW_BITS, key_bits - cb - SB);
-    if (n == 0) {
+    for (uint32_t stride = size >> 2; stride >= 1; stride >>= 1) {
+      for (uint32_t i = threadIdx.x; i < P / 2; i += NT) {
+        const uint32_t blk = i / stride, off = i % stride;
+        const uint32_t lo = blk * 2 * stride + off, hi = lo + stride;
+        if (hi < m && A[hi] < A[lo]) {
+          const K x = A[lo];
+          A[lo] = A[hi];
+          A[hi] = x;
+          const uint32_t c = cv[lo];
+          cv[lo] = cv[hi];
+          cv[hi] = c;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Exclusive scan of S.cnt[0, nsub) in place (thread-contiguous groups).
+template <typename K, int NT>
+GKC_DEV void scan_sub(CountSmem<K> &S, uint32_t nsub) {
+  const uint32_t per = (nsub + NT - 1) / NT, c0 = threadIdx.x * per;
+  uint32_t s = 0;
+  for (uint32_t jj = c0; jj < c0 + per && jj < nsub; jj++) s += S.cnt[jj];
+  uint32_t tot;
+  uint32_t run = block_exclusive_scan<NT>(s, S.tmp, &tot);
+  for (uint32_t jj = c0; jj < c0 + per && jj < nsub; jj++) {
+    const uint32_t v = S.cnt[jj];
+    S.cnt[jj] = run;
+    run += v;
+  }
+  __syncthreads();
+}
+
+// The m keys in S.u.A are grouped by sub-bucket: sub-bucket jb + jj starts at
+// S.cnt[jb + jj] - s0 for jj in [0, nsl) (the last one ends at m).  Each
+// thread sorts the sub-buckets it owns and run-length encodes them in place
+// (keys in A, counts in C); longer segments are sorted by warps first.  Sets
+// S.seg_src / S.seg_pos (exclusive scan of the run counts) and returns the
+// slice's distinct keys.
+template <typename K, int NT>
+GKC_DEV uint32_t slice_runs(CountSmem<K> &S, uint32_t m, uint32_t jb, uint32_t nsl, uint32_t s0) {
+  const int tid = threadIdx.x;
+  K *A = S.u.A;
+  auto start_of = [&](uint32_t jj) -> uint32_t { return jj < nsl ? S.cnt[jb + jj] - s0 : m; };
+  const uint32_t j0 = (uint32_t)(((uint64_t)tid * nsl) / NT), j1 = (uint32_t)(((uint64_t)(tid + 1) * nsl) / NT);
+  const uint32_t s = start_of(j0), e = start_of(j1);
+  if (tid == 0) S.nbig = 0;
+  __syncthreads();
+  bool big = e - s > CC_SEG_MAX;
+  if (big) {
+    const uint32_t t = atomicAdd(&S.nbig, 1u);
+    if (t < (uint32_t)CC_BIG_LIST) S.big[t] = (uint32_t)tid;
+    else big = false;  // list full: sorted by its own thread
+  }
+  if (!big) {
+    for (uint32_t jj = j0; jj < j1; jj++) {
+      const uint32_t b0 = start_of(jj), b1 = start_of(jj + 1);
+      for (uint32_t p = b0 + 1; p < b1; p++) {
+        const K x = A[p];
+        uint32_t q = p;
+        while (q > b0 && x < A[q - 1]) {
+          A[q] = A[q - 1];
+          q--;
+        }
+        A[q] = x;
+      }
+    }
+  }
+  __syncthreads();
+  const uint32_t nbig = min(S.nbig, (uint32_t)CC_BIG_LIST);
+  for (uint32_t t = threadIdx.x >> 5; t < nbig; t += NT / 32) {
+    const uint32_t ow = S.big[t];
+    const uint32_t oj0 = (uint32_t)(((uint64_t)ow * nsl) / NT), oj1 = (uint32_t)(((uint64_t)(ow + 1) * nsl) / NT);
+    const uint32_t os = start_of(oj0);
+    warp_sort<K>(A + os, start_of(oj1) - os);
+  }
+  __syncthreads();
+  uint32_t u = 0;
+  for (uint32_t i = s; i < e;) {
+    const K x = A[i];
+    uint32_t c = 1;
+    i++;
+    while (i < e && A[i] == x) {
+      c++;
+      i++;
+    }
+    A[s + u] = x;
+    S.C[s + u] = (uint16_t)c;  // c <= m <= CAP < 2^16
+    u++;
+  }
+  uint32_t D;
+  const uint32_t pos = block_exclusive_scan<NT>(u, S.tmp, &D);
+  S.seg_pos[tid] = pos;
+  S.seg_src[tid] = s;
+  __syncthreads();
+  return D;
+}
+
+// Writes the D runs of the slice (S.seg_* from slice_runs) at out[ob, ob+D),
+// coalesced: output i comes from the thread whose runs cover it.
+template <typename K, int NT>
+GKC_DEV void write_runs(CountSmem<K> &S, const SortCountArgs &a, uint32_t D, uint64_t ob) {
+  K *out_keys = reinterpret_cast<K *>(a.out_keys);
+  for (uint32_t i = threadIdx.x; i < D; i += NT) {
+    uint32_t lo = 0, hi = NT - 1;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (S.seg_pos[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    const uint32_t src = S.seg_src[lo] + (i - S.seg_pos[lo]);
+    if (ob + i < a.out_cap) {
+      out_keys[ob + i] = S.u.A[src];
+      a.out_counts[ob + i] = S.C[src];
+    } else {
+      atomicOr(a.err, ERR_CAPACITY);
+    }
+  }
+}
+
+// One sub-bucket of n keys at tmp[0, n), too many for shared memory: key
+// ranges are aggregated in the hash table; a range whose distinct keys fill
+// more than 3/4 of it is halved and both halves retried (lower first).  Runs
+// are appended at out[S.out_base + S.run].
+template <typename K, int NT>
+GKC_DEV void heavy_slice(CountSmem<K> &S, const SortCountArgs &a, const K *src, uint64_t n) {
+  constexpr int HN = HeavyTab<K>::N;
+  HeavyTab<K> &T = S.u.h;
+  K *out_keys = reinterpret_cast<K *>(a.out_keys);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    S.sp = 1;
+    S.stk_lo[0] = (K)0;
+    S.stk_hi[0] = ~(K)0;
+  }
+  __syncthreads();
+  while (true) {
+    if (S.sp == 0) break;
+    const K lo = S.stk_lo[S.sp - 1], hi = S.stk_hi[S.sp - 1];
+    for (int s = tid; s < HN; s += NT) {
+      T.cnt[s] = 0;
+      T.state[s] = 0;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      S.sp--;
+      S.flag = 0;
+      S.hfill = 0;
+    }
+    __syncthreads();
+    for (uint64_t i = tid; i < n; i += NT) {
+      const K x = src[i];
+      if (x < lo || x > hi) continue;
+      uint64_t hh = (uint64_t)x ^ (uint64_t)(x >> (4 * sizeof(K))) ^ (uint64_t)(x >> (8 * sizeof(K) - 8));
+      hh = (hh ^ (hh >> 29)) * 0xBF58476D1CE4E5B9ull;
+      uint32_t slot = (uint32_t)(hh >> 40) & (HN - 1);
+      for (uint32_t probes = 0;; probes++) {
+        if (probes >= (uint32_t)HN || *(volatile int *)&S.flag) {
+          S.flag = 1;
+          break;
+        }
+        uint32_t st = *(volatile uint32_t *)&T.state[slot];
+        if (st == 0) {
+          if (atomicCAS(&T.state[slot], 0u, 1u) == 0u) {
+            T.key[slot] = x;
+            __threadfence_block();
+            atomicExch(&T.state[slot], 2u);
+            atomicAdd(&T.cnt[slot], 1u);
+            if (atomicAdd(&S.hfill, 1u) + 1 > (uint32_t)(HN * 3 / 4)) S.flag = 1;
+            break;
+          }
+          st = 1;
+        }
+        if (st == 1) {  // another thread is writing this slot's key
+          uint32_t w = 0;
+          while ((st = *(volatile uint32_t *)&T.state[slot]) != 2u && ++w < (1u << 22)) {
+          }
+          if (st != 2u) {
+            atomicOr(a.err, ERR_SPIN_TIMEOUT);
+            S.flag = 1;
+            break;
+          }
+        }
+        if (*(volatile K *)&T.key[slot] == x) {
+          atomicAdd(&T.cnt[slot], 1u);
+          break;
+        }
+        slot = (slot + 1) & (HN - 1);
+      }
+    }
+    __syncthreads();
+    if (S.flag && lo < hi) {
       if (tid == 0) {
-        a.coarse_start[g] = start;
-        a.coarse_d[g] = 0;
+        const K mid = lo + ((hi - lo) >> 1);
+        if (S.sp + 2 <= CC_STACK) {
+          S.stk_lo[S.sp] = mid + 1;  // upper half below the lower half
+          S.stk_hi[S.sp] = hi;
+          S.stk_lo[S.sp + 1] = lo;
+          S.stk_hi[S.sp + 1] = mid;
+          S.sp += 2;
+        } else {
+          atomicOr(a.err, ERR_BOUNDS);
+        }
       }
       __syncthreads();
       continue;
     }
-    // Sub-bucket counts at sub[1 + j]; their exclusive scan is the cursor of
-    // sub-bucket j while the keys are placed in sub-bucket order in the
-    // bucket's own range of tmp_keys (where they stay in L2), after which
-    // sub[j] is the first placed key of sub-bucket j.  A slice then reads only
-    // its own keys.  Its runs are written at or before its first key, after
-    // all of its keys were read, so the placed keys of later slices survive.
-    K *placed = tkeys + start;
-    if (!in_bounds(a, 11, start + n, a.tmp_cap + 1)) return;
-    for (uint32_t j = tid; j <= nsub; j += SC_NT) S.sub[j] = 0;
-    __syncthreads();
-    {
-      constexpr int U = 8;
-      for (uint64_t i0 = 0; i0 < n; i0 += (uint64_t)SC_NT * U) {
-        K xs[U];
+    // the occupied slots to the front (through registers), sorted, written
+    constexpr int PT = HN / NT;
+    K mk[PT];
+    uint32_t mc[PT], mine = 0;
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-          const uint64_t i = i0 + (uint64_t)u * SC_NT + tid;
-          xs[u] = i < n ? keys[start + i] : (K)0;
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++)
-          if (i0 + (uint64_t)u * SC_NT + tid < n) atomicAdd(&S.sub[1 + key_digit<K>(xs[u], key_bits, cb, SB)], 1u);
-      }
-      __syncthreads();
-      scan_counters(S.sub + 1, nsub, S.tmp);
-      for (uint64_t i0 = 0; i0 < n; i0 += (uint64_t)SC_NT * U) {
-        K xs[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-          const uint64_t i = i0 + (uint64_t)u * SC_NT + tid;
-          xs[u] = i < n ? keys[start + i] : (K)0;
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++)
-          if (i0 + (uint64_t)u * SC_NT + tid < n) {
-            const uint32_t pos = atomicAdd(&S.sub[1 + key_digit<K>(xs[u], key_bits, cb, SB)], 1u);
-            if (in_bounds(a, 12, pos, n)) placed[pos] = xs[u];
-          }
+    for (int u = 0; u < PT; u++) {
+      const int s = u * NT + tid;
+      if (T.state[s] == 2u) {
+        mk[mine] = T.key[s];
+        mc[mine] = T.cnt[s];
+        mine++;
       }
     }
     __syncthreads();
-    PHASE(0)
-    // slices: runs of sub-buckets whose exclusive start falls in the same
-    // multiple of `target` (a slice holds < target keys plus one sub-bucket)
-    {
-      const uint32_t per = (nsub + SC_NT - 1) / SC_NT, j0 = tid * per;
-      uint32_t cnt = 0;
-      for (uint32_t j = j0; j < j0 + per && j < nsub; j++)
-        cnt += (j == 0 || S.sub[j] / target != S.sub[j - 1] / target);
-      uint32_t total;
-      uint32_t idx = block_exclusive_scan<SC_NT>(cnt, S.tmp, &total);
-      for (uint32_t j = j0; j < j0 + per && j < nsub; j++)
-        if (j == 0 || S.sub[j] / target != S.sub[j - 1] / target) S.slo[idx++] = (uint16_t)j;
-      if (tid == 0) S.nsl = total;
-      __syncthreads();
-    }
-    const uint32_t nsl = S.nsl;
-    for (uint32_t sl = 0; sl < nsl; sl++) {
-      // A slice that overflows the table is split at its key midpoint and the
-      // halves retried, the left one first (a stack), so that the output
-      // stays in key order; only a single sub-bucket falls back to sorting.
-      if (tid == 0) {
-        S.stk[0] = ((uint32_t)S.slo[sl] << 16) | ((sl + 1 < nsl) ? (uint32_t)S.slo[sl + 1] : nsub);
-        S.sp = 1;
+    if (tid == 0) S.hfill = 0;
+    __syncthreads();
+    const uint32_t first = atomicAdd(&S.hfill, mine);
+#pragma unroll
+    for (int u = 0; u < PT; u++)
+      if ((uint32_t)u < mine) {
+        T.key[first + u] = mk[u];
+        T.cnt[first + u] = mc[u];
       }
-     while (true) {
-      __syncthreads();
-      const int sp = S.sp;
-      if (sp == 0) break;
-      const uint32_t top = S.stk[sp - 1];
-      __syncthreads();  // every thread has read the top before it is popped
-      if (tid == 0) S.sp = sp - 1;
-      const uint32_t j_lo = top >> 16;
-      const uint32_t j_hi = top & 0xFFFFu;
-      const uint32_t base_cnt = S.sub[j_lo];
-      const uint32_t ns = S.sub[j_hi] - base_cnt;
-      if (ns == 0) continue;
-      if (!in_bounds(a, 13, (uint64_t)base_cnt + ns, n + 1)) continue;  // slice inside its bucket
-      for (uint32_t j = j_lo + tid; j < j_hi; j += SC_NT)
-        S.slot_base[j - j_lo] = (uint32_t)(((uint64_t)(S.sub[j] - base_cnt) * TS) / ns);
-      if (tid == 0) {
-        S.slot_base[j_hi - j_lo] = TS;
-        S.overflow = 0;
-        S.nbig = 0;
-      }
-      // slices of a sort-mode bucket that fit the shared-memory sort go there
-      // directly; larger ones (one heavy sub-bucket) still use the table
-      const bool direct_sort = sort_mode && ns <= (uint32_t)SortCap<K>::value;
-      if (!direct_sort) {  // aggregate in the table
-      // The occupancy bitmap (a bit per slot, set when an insert claims the
-      // slot) lets the cluster walk, the output and the clearing touch only
-      // occupied slots; the whole table is cleared only after a sort reused
-      // its memory.
-      constexpr int NW = (TSO + 31) / 32;
-      static_assert(NW <= SC_NT, "one bitmap word per thread");
-      if (S.dirty) {
-        for (int s = tid; s < TSO; s += SC_NT) {
-          S.u.t.key[s] = empty_key<K>();
-          S.u.t.cnt[s] = 0;
-        }
-        for (int w = tid; w < NW; w += SC_NT) S.occ[w] = 0;
-        __syncthreads();
-        if (tid == 0) S.dirty = 0;
-      }
-      __syncthreads();
-      for (uint32_t i = tid; i < ns; i += SC_NT) {
-        const K x = placed[base_cnt + i];
-        const uint32_t j = key_digit<K>(x, key_bits, cb, SB) - j_lo;
-        const uint32_t low = key_digit<K>(x, key_bits, cb + SB, lbits);
-        const uint32_t w = S.slot_base[j + 1] - S.slot_base[j];
-        int slot = (int)(S.slot_base[j] + (uint32_t)(((uint64_t)low * w) >> lbits));
-        int probes = 0;
-        while (true) {
-          if (slot >= TSO || probes > a.probe_limit) {
-            set_overflow(&S.overflow);
-            break;
-          }
-          // 8-byte keys are read atomically; 16-byte keys only through the CAS
-          K cur = sizeof(K) == 8 ? volatile_load<K>(&S.u.t.key[slot]) : empty_key<K>();
-          if (cur == x) {
-            atomicAdd(&S.u.t.cnt[slot], 1u);
-            break;
-          }
-          if (cur == empty_key<K>()) {
-            K prev = smem_cas(&S.u.t.key[slot], empty_key<K>(), x);
-            if (prev == empty_key<K>()) {
-              atomicOr(&S.occ[slot >> 5], 1u << (slot & 31));
-              atomicAdd(&S.u.t.cnt[slot], 1u);
-              break;
-            }
-            if (prev == x) {
-              atomicAdd(&S.u.t.cnt[slot], 1u);
-              break;
-            }
-          }
-          slot++;
-          probes++;
-        }
-        if (get_overflow(&S.overflow)) break;
-      }
-      __syncthreads();
-      PHASE(1)
-      // clusters: runs of occupied slots; the owner of a cluster's first slot
-      // sorts a short one, long ones go to warps
-      const int w = tid;
-      const uint32_t wbits = w < NW ? S.occ[w] : 0u;
-      uint32_t occ = __popc(wbits);
-      if (!S.overflow && wbits) {
-        uint32_t bits = wbits;
-        while (bits) {
-          const int q = __ffs(bits) - 1;
-          bits &= bits - 1;
-          const int s = w * 32 + q;
-          const bool prev_occ = q > 0 ? ((wbits >> (q - 1)) & 1u) != 0 : (w > 0 && (S.occ[w - 1] >> 31) != 0);
-          if (prev_occ) continue;  // not a cluster start
-          int e = s + 1;
-          for (int ww = e >> 5; ww < NW; ww++) {  // first free slot after s
-            const uint32_t inv = ~S.occ[ww] & (0xFFFFFFFFu << (ww == (e >> 5) ? (e & 31) : 0));
-            if (inv) {
-              e = ww * 32 + __ffs(inv) - 1;
-              break;
-            }
-            e = (ww + 1) * 32;
-            if (e - s > SL_CLUSTER_LIMIT) break;
-          }
-          e = min(e, TSO);
-          if (e - s > SL_CLUSTER_LIMIT) {
-            set_overflow(&S.overflow);
-            break;
-          }
-          if (e - s > CW_MIN) {  // long: sorted by a warp below
-            const uint32_t t = atomicAdd(&S.nbig, 1u);
-            if (t < (uint32_t)CW_LIST) {
-              S.bigl[t] = ((uint32_t)s << 10) | (uint32_t)(e - s);
-              continue;
-            }
-          }
-          for (int qq = s + 1; qq < e; qq++) {  // insertion sort of (key, count)
-            K x = S.u.t.key[qq];
-            uint32_t c = S.u.t.cnt[qq];
-            int r = qq;
-            while (r > s && x < S.u.t.key[r - 1]) {
-              S.u.t.key[r] = S.u.t.key[r - 1];
-              S.u.t.cnt[r] = S.u.t.cnt[r - 1];
-              r--;
-            }
-            S.u.t.key[r] = x;
-            S.u.t.cnt[r] = c;
-          }
-        }
-      }
-      __syncthreads();
-      if (!S.overflow) {
-        const uint32_t nbl = min(S.nbig, (uint32_t)CW_LIST);
-        for (uint32_t t = threadIdx.x >> 5; t < nbl; t += SC_NT / 32)
-          warp_sort_pairs<K>(S.u.t.key + (S.bigl[t] >> 10), S.u.t.cnt + (S.bigl[t] >> 10), S.bigl[t] & 1023u);
-      }
-      __syncthreads();
-      PHASE(2)
-      const bool ok = !S.overflow;
-      if (ok) {
-        uint32_t D;
-        const uint32_t pos = block_exclusive_scan<SC_NT>(occ, S.tmp, &D);
-        const uint64_t base = start + S.run + pos;
-        uint32_t o = 0, bits = wbits;
-        while (bits) {
-          const int s = w * 32 + __ffs(bits) - 1;
-          bits &= bits - 1;
-          if (!in_bounds(a, 8, base + o, a.tmp_cap)) break;
-          tkeys[base + o] = S.u.t.key[s];
-          a.tmp_counts[base + o] = S.u.t.cnt[s];
-          o++;
-        }
-        __syncthreads();
-        if (tid == 0) {
-          S.run += D;
-          S.tot_n += ns;
-          S.tot_d += D;
-        }
-      }
-      // empty the occupied slots and the bitmap (after an overflow too: the
-      // bitmap marks exactly the slots inserts claimed)
-      {
-        uint32_t bits = wbits;
-        while (bits) {
-          const int s = w * 32 + __ffs(bits) - 1;
-          bits &= bits - 1;
-          S.u.t.key[s] = empty_key<K>();
-          S.u.t.cnt[s] = 0;
-        }
-        if (w < NW) S.occ[w] = 0;
-      }
-      __syncthreads();
-      PHASE(3)
-      if (ok) continue;
-      if (j_hi - j_lo > 1 && sp + 1 <= kSliceStack) {
-        if (tid == 0) {  // split: smallest mid in [j_lo+1, j_hi-1] with half the keys before it
-          const uint32_t half = base_cnt + ns / 2;
-          uint32_t lo = j_lo + 1, hi = j_hi - 1;
-          while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (S.sub[mid] >= half) hi = mid; else lo = mid + 1;
-          }
-          S.stk[sp - 1] = (lo << 16) | j_hi;  // the popped entry's place, then one more
-          S.stk[sp] = (j_lo << 16) | lo;
-          S.sp = sp + 1;
-          if (a.prof) atomicAdd(a.prof + 6, 1ull);
-        }
-        continue;
-      }
-      }  // table
-      // ---- gather the slice's keys and sort them (this reuses the table) ----
-      if (tid == 0) S.dirty = 1;
-      if (tid == 0 && a.prof) atomicAdd(a.prof + (direct_sort ? 7 : 5), 1ull);
-      const uint32_t fh = j_hi - 1;
-      const int skip = (j_lo == fh) ? cb + SB : cb + SB - (32 - __clz(j_lo ^ fh));
-      SortSmem<K> &T = S.u.s;
-      if (tid == 0) S.cursor = 0;
-      __syncthreads();
-      const bool fits = ns <= (uint32_t)SortCap<K>::value;
-      if (!fits && ns > a.scratch_keys) {
-        if (tid == 0) atomicOr(a.err, ERR_OVERSIZE_SCRATCH);
-        __syncthreads();
-        continue;
-      }
-      if (!fits) {
-        // the global scratch area is shared by all CTAs: one user at a time
-        if (tid == 0) S.overflow = acquire_lock(a.scratch_lock, a.err) ? 0 : 1;
-        __syncthreads();
-        if (S.overflow) continue;  // wait ran out: reported through the error word
-      }
-      K *dst = fits ? T.A : reinterpret_cast<K *>(a.scratch);
-      for (uint32_t i = tid; i < ns; i += SC_NT) dst[i] = placed[base_cnt + i];
-      if (tid == 0) T.out = start + S.run;
-      __syncthreads();
-      if (fits) {
-        smem_sort<K>(T, ns, key_bits, skip);
-        const uint32_t D = smem_runs<K>(T, ns);
-        if (!in_bounds(a, 10, T.out + D, a.tmp_cap + 1)) {
-          __syncthreads();
-          continue;
-        }
-        write_runs<K>(T, D, tkeys, a.tmp_counts, T.out);
-        __syncthreads();
-        if (tid == 0) {
-          S.run += D;
-          S.tot_n += ns;
-          S.tot_d += D;
-        }
+    __syncthreads();
+    const uint32_t nd = S.hfill;
+    block_sort_pairs<K, NT>(T.key, T.cnt, nd);
+    const uint64_t ob = S.out_base + S.run;
+    for (uint32_t i = tid; i < nd; i += NT) {
+      if (ob + i < a.out_cap) {
+        out_keys[ob + i] = T.key[i];
+        a.out_counts[ob + i] = T.cnt[i];
       } else {
-        __threadfence_block();
-        scratch_sort<K>(T, a, ns, skip, tkeys, a.tmp_counts);
-        if (tid == 0) S.run = T.out - start;
-        // release the scratch area (all threads are past their last access)
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) atomicExch(a.scratch_lock, 0ull);
+        atomicOr(a.err, ERR_CAPACITY);
+      }
+    }
+    __syncthreads();
+    if (tid == 0) S.run += nd;
+    __syncthreads();
+  }
+}
+
+template <typename K>
+__global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCountArgs a) {
+  constexpr int NT = CountShape<K>::NT, CAP = CountShape<K>::CAP, KPT = CAP / NT;
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  CountSmem<K> &S = *reinterpret_cast<CountSmem<K> *>(smem_raw);
+  const K *keys = reinterpret_cast<const K *>(a.keys);
+  K *tmp = reinterpret_cast<K *>(a.scratch);
+  const int key_bits = 2 * a.k;
+  const int room = key_bits < 32 ? key_bits : 32;  // bits of the map
+  const int tid = threadIdx.x;
+  if (*a.err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
+  const uint64_t n_buckets = a.bucket_base[a.nbins];
+  while (true) {
+    if (tid == 0) {
+      S.g = atomicAdd(a.ticket, 1ull);
+      if (S.g < n_buckets) {
+        S.b = find_bin(a.bucket_base, a.nbins, S.g);
+        S.start = a.bucket_start[S.g];
+        S.n = a.bucket_size[S.g];
+      }
+    }
+    __syncthreads();
+    const uint64_t g = S.g;
+    if (g >= n_buckets) break;
+    const uint64_t start = S.start, n = S.n;
+    const uint32_t b = S.b;
+    const int cb = (int)a.bin_bits[b];
+    if (n <= (uint64_t)CAP) {
+      // ---- the whole bucket in shared memory
+      const uint32_t m = (uint32_t)n;
+      int sb = 0;
+      while (sb < CC_SB_MAX && (2u << sb) <= m) sb++;
+      sb = min(sb, room - cb);
+      const uint32_t nsub = 1u << sb;
+      for (uint32_t jj = tid; jj < nsub; jj += NT) S.cnt[jj] = 0;
+      __syncthreads();
+      K xs[KPT];
+      uint32_t rk[(KPT + 1) / 2];
+#pragma unroll
+      for (int u = 0; u < (KPT + 1) / 2; u++) rk[u] = 0;
+#pragma unroll
+      for (int u = 0; u < KPT; u++) {
+        const uint32_t i = u * NT + tid;
+        if (i < m) {
+          xs[u] = keys[start + i];
+          const uint32_t r = atomicAdd(&S.cnt[sub_digit<K>(xs[u], key_bits, cb, sb)], 1u);
+          rk[u / 2] |= r << (16 * (u & 1));
+        }
       }
       __syncthreads();
-      PHASE(4)
-     }
+      scan_sub<K, NT>(S, nsub);
+#pragma unroll
+      for (int u = 0; u < KPT; u++) {
+        const uint32_t i = u * NT + tid;
+        if (i < m)
+          S.u.A[S.cnt[sub_digit<K>(xs[u], key_bits, cb, sb)] + ((rk[u / 2] >> (16 * (u & 1))) & 0xFFFFu)] = xs[u];
+      }
+      __syncthreads();
+      const uint32_t D = slice_runs<K, NT>(S, m, 0, nsub, 0);
+      if (tid == 0) {
+        lb_publish(a.lookback, g, LB_AGG | D);
+        const uint64_t ex = lb_exclusive(a.lookback, g, a.err);
+        lb_publish(a.lookback, g, LB_INC | (ex + D));
+        S.out_base = ex;
+        if (a.bucket_base[b] == g) a.bin_out[b] = ex;
+        if (g + 1 == n_buckets) a.bin_out[a.nbins] = ex + D;
+      }
+      __syncthreads();
+      write_runs<K, NT>(S, a, D, S.out_base);
+      __syncthreads();
+      continue;
+    }
+
+    // ---- oversized bucket: placed by sub-bucket in the scratch area, then
+    // counted in slices of at most CAP keys in key order
+    const int sb = max(0, min(CC_SB_MAX, room - cb));
+    const uint32_t nsub = 1u << sb;
+    if (tid == 0) {
+      S.flag = 0;
+      const unsigned long long at = atomicAdd(a.scratch_cursor, (unsigned long long)n);
+      if (at + n > a.scratch_keys) {
+        atomicOr(a.err, ERR_OVERSIZE_SCRATCH);
+        S.flag = 1;
+      }
+      S.tbase = at;
+    }
+    for (uint32_t jj = tid; jj < nsub; jj += NT) S.cnt[jj] = 0;
+    __syncthreads();
+    if (S.flag) {  // no room: an empty result (the host re-runs with a larger area)
+      if (tid == 0) {
+        const uint64_t ex = lb_exclusive(a.lookback, g, a.err);
+        lb_publish(a.lookback, g, LB_INC | ex);
+        if (a.bucket_base[b] == g) a.bin_out[b] = ex;
+        if (g + 1 == n_buckets) a.bin_out[a.nbins] = ex;
+      }
+      __syncthreads();
+      continue;
+    }
+    K *place = tmp + S.tbase;
+    for (uint64_t i = tid; i < n; i += NT) atomicAdd(&S.cnt[sub_digit<K>(keys[start + i], key_bits, cb, sb)], 1u);
+    __syncthreads();
+    scan_sub<K, NT>(S, nsub);
+    static_assert(sizeof(S.C) / 4 >= CC_NSUB_MAX, "cursors fit in C");
+    uint32_t *cur = reinterpret_cast<uint32_t *>(S.C);
+    for (uint32_t jj = tid; jj < nsub; jj += NT) cur[jj] = S.cnt[jj];
+    __syncthreads();
+    for (uint64_t i = tid; i < n; i += NT) {
+      const K x = keys[start + i];
+      place[atomicAdd(&cur[sub_digit<K>(x, key_bits, cb, sb)], 1u)] = x;
+    }
+    __threadfence_block();
+    __syncthreads();
+    if (tid == 0) {
+      S.out_base = lb_exclusive(a.lookback, g, a.err);
+      if (a.bucket_base[b] == g) a.bin_out[b] = S.out_base;
+      S.run = 0;
+    }
+    __syncthreads();
+    uint32_t jlo = 0;
+    while (jlo < nsub) {
+      // next slice: sub-buckets [jlo, jhi), at most CAP keys, or one heavy sub-bucket
+      const uint32_t s0 = S.cnt[jlo];
+      uint32_t lo = jlo + 1, hi = nsub;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        const uint64_t e = mid < nsub ? S.cnt[mid] : n;
+        if (e - s0 <= (uint64_t)CAP) lo = mid; else hi = mid - 1;
+      }
+      const uint32_t jhi = lo;
+      const uint64_t se = jhi < nsub ? S.cnt[jhi] : n;
+      const uint64_t ns = se - s0;
+      if (ns <= (uint64_t)CAP) {
+        const uint32_t m = (uint32_t)ns;
+        for (uint32_t i = tid; i < m; i += NT) S.u.A[i] = place[s0 + i];
+        __syncthreads();
+        const uint32_t D = slice_runs<K, NT>(S, m, jlo, jhi - jlo, s0);
+        write_runs<K, NT>(S, a, D, S.out_base + S.run);
+        __syncthreads();
+        if (tid == 0) S.run += D;
+        __syncthreads();
+      } else {
+        heavy_slice<K, NT>(S, a, place + s0, ns);
+      }
+      jlo = jhi;
     }
     if (tid == 0) {
-      a.coarse_start[g] = start;
-      a.coarse_d[g] = S.run;
+      lb_publish(a.lookback, g, LB_INC | (S.out_base + S.run));
+      if (g + 1 == n_buckets) a.bin_out[a.nbins] = S.out_base + S.run;
     }
     __syncthreads();
   }
-  if (prof && tid == 0)
-    for (int i = 0; i < 8; i++) atomicAdd(a.prof + 16 + i, S.ph[i]);
-#undef PHASE
 }
 
-// Moves each coarse bucket's sorted runs to its final offset.
-template <typename K>
-__global__ void k_compact(const K *tkeys, const uint32_t *tcounts, const uint64_t *coarse_start,
-                          const unsigned long long *coarse_d, const uint64_t *coarse_out,
-                          const uint64_t *bucket_base, uint32_t nbins, K *out_keys,
-                          uint32_t *out_counts) {
-  const uint64_t nb = bucket_base[nbins];
-  for (uint64_t g = blockIdx.x; g < nb; g += gridDim.x) {
-    const uint64_t s = coarse_start[g], d = coarse_d[g], o = coarse_out[g];
-    for (uint64_t i = threadIdx.x; i < d; i += blockDim.x) {
-      out_keys[o + i] = tkeys[s + i];
-      out_counts[o + i] = tcounts[s + i];
-    }
-  }
-}
-
-// bin_out[b] = output offset of the first coarse bucket of bin b.
-__global__ void k_bin_out_offsets(const uint64_t *coarse_out, const uint64_t *bucket_base,
-                                  uint32_t nbins, uint64_t *bin_out) {
-  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b <= nbins; b += gridDim.x * blockDim.x)
-    bin_out[b] = coarse_out[bucket_base[b]];
-}
-
-template __global__ void k_coarse_hist<uint64_t>(ExpandArgs);
-template __global__ void k_coarse_hist<u128>(ExpandArgs);
-template __global__ void k_coarse_scatter<uint64_t>(ExpandArgs);
-template __global__ void k_coarse_scatter<u128>(ExpandArgs);
-template __global__ void k_coarse_count<uint64_t>(SortCountArgs);
-template __global__ void k_coarse_count<u128>(SortCountArgs);
-template __global__ void k_compact<uint64_t>(const uint64_t *, const uint32_t *, const uint64_t *,
-                                             const unsigned long long *, const uint64_t *,
-                                             const uint64_t *, uint32_t, uint64_t *, uint32_t *);
-template __global__ void k_compact<u128>(const u128 *, const uint32_t *, const uint64_t *,
-                                         const unsigned long long *, const uint64_t *,
-                                         const uint64_t *, uint32_t, u128 *, uint32_t *);
+template __global__ void k_bucket_scatter<uint64_t>(ExpandArgs);
+template __global__ void k_bucket_scatter<u128>(ExpandArgs);
+template __global__ void k_bucket_count<uint64_t>(SortCountArgs);
+template __global__ void k_bucket_count<u128>(SortCountArgs);
 
 }  // namespace gkc

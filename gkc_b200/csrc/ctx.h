@@ -30,8 +30,17 @@ struct GraphKey {
   }
 };
 
+// Launch shapes picked per device and workload class (the tuner's choices;
+// zero means the built-in default).
+struct TuneChoice {
+  uint32_t coarse_target = 0;  // largest mean keys per count bucket
+  uint32_t chunk_kmers = 0;    // k-mers per histogram chunk (a power of two)
+  uint32_t count_ctas = 0;     // count kernel CTAs per SM
+};
+
 struct gkc_ctx {
   int dev = 0;
+  TuneChoice tune;
   int filter = 0;  // minimizer filter (gkc_filter)
   int n_sms = 148;
   int max_smem_optin = 0;

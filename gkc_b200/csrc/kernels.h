@@ -30,6 +30,9 @@ constexpr int kPartTile = 4096;
 size_t partition_smem_bytes(int nbins_smem);
 __global__ void k_partition(PartArgs a);
 constexpr int kBinChunk = 8192;          // superkmers per placement chunk
+constexpr int kBinRound = 2048;          // superkmers grouped by bin at a time
+constexpr int kBinPlaceThreads = 512;
+size_t bin_place_smem_bytes(uint32_t nbins);
 constexpr int kBinPlaceMaxBins = 2048;   // larger bin counts use k_bin_scatter
 __global__ void k_bin_count(const unsigned long long *n_skm_ptr, const uint32_t *mm, uint32_t nbins,
                             uint64_t nch_cap, unsigned long long *mat, const uint32_t *err);
@@ -51,8 +54,8 @@ struct CountPlan {
   uint32_t nbins;
   const uint64_t *bin_start;   // superkmers per bin (exclusive prefix, nbins+1)
   const uint64_t *bin_kstart;  // k-mers per bin (exclusive prefix, nbins+1)
-  uint32_t coarse_target;      // desired mean keys per coarse bucket
-  uint32_t max_bits;           // coarse bucket bits cap (<= 10)
+  uint32_t coarse_target;      // desired largest mean keys per coarse bucket
+  uint32_t max_bits;           // coarse bucket bits cap (<= kCoarseMaxBits)
   uint64_t chunk_kmers;        // k-mers per expansion chunk
   int k;
   const uint32_t *err;         // nothing is planned after an upstream overflow
@@ -73,63 +76,52 @@ struct ExpandArgs {
   const uint64_t *bin_kstart;
   const uint64_t *chunk_base;
   const uint64_t *hist_base;
+  const uint64_t *bucket_base;
   const uint32_t *bin_bits;
-  uint32_t max_bits;
   uint64_t chunk_kmers;
   int k;
-  unsigned long long *chunk_hist;  // (bin, digit, chunk) counts
-  const uint64_t *chunk_off;       // their exclusive scan
-  void *keys;                      // scatter output (uint64 or u128)
+  uint64_t *chunk_s0;          // first superkmer of each chunk
+  uint32_t *hist;              // (bin, chunk, digit) counts, then write offsets in the bin
+  void *keys;                  // scatter output (uint64 or u128)
   uint64_t keys_cap;
   uint32_t *err;
 };
-template <typename K> __global__ void k_coarse_hist(ExpandArgs a);
-template <typename K> __global__ void k_coarse_scatter(ExpandArgs a);
-constexpr int SCT_NT = 1024;  // k_coarse_scatter block
-template <typename K> struct SctSub { static constexpr int value = sizeof(K) == 8 ? 8192 : 4096; };
-template <typename K> size_t coarse_scatter_smem_bytes(uint32_t max_bits);
+__global__ void k_chunk_first(ExpandArgs a);
+__global__ void k_bucket_hist(ExpandArgs a);
+__global__ void k_bucket_scan(ExpandArgs a, uint64_t *bucket_start, uint64_t *bucket_size);
+template <typename K> __global__ void k_bucket_scatter(ExpandArgs a);
+template <typename K> size_t bucket_scatter_smem_bytes();
+constexpr int kBucketScanThreads = 1024;
+constexpr int kBucketHistThreads = 256;
+constexpr int kBucketScatterThreads = 512;
 __global__ void k_skm_nk(const uint64_t *desc, const unsigned long long *n_skm_dev, int k,
                          unsigned long long *nk);
 
 struct SortCountArgs {
   uint32_t nbins;
   int k;
-  const uint64_t *bucket_base;    // coarse buckets per bin (prefix, nbins+1)
-  const uint64_t *chunk_base;
-  const uint64_t *hist_base;
+  const uint64_t *bucket_base;    // buckets per bin (prefix, nbins + 1)
   const uint32_t *bin_bits;
-  const uint64_t *chunk_off;      // coarse bucket (bin, digit) starts: entry (b, d, chunk 0)
-  const void *keys;               // coarse-bucketed keys
-  void *tmp_keys;                 // sorted runs per coarse bucket, at the bucket's start
-  uint32_t *tmp_counts;
-  uint64_t *coarse_start;         // per coarse bucket
-  unsigned long long *coarse_d;   // distinct keys per coarse bucket
-  unsigned long long *ticket;     // zeroed
-  unsigned long long *scratch_lock;  // zeroed; one CTA at a time uses the scratch
-  void *scratch;                  // 2 * scratch_keys keys for oversized slices
+  const uint64_t *bucket_start;   // first key of each bucket
+  const uint64_t *bucket_size;
+  const void *keys;               // bucketed keys
+  void *scratch;                  // oversized buckets, placed by sub-bucket
   uint64_t scratch_keys;
-  uint32_t *scratch_cnt;          // 24 * 4096 counters
+  unsigned long long *scratch_cursor;  // zeroed
+  void *out_keys;                 // per-bin sorted distinct keys
+  uint32_t *out_counts;
+  uint64_t out_cap;
+  uint64_t *bin_out;              // nbins + 1 output offsets
+  unsigned long long *lookback;   // one word per bucket, zeroed
+  unsigned long long *ticket;     // zeroed
   uint32_t *err;
-  unsigned long long *prof;       // optional counters, else null
-  int probe_limit;                // table probes before a slice falls back to sorting
-  uint64_t tmp_cap;               // capacity of tmp_keys / tmp_counts
-  unsigned long long *dbg;        // first failed bounds check: code, index, limit
 };
-template <typename K> __global__ void k_coarse_count(SortCountArgs a);
-template <typename K>
-__global__ void k_compact(const K *tkeys, const uint32_t *tcounts, const uint64_t *coarse_start,
-                          const unsigned long long *coarse_d, const uint64_t *coarse_out,
-                          const uint64_t *bucket_base, uint32_t nbins, K *out_keys,
-                          uint32_t *out_counts);
-template <typename K> size_t coarse_smem_bytes();
-template <typename K> int sort_count_cap();
-constexpr int kSortThreads = 1024;
-constexpr uint32_t kCoarseTarget = 8192;
-constexpr uint32_t kCoarseMaxBits = 10;
+template <typename K> __global__ void k_bucket_count(SortCountArgs a);
+template <typename K> size_t bucket_count_smem_bytes();
+constexpr int kBucketCountThreads = 512;
+constexpr uint32_t kCoarseTarget = 4096;
+constexpr uint32_t kCoarseMaxBits = 12;
 constexpr uint64_t kChunkKmers = 65536;
-
-__global__ void k_bin_out_offsets(const uint64_t *coarse_out, const uint64_t *bucket_base,
-                                  uint32_t nbins, uint64_t *bin_out);
 
 // device-wide exclusive scan of uint64 counters (n <= 2^31)
 void scan_u64(const unsigned long long *in, uint64_t *out, uint64_t n, uint64_t *block_tmp,

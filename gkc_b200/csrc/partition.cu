@@ -32,6 +32,7 @@ constexpr int PT_NW = PT_T + PT_H;               // windows with break flags
 constexpr int PT_WORDS = PT_NLOC / 32;
 constexpr int PT_PER_THREAD = PT_NW / PT_NT;     // 9 contiguous windows per thread
 constexpr int PT_PT = 9;                         // positions per rolling p-mer task
+constexpr int PT_STG = 8192;                     // packed bytes of a tile staged in shared memory
 static_assert(PT_NW % PT_NT == 0, "windows per thread");
 static_assert(PT_NLOC % 64 == 0, "tile alignment");
 
@@ -47,13 +48,17 @@ struct PartSmem {
   } a;
   union {
     uint32_t pre[PT_NLOC];         // prefix minima
-    uint32_t mm[PT_NLOC];          // window minimizer (after the window pass)
+    uint32_t smm[PT_T + 1];        // minimizer of each core superkmer (after the window pass)
   } b;
+  uint32_t pk[PT_NLOC / 16 + 1];   // the tile's bases, 2 bits each, first base in the top bits
+  uint8_t stg[PT_STG];             // the tile's packed superkmers before they are written out
+  uint8_t code_tab[256];           // byte -> 2-bit code or 255
   uint16_t brk[PT_NW + 1];         // local positions of breaks, ascending
   uint16_t skm[PT_T + 1];          // break index of each core superkmer start
   uint32_t scan_tmp[64];
   uint64_t red_tmp[32];
   int ext_end;                     // local end window of an extended last superkmer
+  int use_stg;                     // the tile's superkmers are packed through stg
   uint32_t n_brk, n_skm, n_bytes;
   unsigned long long base_skm, base_byte;
 };
@@ -135,6 +140,8 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
     h_skm[i] = 0;
     h_km[i] = 0;
   }
+  for (int i = tid; i < 256; i += PT_NT) S.code_tab[i] = (uint8_t)code_of_byte((uint32_t)i);
+  __syncthreads();
 
   for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const int64_t ts = (int64_t)tile * PT_T;
@@ -147,19 +154,31 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
       const int q = tid * 16;
       const bool act = q < PT_NLOC;
       uint32_t cw[4] = {0u, 0u, 0u, 0u};
-      uint32_t bad16 = 0;
+      uint32_t bad16 = 0, pkw = 0;
       if (act) {
         const int64_t g = G0 + q;
-        uint8_t bytes[16];
         const bool fast = g >= 0 && (uint64_t)(g + 16) <= a.nbytes && a.aligned16;
-        if (fast) *reinterpret_cast<uint4 *>(bytes) = __ldg(reinterpret_cast<const uint4 *>(a.reads + g));
+        if (fast) {
+          const uint4 v = __ldg(reinterpret_cast<const uint4 *>(a.reads + g));
+          const uint32_t vw[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-        for (int t = 0; t < 16; t++) {
-          const uint32_t c = fast ? code_of_byte(bytes[t]) : global_code(a.reads, a.nbytes, g + t);
-          cw[t >> 2] |= c << (8 * (t & 3));
-          bad16 |= (c == 255u ? 1u : 0u) << t;
+          for (int t = 0; t < 16; t++) {
+            const uint32_t c = S.code_tab[(vw[t >> 2] >> (8 * (t & 3))) & 0xFFu];
+            cw[t >> 2] |= c << (8 * (t & 3));
+            bad16 |= (c >> 7) << t;
+            pkw |= (c & 3u) << (30 - 2 * t);
+          }
+        } else {
+#pragma unroll
+          for (int t = 0; t < 16; t++) {
+            const uint32_t c = global_code(a.reads, a.nbytes, g + t);
+            cw[t >> 2] |= c << (8 * (t & 3));
+            bad16 |= (c >> 7) << t;
+            pkw |= (c & 3u) << (30 - 2 * t);
+          }
         }
         *reinterpret_cast<uint4 *>(S.cd + q) = make_uint4(cw[0], cw[1], cw[2], cw[3]);
+        S.pk[q >> 4] = pkw;
       }
       const uint32_t other = __shfl_xor_sync(0xffffffffu, bad16, 1);
       if (act && (tid & 1) == 0) S.badw[q >> 5] = bad16 | (other << 16);
@@ -169,6 +188,7 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
       S.rsw[w] = (gw >= 0 && (uint64_t)gw < a.rs_words) ? a.rs_bits[gw] : 0u;
       S.validw[w] = 0u;
     }
+    if (tid == 0) S.pk[PT_NLOC / 16] = 0u;
     __syncthreads();
     // Windows are valid when no read starts inside them (after their first
     // byte) and they lie inside the data; they touch a bad byte when one of
@@ -222,16 +242,28 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
     }
     __syncthreads();
 
-    // ---- window minimizers and validity for local windows [PRE-1, PRE+NW) ----
+    // ---- window minimizers and breaks, thread-contiguous: windows
+    //      [lw0 - 1, lw0 + 9), the first only for the comparison ----
+    uint32_t nb_local = 0, ns_local = 0;
+    uint32_t brkbits = 0, startbits = 0;
+    const int lw0 = PT_PRE + tid * PT_PER_THREAD;
     uint32_t mmv[PT_PER_THREAD + 1];
+    uint32_t vbits, tbits, rbits;  // bit j: window lw0 - 1 + j
     {
-      // strided ownership: window l = PRE-1 + tid + j*NT
+      const int l0 = lw0 - 1, w0 = l0 >> 5, sh = l0 & 31;
+      auto bits10 = [&](const uint32_t *arr) -> uint32_t {
+        const uint64_t v = (uint64_t)arr[w0] | ((uint64_t)(w0 + 1 < PT_WORDS ? arr[w0 + 1] : 0u) << 32);
+        return (uint32_t)(v >> sh) & 0x3FFu;
+      };
+      vbits = bits10(S.validw);
+      tbits = bits10(S.touchw);
+      rbits = bits10(S.rsw);
 #pragma unroll
       for (int j = 0; j <= PT_PER_THREAD; j++) {
-        int l = PT_PRE - 1 + tid + j * PT_NT;
+        const int l = l0 + j;
         mmv[j] = 0xFFFFFFFFu;
-        if (l < PT_PRE + PT_NW && bit_at(S.validw, l)) {
-          if (!bit_at(S.touchw, l)) {
+        if ((vbits >> j) & 1u) {
+          if (!((tbits >> j) & 1u)) {
             mmv[j] = min(S.a.g[l], S.b.pre[l + omega - 1]);
           } else {
             const uint8_t *cw = S.cd + l;
@@ -240,26 +272,14 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
         }
       }
     }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j <= PT_PER_THREAD; j++) {
-      int l = PT_PRE - 1 + tid + j * PT_NT;
-      if (l < PT_PRE + PT_NW) S.b.mm[l] = mmv[j];
-    }
-    __syncthreads();
-
-    // ---- breaks (window not valid, or a superkmer start) over [PRE, PRE+NW) ----
-    uint32_t nb_local = 0, ns_local = 0;
-    uint32_t brkbits = 0, startbits = 0;
-    const int lw0 = PT_PRE + tid * PT_PER_THREAD;
 #pragma unroll
     for (int j = 0; j < PT_PER_THREAD; j++) {
-      int l = lw0 + j;
-      bool valid = bit_at(S.validw, l);
-      bool start = valid && (bit_at(S.rsw, l) || S.b.mm[l] != S.b.mm[l - 1] || !bit_at(S.validw, l - 1));
-      bool brk = !valid || start;
+      const int l = lw0 + j;
+      const bool valid = (vbits >> (j + 1)) & 1u;
+      const bool start = valid && (((rbits >> (j + 1)) & 1u) || mmv[j + 1] != mmv[j] || !((vbits >> j) & 1u));
+      const bool brk = !valid || start;
       brkbits |= (brk ? 1u : 0u) << j;
-      bool core_start = start && l < PT_PRE + PT_T;
+      const bool core_start = start && l < PT_PRE + PT_T;
       startbits |= (core_start ? 1u : 0u) << j;
       nb_local += brk;
       ns_local += core_start;
@@ -271,7 +291,10 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
 #pragma unroll
       for (int j = 0; j < PT_PER_THREAD; j++) {
         if ((brkbits >> j) & 1u) {
-          if ((startbits >> j) & 1u) S.skm[si++] = (uint16_t)bi;
+          if ((startbits >> j) & 1u) {
+            S.b.smm[si] = mmv[j + 1];  // pre[] is no longer read: the scan above ended with a barrier
+            S.skm[si++] = (uint16_t)bi;
+          }
           S.brk[bi++] = (uint16_t)(lw0 + j);
         }
       }
@@ -289,7 +312,7 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
       uint32_t jlast = S.skm[n_skm - 1];
       if (jlast + 1 >= n_brk) {
         int l = S.brk[jlast];
-        uint32_t mv = S.b.mm[l];
+        uint32_t mv = S.b.smm[n_skm - 1];
         uint64_t w = (uint64_t)(G0 + PT_PRE + PT_NW);
         // walk windows beyond the halo with the exact rule until a break
         while (w < a.nbytes) {
@@ -328,6 +351,8 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
     if (tid == 0) {
       S.n_bytes = tile_bytes;
       uint32_t rounded = (tile_bytes + 15u) & ~15u;
+      // the staged packing needs every superkmer's bases in the tile's data
+      S.use_stg = rounded <= (uint32_t)PT_STG && (S.ext_end < 0 || S.ext_end + k - 1 <= PT_NLOC);
       S.base_skm = n_skm ? atomicAdd(a.cursors + 0, (unsigned long long)n_skm) : 0ull;
       S.base_byte = rounded ? atomicAdd(a.cursors + 1, (unsigned long long)rounded) : 0ull;
       if (S.base_skm + n_skm > a.cap_skm || S.base_byte + rounded > a.cap_bytes)
@@ -344,7 +369,7 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
       int e = (j + 1 < n_brk) ? S.brk[j + 1] : S.ext_end;
       uint32_t nk = (uint32_t)(e - l);
       uint32_t len = nk + k - 1;
-      uint32_t mv = S.b.mm[l];
+      uint32_t mv = S.b.smm[i];
       uint32_t bin = mv % (uint32_t)a.nbins;
       if (len > 0xFFFFFFu) atomicOr(a.err, ERR_BAD_READ);
       if (fits && len <= 0xFFFFFFu) {
@@ -362,8 +387,32 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
       }
     }
 
-    // ---- packed bytes: one 32-bit word per thread step ----
-    if (fits) {
+    // ---- packed bytes: each superkmer's bases cut from the tile's 2-bit
+    //      stream into the staging area, then written out in 16-byte pieces ----
+    if (fits && S.use_stg) {
+      for (int i = tid; i < (int)n_skm; i += PT_NT) {
+        const uint32_t j = S.skm[i];
+        const int l = S.brk[j];
+        const int e = (j + 1 < n_brk) ? S.brk[j + 1] : S.ext_end;
+        const uint32_t len = (uint32_t)(e - l) + k - 1, nb = (len + 3) / 4;
+        uint8_t *dst = S.stg + S.a.boff[i];
+        for (uint32_t m = 0; 16 * m < len; m++) {
+          const uint32_t B = (uint32_t)l + 16 * m, w = B >> 4, sh = 2 * (B & 15u);
+          uint32_t v = sh ? (S.pk[w] << sh) | (S.pk[w + 1] >> (32 - sh)) : S.pk[w];
+          const uint32_t rem = len - 16 * m;
+          if (rem < 16) v &= 0xFFFFFFFFu << (32 - 2 * rem);  // zero padding after the last base
+#pragma unroll
+          for (int u = 0; u < 4; u++)
+            if (4 * m + u < nb) dst[4 * m + u] = (uint8_t)(v >> (24 - 8 * u));
+        }
+      }
+      if (tid < 16 && tile_bytes + tid < ((tile_bytes + 15u) & ~15u)) S.stg[tile_bytes + tid] = 0;
+      __syncthreads();
+      const uint32_t n16 = (tile_bytes + 15u) / 16u;
+      uint4 *dst16 = reinterpret_cast<uint4 *>(a.packed + base_byte);
+      const uint4 *src16 = reinterpret_cast<const uint4 *>(S.stg);
+      for (uint32_t v = tid; v < n16; v += PT_NT) dst16[v] = src16[v];
+    } else if (fits) {
       const uint32_t nwords = (tile_bytes + 3) / 4;
       uint32_t *dst = reinterpret_cast<uint32_t *>(a.packed + base_byte);
       for (uint32_t w = tid; w < nwords; w += PT_NT) {
@@ -479,25 +528,83 @@ __global__ void k_bin_count(const unsigned long long *n_skm_ptr, const uint32_t 
   }
 }
 
-__global__ void k_bin_place(const unsigned long long *n_skm_ptr, const uint64_t *desc, const uint32_t *mm,
-                            uint32_t nbins, uint64_t nch_cap, const uint64_t *off, uint64_t *out_desc,
-                            uint32_t *out_mm, const uint32_t *err) {
-  extern __shared__ unsigned long long cur[];
+// Each chunk is placed in sub-rounds of kBinRound superkmers: counted per
+// bin in shared memory, grouped by bin there, then written out so that each
+// bin's superkmers leave as a run of consecutive slots.
+__global__ void __launch_bounds__(kBinPlaceThreads, 2) k_bin_place(const unsigned long long *n_skm_ptr,
+                                                                const uint64_t *desc, const uint32_t *mm,
+                                                                uint32_t nbins, uint64_t nch_cap,
+                                                                const uint64_t *off, uint64_t *out_desc,
+                                                                uint32_t *out_mm, const uint32_t *err) {
+  extern __shared__ __align__(16) uint8_t bp_raw[];
+  uint64_t *st_desc = reinterpret_cast<uint64_t *>(bp_raw);               // kBinRound
+  uint32_t *st_mm = reinterpret_cast<uint32_t *>(st_desc + kBinRound);   // kBinRound
+  uint64_t *cur = reinterpret_cast<uint64_t *>(st_mm + kBinRound);       // nbins: next global slot
+  uint32_t *cnt = reinterpret_cast<uint32_t *>(cur + nbins);             // nbins: counts, then cursors
+  uint32_t *lst = cnt + nbins;                                            // nbins: starts in the round
+  __shared__ uint32_t tmp[64];
   if (*err & (ERR_CAPACITY | ERR_BAD_READ)) return;
   const uint64_t n = *n_skm_ptr;
   const uint64_t nch = min(nch_cap, (n + kBinChunk - 1) / kBinChunk);
+  const int tid = threadIdx.x;
   for (uint64_t c = blockIdx.x; c < nch; c += gridDim.x) {
-    for (uint32_t b = threadIdx.x; b < nbins; b += blockDim.x) cur[b] = off[(uint64_t)b * nch_cap + c];
-    __syncthreads();
-    const uint64_t i1 = min(n, (c + 1) * (uint64_t)kBinChunk);
-    for (uint64_t i = c * (uint64_t)kBinChunk + threadIdx.x; i < i1; i += blockDim.x) {
-      const uint32_t m = mm[i];
-      const uint64_t slot = atomicAdd(&cur[m % nbins], 1ull);
-      out_desc[slot] = desc[i];
-      out_mm[slot] = m;
+    for (uint32_t b = tid; b < nbins; b += kBinPlaceThreads) cur[b] = off[(uint64_t)b * nch_cap + c];
+    const uint64_t c1 = min(n, (c + 1) * (uint64_t)kBinChunk);
+    for (uint64_t r0 = c * (uint64_t)kBinChunk; r0 < c1; r0 += kBinRound) {
+      const uint32_t m = (uint32_t)min((uint64_t)kBinRound, c1 - r0);
+      for (uint32_t b = tid; b < nbins; b += kBinPlaceThreads) cnt[b] = 0;
+      __syncthreads();
+      constexpr int PER = kBinRound / kBinPlaceThreads;
+      uint64_t dv[PER];
+      uint32_t mv[PER], rk[PER];
+#pragma unroll
+      for (int u = 0; u < PER; u++) {
+        const uint32_t i = u * kBinPlaceThreads + tid;
+        if (i < m) {
+          dv[u] = desc[r0 + i];
+          mv[u] = mm[r0 + i];
+          rk[u] = atomicAdd(&cnt[mv[u] % nbins], 1u);
+        }
+      }
+      __syncthreads();
+      // exclusive scan of the bin counts (thread-contiguous groups)
+      {
+        const uint32_t per = (nbins + kBinPlaceThreads - 1) / kBinPlaceThreads, b0 = tid * per;
+        uint32_t s = 0;
+        for (uint32_t b = b0; b < b0 + per && b < nbins; b++) s += cnt[b];
+        uint32_t tot;
+        uint32_t run = block_exclusive_scan<kBinPlaceThreads>(s, tmp, &tot);
+        for (uint32_t b = b0; b < b0 + per && b < nbins; b++) {
+          lst[b] = run;
+          run += cnt[b];
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < PER; u++) {
+        const uint32_t i = u * kBinPlaceThreads + tid;
+        if (i < m) {
+          const uint32_t p = lst[mv[u] % nbins] + rk[u];
+          st_desc[p] = dv[u];
+          st_mm[p] = mv[u];
+        }
+      }
+      __syncthreads();
+      for (uint32_t i = tid; i < m; i += kBinPlaceThreads) {
+        const uint32_t v = st_mm[i], b = v % nbins;
+        const uint64_t slot = cur[b] + (i - lst[b]);
+        out_desc[slot] = st_desc[i];
+        out_mm[slot] = v;
+      }
+      __syncthreads();
+      for (uint32_t b = tid; b < nbins; b += kBinPlaceThreads) cur[b] += cnt[b];
+      __syncthreads();
     }
-    __syncthreads();
   }
+}
+
+size_t bin_place_smem_bytes(uint32_t nbins) {
+  return (size_t)kBinRound * 12 + (size_t)nbins * 16;
 }
 
 // Exclusive scans of the per-bin counters (one thread; nbins is small).

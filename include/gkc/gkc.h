@@ -272,6 +272,47 @@ gkc_status gkc_db_lookup(const gkc_db *db, const uint64_t *keys, uint64_t n, uin
 /* Records first .. first+n-1 as keys and counts (either may be NULL). */
 gkc_status gkc_db_read(const gkc_db *db, uint64_t first, uint64_t n, uint64_t *keys, uint32_t *counts);
 
+/* ---- launch-shape tuning (the reference fixes its launch shape by hand:
+ *      NUM_BLOCKS_PER_GRID, NUM_THREADS_PER_BLOCK and the stream count,
+ *      experiment.cpp:234-238).  Shapes of the batched count stage that need
+ *      no rebuild: the largest mean keys per count bucket (the coarse digit
+ *      width of each bin follows from it), the k-mers per histogram chunk
+ *      (a power of two) and the count kernel's CTAs per SM.  Zero fields
+ *      mean the default. ---- */
+typedef struct gkc_tune_params {
+  uint32_t coarse_target;      /* 256 .. 65536; default 4096 */
+  uint32_t chunk_kmers;        /* 4096 .. 2^22, a power of two; default 65536 */
+  uint32_t count_ctas_per_sm;  /* 1 .. 4; default 2 */
+  uint32_t reserved;
+} gkc_tune_params;
+typedef struct gkc_tune_report {
+  gkc_tune_params chosen, defaults;
+  float default_ms, tuned_ms;  /* count stages on the sample, median of 3 replays */
+  uint32_t candidates;         /* shapes timed */
+  int from_cache;              /* 1: taken from the cache, nothing timed */
+  uint64_t sample_bases;
+} gkc_tune_report;
+gkc_status gkc_tune_get(const gkc_ctx *ctx, gkc_tune_params *out);
+/* NULL restores the defaults.  Applies to the context's later calls. */
+gkc_status gkc_tune_set(gkc_ctx *ctx, const gkc_tune_params *p);
+/* Chooses the shapes for this input's class by timing candidates on a sample
+ * of the reads (the first ones, about 2^28 bases), one dimension at a time
+ * from the defaults, and sets them on the context.  The choice is cached per
+ * (SM count, key width, read-length class: mean above 1 kbp or not, bin
+ * count); a cached choice is used without timing unless force != 0.  The
+ * context's partition and count results are replaced by the sample's. */
+gkc_status gkc_autotune_device(gkc_ctx *ctx, const gkc_params *prm, const char *d_reads, uint64_t n_bytes,
+                               const uint64_t *d_offs, uint64_t n_reads, int force, gkc_tune_report *out);
+/* The process-wide cache (host only, needs no GPU). */
+gkc_status gkc_tune_cache_lookup(int sm_count, const gkc_params *prm, uint64_t n_bases, uint64_t n_reads,
+                                 gkc_tune_params *out);
+gkc_status gkc_tune_cache_store(int sm_count, const gkc_params *prm, uint64_t n_bases, uint64_t n_reads,
+                                const gkc_tune_params *p);
+void gkc_tune_cache_clear(void);
+/* Text file, one entry per line; load merges into the cache. */
+gkc_status gkc_tune_cache_save(const char *path);
+gkc_status gkc_tune_cache_load(const char *path);
+
 /* ---- whole pipeline: reads -> superkmer partitions -> sorted (k-mer, count)
  *      (reference: process_reads_count + gen_skm_and_count_with_TP,
  *      experiment.cpp:76-89,156-219) ---- */
