@@ -140,6 +140,8 @@ SIGNATURES = [
     ("gkc_pipeline_device", C.c_int, [vp, P(Params), C.c_int, vp, u64, vp, u64, P(PartitionView),
                                       P(CountView)]),
     ("gkc_pipeline_host", C.c_int, [vp, P(Params), C.c_int, vp, vp, u64, P(CountView)]),
+    ("gkc_stream_submit", C.c_int, [vp, P(Params), vp, vp, u64, vp, vp, vp, u64, P(u64)]),
+    ("gkc_stream_wait", C.c_int, [vp, u64, P(u64), P(u64)]),
     ("gkc_minimizers_device", C.c_int, [vp, P(Params), vp, u64, vp, u64, vp, vp, vp]),
     ("gkc_subsample_positions_device", C.c_int, [vp, P(Params), u32, vp, u64, vp, u64,
                                                  P(PoslistView)]),
@@ -398,6 +400,20 @@ class Context:
                                               _ptr(offs), len(offs) - 1, C.byref(cv)),
                     "pipeline_host")
         return cv
+
+    def stream_submit(self, reads, offs, n_reads, prm, bin_off, keys, counts, capacity):
+        """Streaming host form: page-locked tensors in and out; -> ticket."""
+        t = C.c_uint64()
+        self._check(self._L.gkc_stream_submit(self.h, C.byref(prm), _ptr(reads), _ptr(offs), int(n_reads),
+                                              _ptr(bin_off), _ptr(keys), _ptr(counts), int(capacity),
+                                              C.byref(t)), "stream_submit")
+        return int(t.value)
+
+    def stream_wait(self, ticket):
+        """-> (n_distinct, n_kmers) once the call's results are in host memory."""
+        nd, nk = C.c_uint64(), C.c_uint64()
+        self._check(self._L.gkc_stream_wait(self.h, int(ticket), C.byref(nd), C.byref(nk)), "stream_wait")
+        return int(nd.value), int(nk.value)
 
     def minimizers_device(self, d_reads, n_bytes, d_offs, n_reads, prm, d_mm, d_pos, d_strand):
         self._check(self._L.gkc_minimizers_device(self.h, C.byref(prm), _ptr(d_reads), int(n_bytes),

@@ -148,7 +148,7 @@ void *ws_get(gkc_ctx *c, const char *name, size_t bytes, gkc_status *st) {
     cudaFreeAsync(it->second.p, c->st);
     c->used -= old;
     c->bufs.erase(it);
-    c->graph_valid = false;
+    graphs_invalidate(c);
   }
   size_t want = std::max(bytes, old + old / 4);
   if (c->budget && c->used + want > c->budget) want = bytes;
@@ -167,22 +167,23 @@ void *ws_get(gkc_ctx *c, const char *name, size_t bytes, gkc_status *st) {
   }
   c->used += want;
   c->bufs[name] = DevBuf{p, want};
-  c->graph_valid = false;
+  if (old) graphs_invalidate(c);  // captured graphs may hold the freed buffer; a new one is in none
   return p;
 }
 
 // Frees every workspace of c into the pool (ordered on c's stream).
 void ws_release_all(gkc_ctx *c) {
   cudaStreamSynchronize(c->st);
-  if (c->gexec) {
-    cudaGraphExecDestroy(c->gexec);
-    c->gexec = nullptr;
-  }
+  for (auto &g : c->graphs)
+    if (g.exec) {
+      cudaGraphExecDestroy(g.exec);
+      g.exec = nullptr;
+    }
   for (auto &kv : c->bufs) cudaFreeAsync(kv.second.p, c->st);
   cudaStreamSynchronize(c->st);
   c->bufs.clear();
   c->used = 0;
-  c->graph_valid = false;
+  graphs_invalidate(c);
   c->have_part = c->have_count = false;
 }
 
@@ -238,10 +239,12 @@ gkc_status gkc_ctx_create(int device_id, uint64_t hbm_budget_bytes, gkc_ctx **ou
     return GKC_ERR_CUDA;
   }
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMallocHost(&c->h_tot, sizeof(DevTotals)) != cudaSuccess) {
+      cudaMallocHost(&c->h_tots[0], 2 * sizeof(DevTotals)) != cudaSuccess) {
     delete c;
     return GKC_ERR_CUDA;
   }
+  c->h_tots[1] = c->h_tots[0] + 1;
+  c->h_tot = c->h_tots[0];
   c->own_stream = true;
   for (int i = 0; i < 4; i++) cudaEventCreate(&c->ev[i]);
   for (int i = 0; i <= GKC_MAX_STAGES; i++) cudaEventCreate(&c->sev[i]);
@@ -259,7 +262,14 @@ void gkc_ctx_destroy(gkc_ctx *c) {
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   for (int i = 0; i <= GKC_MAX_STAGES; i++)
     if (c->sev[i]) cudaEventDestroy(c->sev[i]);
-  if (c->h_tot) cudaFreeHost(c->h_tot);
+  if (c->h_tots[0]) cudaFreeHost(c->h_tots[0]);
+  if (c->st_up) cudaStreamDestroy(c->st_up);
+  if (c->st_dl) cudaStreamDestroy(c->st_dl);
+  for (int i = 0; i < 2; i++) {
+    if (c->ev_up[i]) cudaEventDestroy(c->ev_up[i]);
+    if (c->ev_comp[i]) cudaEventDestroy(c->ev_comp[i]);
+    if (c->ev_dl[i]) cudaEventDestroy(c->ev_dl[i]);
+  }
   if (c->own_stream && c->st) cudaStreamDestroy(c->st);
   delete c;
 }
@@ -272,7 +282,7 @@ gkc_status gkc_ctx_set_filter(gkc_ctx *c, int filter) {
     return ctx_fail(c, GKC_ERR_INVALID_ARG, "unknown minimizer filter");
   if (filter != c->filter) {
     c->filter = filter;
-    c->graph_valid = false;
+    graphs_invalidate(c);
     c->have_part = c->have_count = false;
   }
   return GKC_OK;
@@ -285,7 +295,7 @@ gkc_status gkc_ctx_set_stream(gkc_ctx *c, void *stream) {
   if (c->own_stream) cudaStreamDestroy(c->st);
   c->st = (cudaStream_t)stream;
   c->own_stream = false;
-  c->graph_valid = false;
+  graphs_invalidate(c);
   return GKC_OK;
 }
 
@@ -523,7 +533,7 @@ static gkc_status fill_partition_view(gkc_ctx *c, const gkc_params *prm, uint64_
 
 static gkc_status read_totals(gkc_ctx *c, bool with_count, uint32_t nbins) {
   const uint64_t *bk = (const uint64_t *)c->bufs["bin_kstart"].p;
-  const uint64_t *bo = with_count ? (const uint64_t *)c->bufs["bin_out"].p : nullptr;
+  const uint64_t *bo = with_count ? (const uint64_t *)c->bufs[slot_name(c, "bin_out")].p : nullptr;
   WS(dt, DevTotals, "totals", 1);
   k_finalize<<<1, 1, 0, c->st>>>(dt, (const unsigned long long *)c->bufs["cursors"].p,
                                  (const uint32_t *)c->bufs["err"].p, bk, nbins, c->part_nbytes_dev, bo);
@@ -548,7 +558,7 @@ gkc_status partition_device_impl(gkc_ctx *c, const gkc_params *prm, const char *
   uint64_t cap_skm, cap_bytes;
   partition_caps(prm, n_bytes, n_reads, &cap_skm, &cap_bytes);
   for (int attempt = 0; attempt < 2; attempt++) {
-    c->graph_valid = false;
+    graphs_invalidate(c);
     gkc_status s = enqueue_partition(c, prm, d_reads, n_bytes, d_offs, n_reads, cap_skm, cap_bytes);
     if (s != GKC_OK) return s;
     s = read_totals(c, false, (uint32_t)prm->nbins);
@@ -674,13 +684,13 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   LAUNCHED(c);
 
   // counting: one look-back word per bucket; oversized buckets go through the scratch area
-  WS(out_keys, K, "out_keys", keys_cap);
-  WS(out_counts, uint32_t, "counts", keys_cap);
+  WS(out_keys, K, slot_name(c, "out_keys").c_str(), keys_cap);
+  WS(out_counts, uint32_t, slot_name(c, "counts").c_str(), keys_cap);
   WS(lookback, unsigned long long, "lookback", max_buckets + 1);
   WS(ticket, unsigned long long, "lb_ticket", 4);
   scratch_keys = std::max<uint64_t>(scratch_keys, 1 << 16);
   WS(scratch, K, "sort_scratch", scratch_keys);
-  WS(bin_out, uint64_t, "bin_out", nbins + 1);
+  WS(bin_out, uint64_t, slot_name(c, "bin_out").c_str(), nbins + 1);
   CK(cudaMemsetAsync(ticket, 0, 32, c->st));
   CK(cudaMemsetAsync(lookback, 0, (max_buckets + 1) * 8, c->st));
   SortCountArgs sa;
@@ -732,9 +742,9 @@ static void fill_count_view(gkc_ctx *c, const gkc_params *prm) {
   v.n_kmers = c->h_tot->n_kmers;
   v.nbins = (uint32_t)prm->nbins;
   v.key_words = prm->k <= 32 ? 1 : 2;
-  v.bin_off = (const uint64_t *)c->bufs["bin_out"].p;
-  v.keys = (const uint64_t *)c->bufs["out_keys"].p;
-  v.counts = (const uint32_t *)c->bufs["counts"].p;
+  v.bin_off = (const uint64_t *)c->bufs[slot_name(c, "bin_out")].p;
+  v.keys = (const uint64_t *)c->bufs[slot_name(c, "out_keys")].p;
+  v.counts = (const uint32_t *)c->bufs[slot_name(c, "counts")].p;
   c->ck = prm->k;
   c->have_count = true;
   c->count_gen++;
@@ -793,30 +803,36 @@ gkc_status gkc_count_device(gkc_ctx *c, const gkc_params *prm, gkc_mode mode, gk
 
 // Batched: the whole partition -> count pipeline is enqueued once under
 // stream capture and replayed as a CUDA graph while inputs and parameters are
-// unchanged.  All sizes the kernels need are read on the device.
+// unchanged (one graph per buffer slot).  All sizes the kernels need are read
+// on the device.  With `async`, a replay is only enqueued: its totals land in
+// the slot's pinned totals and are checked by the caller after the stream.
 static gkc_status pipeline_batched(gkc_ctx *c, const gkc_params *prm, const char *d_reads,
-                                   uint64_t n_bytes, const uint64_t *d_offs, uint64_t n_reads) {
+                                   uint64_t n_bytes, const uint64_t *d_offs, uint64_t n_reads,
+                                   bool async = false) {
   GraphKey key{d_reads, d_offs, n_bytes, n_reads, prm->k, prm->p, prm->hpc, prm->nbins, c->filter};
+  SlotGraph &G = c->graphs[c->slot];
   uint64_t cap_skm, cap_bytes;
   partition_caps(prm, n_bytes, n_reads, &cap_skm, &cap_bytes);
-  if (c->graph_valid && c->gkey == key && c->gexec) {
+  const bool have = G.valid && G.key == key && G.exec;
+  if (have) {
     cap_skm = c->part_cap_skm;
     cap_bytes = c->part_cap_bytes;
   }
   uint64_t keys_cap = std::max<uint64_t>(n_bytes, 16);
-  if (c->graph_valid && c->gkey == key) keys_cap = c->count_keys_cap;
+  if (have) keys_cap = c->count_keys_cap;
   for (int attempt = 0; attempt < 3; attempt++) {
-    if (c->graph_valid && c->gkey == key && c->gexec) {
-      CK(cudaGraphLaunch(c->gexec, c->st));
+    if (G.valid && G.key == key && G.exec) {
+      CK(cudaGraphLaunch(G.exec, c->st));
       c->tm.graph_replayed = 1;
-      c->launches = c->graph_launches;
+      c->launches = G.launches;
+      if (async) return GKC_OK;
     } else {
       // allocate every workspace outside capture: one dry enqueue sizes them
       c->launches = 0;
       CK(cudaStreamSynchronize(c->st));
-      if (c->gexec) {
-        cudaGraphExecDestroy(c->gexec);
-        c->gexec = nullptr;
+      if (G.exec) {
+        cudaGraphExecDestroy(G.exec);
+        G.exec = nullptr;
       }
       cudaStreamCaptureStatus cs;
       CK(cudaStreamIsCapturing(c->st, &cs));
@@ -833,7 +849,7 @@ static gkc_status pipeline_batched(gkc_ctx *c, const gkc_params *prm, const char
       }
       if (!(c->h_tot->err & (ERR_CAPACITY | ERR_OVERSIZE_SCRATCH))) {
         // capture the same sequence into a graph for later replays
-        c->graph_valid = true;
+        G.valid = true;
         uint32_t launches = c->launches;
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
@@ -846,13 +862,13 @@ static gkc_status pipeline_batched(gkc_ctx *c, const gkc_params *prm, const char
         c->capturing = false;
         if (s != GKC_OK) return s;
         CK(e);
-        if (!c->graph_valid) {  // a workspace moved during capture: do not keep it
+        if (!G.valid) {  // a workspace moved during capture: do not keep it
           cudaGraphDestroy(g);
         } else {
-          CK(cudaGraphInstantiate(&c->gexec, g, 0));
+          CK(cudaGraphInstantiate(&G.exec, g, 0));
           cudaGraphDestroy(g);
-          c->gkey = key;
-          c->graph_launches = c->launches;
+          G.key = key;
+          G.launches = c->launches;
         }
         c->launches = launches;
         c->tm.graph_replayed = 0;
@@ -862,7 +878,7 @@ static gkc_status pipeline_batched(gkc_ctx *c, const gkc_params *prm, const char
     CK(cudaStreamSynchronize(c->st));
     if (!(c->h_tot->err & (ERR_CAPACITY | ERR_OVERSIZE_SCRATCH))) break;
     // grow to the sizes the device reported and retry
-    c->graph_valid = false;
+    graphs_invalidate(c);
     if (c->h_tot->err & ERR_OVERSIZE_SCRATCH) c->scratch_full = true;
     cap_skm = std::max<uint64_t>(cap_skm, c->h_tot->n_skm + 16);
     cap_bytes = std::max<uint64_t>(cap_bytes, c->h_tot->n_packed + 64);
@@ -871,7 +887,7 @@ static gkc_status pipeline_batched(gkc_ctx *c, const gkc_params *prm, const char
   }
   CK(cudaStreamSynchronize(c->st));
   if (c->h_tot->err & (ERR_CAPACITY | ERR_OVERSIZE_SCRATCH)) {
-    c->graph_valid = false;
+    graphs_invalidate(c);
     return ctx_fail(c, GKC_ERR_CAPACITY, "pipeline capacity");
   }
   gkc_status s = check_device_err(c);
@@ -919,8 +935,8 @@ gkc_status upload_reads(gkc_ctx *c, const char *reads, const uint64_t *offs, uin
                         char **d_reads, uint64_t **d_offs, uint64_t *n_bytes) {
   const uint64_t base = n_reads ? offs[0] : 0;
   const uint64_t nb = n_reads ? offs[n_reads] - base : 0;
-  WS(dr, char, "in_reads", nb + 64);
-  WS(doffs, uint64_t, "in_offs", n_reads + 1);
+  WS(dr, char, slot_name(c, "in_reads").c_str(), nb + 64);
+  WS(doffs, uint64_t, slot_name(c, "in_offs").c_str(), n_reads + 1);
   if (nb) CK(cudaMemcpyAsync(dr, reads + base, nb, cudaMemcpyHostToDevice, c->st));
   if (base == 0) {
     CK(cudaMemcpyAsync(doffs, offs, (n_reads + 1) * 8, cudaMemcpyHostToDevice, c->st));
@@ -965,6 +981,144 @@ gkc_status gkc_pipeline_host(gkc_ctx *c, const gkc_params *prm, gkc_mode mode, c
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev[3], c->ev[0]);
   c->tm.h2d_ms = ms;
+  return GKC_OK;
+}
+
+// ------------------------------------------------------ streaming host form
+
+// offs[i] -= offs[0] (offsets of a batch cut from a larger CSR); one CTA
+__global__ void k_rebase_offs(uint64_t *offs, uint64_t n) {
+  const uint64_t base = offs[0];
+  __syncthreads();  // every thread has read offs[0]
+  for (uint64_t i = threadIdx.x + 1; i <= n; i += blockDim.x) offs[i] -= base;
+  __syncthreads();
+  if (threadIdx.x == 0) offs[0] = 0;
+}
+
+// The slot's count result into host memory the device can write (page-locked
+// buffers): bin offsets, then at most `capacity` keys and counts, in 16-byte
+// pieces where both sides allow it.  The totals' n_distinct (copied to the
+// host inside the pipeline) tells the waiter how much is valid.
+__global__ void k_copy_out(const uint64_t *bin_out, uint32_t nbins, const uint8_t *keys, const uint8_t *counts,
+                           int key_words, uint64_t capacity, uint64_t *h_bin_off, uint8_t *h_keys,
+                           uint8_t *h_counts) {
+  const uint64_t nd = min(bin_out[nbins], capacity);
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t nt = (uint64_t)gridDim.x * blockDim.x;
+  if (h_bin_off)
+    for (uint64_t i = tid; i <= nbins; i += nt) h_bin_off[i] = bin_out[i];
+  auto copy = [&](const uint8_t *src, uint8_t *dst, uint64_t bytes) {
+    if (!dst) return;
+    const bool vec = (((uintptr_t)src | (uintptr_t)dst) & 15) == 0;
+    const uint64_t n16 = vec ? bytes / 16 : 0;
+    for (uint64_t i = tid; i < n16; i += nt)
+      reinterpret_cast<uint4 *>(dst)[i] = reinterpret_cast<const uint4 *>(src)[i];
+    for (uint64_t i = n16 * 16 + tid; i < bytes; i += nt) dst[i] = src[i];
+  };
+  copy(keys, h_keys, nd * 8 * (uint64_t)key_words);
+  copy(counts, h_counts, nd * 4);
+}
+
+static bool host_visible(const void *p) {
+  if (!p) return true;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost && a.devicePointer != nullptr;
+}
+
+gkc_status gkc_stream_submit(gkc_ctx *c, const gkc_params *prm, const char *reads, const uint64_t *offs,
+                             uint64_t n_reads, uint64_t *bin_off, uint64_t *keys, uint32_t *counts,
+                             uint64_t capacity, uint64_t *ticket) {
+  if (!c || !ticket || (n_reads && (!reads || !offs))) return GKC_ERR_INVALID_ARG;
+  gkc_status s = check_params(c, prm);
+  if (s != GKC_OK) return s;
+  if (!host_visible(reads) || !host_visible(offs) || !host_visible(bin_off) || !host_visible(keys) ||
+      !host_visible(counts))
+    return ctx_fail(c, GKC_ERR_INVALID_ARG, "streaming buffers must be page-locked host memory");
+  cudaSetDevice(c->dev);
+  if (!c->st_up) {
+    CK(cudaStreamCreateWithFlags(&c->st_up, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->st_dl, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; i++) {
+      CK(cudaEventCreateWithFlags(&c->ev_up[i], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->ev_comp[i], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->ev_dl[i], cudaEventDisableTiming));
+    }
+  }
+  const uint64_t t = c->next_ticket;
+  const int slot = (int)(t & 1);
+  // the slot's input buffers; growing them waits for everything in flight
+  const uint64_t base = n_reads ? offs[0] : 0, nb = n_reads ? offs[n_reads] - base : 0;
+  c->slot = slot;
+  c->h_tot = c->h_tots[slot];
+  struct SlotReset {  // every return leaves the context on slot 0
+    gkc_ctx *c;
+    ~SlotReset() {
+      c->slot = 0;
+      c->h_tot = c->h_tots[0];
+    }
+  } reset{c};
+  const std::string rn = slot_name(c, "in_reads"), on = slot_name(c, "in_offs");
+  auto fits = [&](const std::string &n, size_t bytes) {
+    auto it = c->bufs.find(n);
+    return it != c->bufs.end() && it->second.bytes >= bytes;
+  };
+  if (!fits(rn, nb + 64) || !fits(on, 8 * (n_reads + 1))) {
+    CK(cudaStreamSynchronize(c->st_up));
+    CK(cudaStreamSynchronize(c->st_dl));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  WS(dr, char, rn.c_str(), nb + 64);
+  WS(doffs, uint64_t, on.c_str(), n_reads + 1);
+  // inputs of the slot's previous call must have been read before they are replaced
+  if (t >= 2) CK(cudaStreamWaitEvent(c->st_up, c->ev_comp[slot], 0));
+  if (nb) CK(cudaMemcpyAsync(dr, reads + base, nb, cudaMemcpyHostToDevice, c->st_up));
+  CK(cudaMemcpyAsync(doffs, offs, 8 * (n_reads + 1), cudaMemcpyHostToDevice, c->st_up));
+  CK(cudaEventRecord(c->ev_up[slot], c->st_up));
+  CK(cudaStreamWaitEvent(c->st, c->ev_up[slot], 0));
+  // and its outputs must have been copied out before they are recomputed
+  if (t >= 2) CK(cudaStreamWaitEvent(c->st, c->ev_dl[slot], 0));
+  if (base) {
+    k_rebase_offs<<<1, 1024, 0, c->st>>>(doffs, n_reads);
+    LAUNCHED(c);
+  }
+  c->tm = gkc_timings{};
+  s = pipeline_batched(c, prm, dr, nb, doffs, n_reads, true);
+  if (s != GKC_OK) return s;
+  CK(cudaEventRecord(c->ev_comp[slot], c->st));
+  CK(cudaStreamWaitEvent(c->st_dl, c->ev_comp[slot], 0));
+  const int kw = prm->k <= 32 ? 1 : 2;
+  k_copy_out<<<64, 256, 0, c->st_dl>>>((const uint64_t *)c->bufs[slot_name(c, "bin_out")].p, (uint32_t)prm->nbins,
+                                      (const uint8_t *)c->bufs[slot_name(c, "out_keys")].p,
+                                      (const uint8_t *)c->bufs[slot_name(c, "counts")].p, kw, capacity, bin_off,
+                                      reinterpret_cast<uint8_t *>(keys), reinterpret_cast<uint8_t *>(counts));
+  LAUNCHED(c);
+  CK(cudaEventRecord(c->ev_dl[slot], c->st_dl));
+  c->calls[slot] = StreamCall{t, capacity, (uint32_t)prm->nbins, kw};
+  c->next_ticket = t + 1;
+  *ticket = t;
+  return GKC_OK;
+}
+
+gkc_status gkc_stream_wait(gkc_ctx *c, uint64_t ticket, uint64_t *n_distinct, uint64_t *n_kmers) {
+  if (!c) return GKC_ERR_INVALID_ARG;
+  const int slot = (int)(ticket & 1);
+  if (c->calls[slot].ticket != ticket) return ctx_fail(c, GKC_ERR_NOT_FOUND, "no call in flight with this ticket");
+  cudaSetDevice(c->dev);
+  CK(cudaEventSynchronize(c->ev_dl[slot]));
+  const DevTotals *h = c->h_tots[slot];
+  if (n_distinct) *n_distinct = h->n_distinct;
+  if (n_kmers) *n_kmers = h->n_kmers;
+  if (h->err & (ERR_CAPACITY | ERR_OVERSIZE_SCRATCH))
+    return ctx_fail(c, GKC_ERR_CAPACITY, "the call's input outgrew the captured pipeline: run it with gkc_pipeline_host");
+  if (h->err & ERR_BIN_TOO_LARGE) return ctx_fail(c, GKC_ERR_CAPACITY, "a bin holds 2^32 or more k-mers");
+  if (h->err & ERR_SPIN_TIMEOUT) return ctx_fail(c, GKC_ERR_DEVICE_TIMEOUT, "device look-back wait timed out");
+  if (h->err & (ERR_BOUNDS | ERR_BAD_READ)) return ctx_fail(c, GKC_ERR_INTERNAL, "device check failed");
+  if (h->n_distinct > c->calls[slot].capacity)
+    return ctx_fail(c, GKC_ERR_CAPACITY, "result larger than the output capacity (first entries copied)");
   return GKC_OK;
 }
 
@@ -1107,7 +1261,7 @@ gkc_status gkc_count_superkmers_host(gkc_ctx *c, int k, const uint32_t *skm_len,
   c->have_part = true;
   gkc_params prm{k, 3, 0, 1};
   c->pp = prm;
-  c->graph_valid = false;
+  graphs_invalidate(c);
   gkc_status s = gkc_count_device(c, &prm, mode, nullptr);
   if (s != GKC_OK) return s;
   if (n_distinct) *n_distinct = c->cv.n_distinct;

@@ -38,6 +38,22 @@ struct TuneChoice {
   uint32_t count_ctas = 0;     // count kernel CTAs per SM
 };
 
+// A captured batched pipeline for one buffer slot.
+struct SlotGraph {
+  bool valid = false;  // captured against the current workspaces and parameters
+  GraphKey key{};
+  cudaGraphExec_t exec = nullptr;
+  uint32_t launches = 0;
+};
+
+// A call of the streaming host form in flight on a slot.
+struct StreamCall {
+  uint64_t ticket = ~0ull;
+  uint64_t capacity = 0;
+  uint32_t nbins = 0;
+  int key_words = 1;
+};
+
 struct gkc_ctx {
   int dev = 0;
   TuneChoice tune;
@@ -49,7 +65,9 @@ struct gkc_ctx {
   uint64_t budget = 0, used = 0;
   std::string err;
   std::unordered_map<std::string, DevBuf> bufs;
-  DevTotals *h_tot = nullptr;  // pinned
+  DevTotals *h_tots[2] = {nullptr, nullptr};  // pinned, one per slot
+  DevTotals *h_tot = nullptr;                 // the current slot's
+  int slot = 0;  // buffer set of the inputs and outputs in use (streaming form: 0 or 1)
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t sev[GKC_MAX_STAGES + 1] = {};  // stage boundaries of the batched pipeline
   bool capturing = false;
@@ -77,14 +95,20 @@ struct gkc_ctx {
   uint64_t count_keys_cap = 0;
   bool scratch_full = false;  // oversized buckets needed a full-size sort scratch
   bool one_shot = false;      // inputs are not run again: no graph capture
-  // graph of the batched pipeline
-  bool graph_valid = false;
-  GraphKey gkey{};
-  cudaGraphExec_t gexec = nullptr;
-  uint32_t graph_launches = 0;
+  // graphs of the batched pipeline, one per slot
+  SlotGraph graphs[2];
+  // streaming host form: upload and download streams, events per slot
+  cudaStream_t st_up = nullptr, st_dl = nullptr;
+  cudaEvent_t ev_up[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr}, ev_dl[2] = {nullptr, nullptr};
+  StreamCall calls[2];
+  uint64_t next_ticket = 0;
   // host scratch
   std::vector<uint64_t> offs_tmp, desc_tmp;
 };
+
+inline void graphs_invalidate(gkc_ctx *c) { c->graphs[0].valid = c->graphs[1].valid = false; }
+// Workspace name of the current slot's copy of a per-slot buffer.
+inline std::string slot_name(const gkc_ctx *c, const char *n) { return c->slot ? std::string(n) + "#1" : std::string(n); }
 
 gkc_status ctx_fail(gkc_ctx *c, gkc_status s, const std::string &msg);
 gkc_status ctx_cuda(gkc_ctx *c, cudaError_t e, const char *what);

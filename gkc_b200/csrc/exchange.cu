@@ -240,7 +240,7 @@ gkc_status gkc_partition_import(gkc_ctx *c, const gkc_params *prm, uint32_t n_sr
   c->pp = *prm;
   c->have_part = true;
   c->have_count = false;
-  c->graph_valid = false;
+  graphs_invalidate(c);
   if (out) *out = v;
   return GKC_OK;
 }

@@ -83,7 +83,7 @@ gkc_status gkc_tune_set(gkc_ctx *c, const gkc_tune_params *p) {
     c->tune.coarse_target = v.coarse_target;
     c->tune.chunk_kmers = v.chunk_kmers;
     c->tune.count_ctas = v.count_ctas_per_sm;
-    c->graph_valid = false;  // the captured pipeline holds the old shapes
+    graphs_invalidate(c);  // the captured pipeline holds the old shapes
   }
   return GKC_OK;
 }

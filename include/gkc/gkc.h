@@ -323,6 +323,28 @@ gkc_status gkc_pipeline_host(gkc_ctx *ctx, const gkc_params *prm, gkc_mode mode,
                              const char *reads, const uint64_t *offs, uint64_t n_reads,
                              gkc_count_view *cnt);
 
+/* ---- streaming host form: consecutive calls overlap.  Each submitted call
+ *      is copied in, counted and its result copied out into the caller's
+ *      buffers on separate streams, so that one call's upload, the previous
+ *      call's counting and the one before's download run at the same time
+ *      (two calls' inputs and outputs are held on the device).  All buffers
+ *      must be page-locked host memory (cudaHostAlloc or cudaHostRegister),
+ *      read or written by the device until gkc_stream_wait returns for the
+ *      call; a call's results go to bin_off[nbins+1], keys and counts (room
+ *      for `capacity` pairs).  The reads of a call may be cut from a larger
+ *      CSR (offs[0] need not be 0).  A call whose reads have the size of the
+ *      call two before (the same buffer slot) replays that call's captured
+ *      pipeline; another size captures anew, which waits for the device.
+ *      gkc_stream_wait blocks until the call's results are in host memory
+ *      and returns its status; at most two calls may be in flight, and the
+ *      context's device views do not describe them.  (No reference
+ *      counterpart: the reference uploads, computes and downloads each batch
+ *      in turn, gkc_cuda.cu:414-498.) ---- */
+gkc_status gkc_stream_submit(gkc_ctx *ctx, const gkc_params *prm, const char *reads, const uint64_t *offs,
+                             uint64_t n_reads, uint64_t *bin_off, uint64_t *keys, uint32_t *counts,
+                             uint64_t capacity, uint64_t *ticket);
+gkc_status gkc_stream_wait(gkc_ctx *ctx, uint64_t ticket, uint64_t *n_distinct, uint64_t *n_kmers);
+
 /* ---- per-window minimizers with position and strand (reference declares
  *      d_mm_pos / d_mm_strand, gkc_cuda.cu:159-160, but never fills them).
  *      Arrays have n_bytes entries indexed by window start in the CSR;
