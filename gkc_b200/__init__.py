@@ -147,6 +147,7 @@ SIGNATURES = [
                                                  P(PoslistView)]),
     ("gkc_hpc_device", C.c_int, [vp, vp, u64, vp, u64, vp, vp, vp]),
     ("gkc_fastx_load", C.c_int, [C.c_char_p, C.c_int, C.c_int, P(vp), P(vp), P(u64)]),
+    ("gkc_fastx_load_ex", C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, P(vp), P(vp), P(u64)]),
     ("gkc_fastx_free", None, [vp, vp, C.c_int]),
     ("gkc_db_write", C.c_int, [vp, C.c_char_p, u32, u32, C.c_int]),
     ("gkc_db_open", C.c_int, [C.c_char_p, P(vp)]),
@@ -572,11 +573,17 @@ class Database:
         return keys[:n], counts[:n]
 
 
-def load_fastx(path, threads=0):
-    """(reads uint8, offs uint64) of a FASTA / FASTQ file (gkc_fastx_load)."""
+FASTX_JOIN_LINES, FASTX_FORMAT_FROM_CONTENT = 1, 2
+
+
+def load_fastx(path, threads=0, flags=0):
+    """(reads uint8, offs uint64) of a FASTA / FASTQ file (gkc_fastx_load_ex):
+    by default the reference's record rules (format from the file name, one
+    sequence line per FASTA record); flags FASTX_JOIN_LINES,
+    FASTX_FORMAT_FROM_CONTENT."""
     L = lib()
     r, o, n = C.c_void_p(), C.c_void_p(), C.c_uint64()
-    st = L.gkc_fastx_load(os.fsencode(path), int(threads), 0, C.byref(r), C.byref(o), C.byref(n))
+    st = L.gkc_fastx_load_ex(os.fsencode(path), int(threads), 0, int(flags), C.byref(r), C.byref(o), C.byref(n))
     if st != 0:
         raise GkcError(st, f"gkc_fastx_load {path}")
     try:

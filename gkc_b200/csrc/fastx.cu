@@ -9,13 +9,15 @@
 // the range's first line on), first counting and then copying, so that the
 // reads land in file order in one CSR without hand-offs.
 //
-// Record rules (those of the reference):
+// Record rules, by default those of the reference:
+//   format: FASTQ when the file name ends in 'q', else FASTA (load_file,
+//          read_loader.hpp:285); GKC_FASTX_FORMAT_FROM_CONTENT decides by
+//          the first byte ('@' or '>') instead;
 //   FASTQ: '@' header line, sequence line, '+' line, quality line; the
-//          sequence is the second line of the record.
-//   FASTA: '>' header line followed by sequence; the sequence is the text up
-//          to the next line that starts with '>'.  The reference takes only
-//          the first line after each header (single-line FASTA); the lines of
-//          a multi-line record are joined here.
+//          sequence is the second line of the record (:110-122);
+//   FASTA: '>' header line and the one line after it (:180-193: records of
+//          two lines); with GKC_FASTX_JOIN_LINES the sequence is every line
+//          up to the next line that starts with '>', joined.
 //   A '\r' before a line end is dropped.  Bytes are kept as they are (the
 //   pipeline maps A/C/G/T/U in either case and treats anything else as N).
 #include <cuda_runtime.h>
@@ -70,7 +72,7 @@ size_t line_end(const char *d, size_t n, size_t pos) {  // index of '\n' or n
 // Walks the records starting in [r.b, r.e); calls emit(ptr, len) for every
 // sequence piece (FASTA pieces of one record in order) and end() per record.
 template <typename Piece, typename End>
-void walk(const char *d, size_t n, Range r, bool fastq, Piece piece, End end) {
+void walk(const char *d, size_t n, Range r, bool fastq, bool join, Piece piece, End end) {
   size_t pos = r.b;
   while (pos < r.e && pos < n) {
     size_t h = line_end(d, n, pos);  // header line
@@ -85,6 +87,15 @@ void walk(const char *d, size_t n, Range r, bool fastq, Piece piece, End end) {
       size_t plus = se < n ? line_end(d, n, se + 1) : n;       // '+' line
       size_t qual = plus < n ? line_end(d, n, plus + 1) : n;   // quality line
       pos = qual < n ? qual + 1 : n;
+    } else if (!join) {
+      // the line after the header; the rest of the record up to the next
+      // header is skipped
+      size_t se = line_end(d, n, s);
+      size_t len = se - s;
+      if (len && d[s + len - 1] == '\r') len--;
+      piece(d + s, len);
+      end();
+      pos = next_record(d, n, se < n ? se + 1 : n, false);
     } else {
       size_t q = s;
       while (q < n && d[q] != '>') {
@@ -102,9 +113,11 @@ void walk(const char *d, size_t n, Range r, bool fastq, Piece piece, End end) {
 
 }  // namespace
 
-extern "C" gkc_status gkc_fastx_load(const char *path, int n_threads, int pinned, char **reads,
-                                     uint64_t **offs, uint64_t *n_reads) {
+extern "C" gkc_status gkc_fastx_load_ex(const char *path, int n_threads, int pinned, int flags, char **reads,
+                                        uint64_t **offs, uint64_t *n_reads) {
   if (!path || !reads || !offs || !n_reads || n_threads < 0) return GKC_ERR_INVALID_ARG;
+  if (flags & ~(GKC_FASTX_JOIN_LINES | GKC_FASTX_FORMAT_FROM_CONTENT)) return GKC_ERR_INVALID_ARG;
+  const bool join = (flags & GKC_FASTX_JOIN_LINES) != 0;
   *reads = nullptr;
   *offs = nullptr;
   *n_reads = 0;
@@ -121,8 +134,15 @@ extern "C" gkc_status gkc_fastx_load(const char *path, int n_threads, int pinned
   const size_t n = data.size();
   size_t first = 0;
   while (first < n && (d[first] == '\n' || d[first] == '\r')) first++;
-  if (first < n && d[first] != '>' && d[first] != '@') return GKC_ERR_INVALID_ARG;  // neither format
-  const bool fastq = first < n && d[first] == '@';
+  bool fastq;
+  if (flags & GKC_FASTX_FORMAT_FROM_CONTENT) {
+    if (first < n && d[first] != '>' && d[first] != '@') return GKC_ERR_INVALID_ARG;  // neither format
+    fastq = first < n && d[first] == '@';
+  } else {
+    const size_t pl = strlen(path);
+    fastq = pl > 0 && path[pl - 1] == 'q';
+    if (first < n && d[first] != (fastq ? '@' : '>')) return GKC_ERR_INVALID_ARG;  // not the named format
+  }
   int T = n_threads ? n_threads : (int)std::max(1u, std::thread::hardware_concurrency());
   T = (int)std::max<size_t>(1, std::min<size_t>((size_t)T, n / (1 << 20) + 1));
   // one byte range per thread, each starting at a record start
@@ -136,7 +156,7 @@ extern "C" gkc_status gkc_fastx_load(const char *path, int n_threads, int pinned
     for (auto &x : th) x.join();
   };
   run([&](int t) {
-    walk(d, n, Range{cut[t], cut[t + 1]}, fastq, [&](const char *, size_t len) { cnt_bytes[t] += len; },
+    walk(d, n, Range{cut[t], cut[t + 1]}, fastq, join, [&](const char *, size_t len) { cnt_bytes[t] += len; },
          [&] { cnt_reads[t]++; });
   });
   uint64_t R = 0, B = 0;
@@ -168,7 +188,7 @@ extern "C" gkc_status gkc_fastx_load(const char *path, int n_threads, int pinned
   run([&](int t) {
     uint64_t r = r0[t], b = b0[t];
     o[r] = b;
-    walk(d, n, Range{cut[t], cut[t + 1]}, fastq,
+    walk(d, n, Range{cut[t], cut[t + 1]}, fastq, join,
          [&](const char *p, size_t len) {
            memcpy(out + b, p, len);
            b += len;
@@ -181,6 +201,11 @@ extern "C" gkc_status gkc_fastx_load(const char *path, int n_threads, int pinned
   *offs = o;
   *n_reads = R;
   return GKC_OK;
+}
+
+extern "C" gkc_status gkc_fastx_load(const char *path, int n_threads, int pinned, char **reads, uint64_t **offs,
+                                     uint64_t *n_reads) {
+  return gkc_fastx_load_ex(path, n_threads, pinned, 0, reads, offs, n_reads);
 }
 
 extern "C" void gkc_fastx_free(char *reads, uint64_t *offs, int pinned) {

@@ -375,18 +375,25 @@ gkc_status gkc_hpc_device(gkc_ctx *ctx, const char *d_reads, uint64_t n_bytes,
                           uint64_t *d_out_offs, int32_t *d_orig_pos);
 
 /* ---- FASTA / FASTQ ingest (reference: ReadLoader, read_loader.hpp:44-196,
- *      :276-321, :470-520).  Reads the file (format from its first byte, '>'
- *      or '@'; the reference goes by the file name's last letter, :285) on
- *      n_threads threads (0: all cores) into one read CSR, in file
- *      order: *reads holds the sequences back to back, *offs their n_reads+1
- *      offsets.  FASTQ: the second line of each 4-line record; FASTA: the
- *      lines after a header up to the next header, joined (the reference
- *      keeps only the first).  A '\r' before a line end is dropped.  With
- *      pinned != 0 the arrays are page-locked (fast host-to-device copies).
- *      Free them with gkc_fastx_free and the same `pinned`.  No GPU is
- *      needed unless pinned != 0. ---- */
+ *      :276-321, :470-520).  Reads the file on n_threads threads (0: all
+ *      cores) into one read CSR, in file order: *reads holds the sequences
+ *      back to back, *offs their n_reads+1 offsets.  By default the
+ *      reference's rules: FASTQ when the file name ends in 'q', else FASTA
+ *      (:285); FASTQ: the second line of each 4-line record; FASTA: the line
+ *      after each header (the reference reads two-line records).  Flags:
+ *      GKC_FASTX_JOIN_LINES joins all lines of a FASTA record up to the next
+ *      header; GKC_FASTX_FORMAT_FROM_CONTENT takes the format from the first
+ *      byte ('>' or '@') instead of the name.  A '\r' before a line end is
+ *      dropped.  A file that does not start as its format does is refused
+ *      (GKC_ERR_INVALID_ARG).  With pinned != 0 the arrays are page-locked
+ *      (fast host-to-device copies).  Free them with gkc_fastx_free and the
+ *      same `pinned`.  No GPU is needed unless pinned != 0. ---- */
+#define GKC_FASTX_JOIN_LINES 1
+#define GKC_FASTX_FORMAT_FROM_CONTENT 2
 gkc_status gkc_fastx_load(const char *path, int n_threads, int pinned, char **reads, uint64_t **offs,
                           uint64_t *n_reads);
+gkc_status gkc_fastx_load_ex(const char *path, int n_threads, int pinned, int flags, char **reads,
+                             uint64_t **offs, uint64_t *n_reads);
 void gkc_fastx_free(char *reads, uint64_t *offs, int pinned);
 
 /* ---- serving: continuous batching of counting jobs against an HBM budget ---- */

@@ -388,3 +388,28 @@ def ref_balance_report(sizes):
     n = lib.ref_cal_var_stdev(_ptr(sizes, u64p), len(sizes), buf, len(buf))
     assert n < len(buf)
     return buf.value.decode()
+
+
+REF_LOADER_SO = os.path.join(ROOT, "oracle", "_ref", "libgkcref_loader.so")
+
+
+def ref_loader_available():
+    return os.path.exists(REF_LOADER_SO)
+
+
+def ref_load_reads(path, n_threads=1, buffer_size=0):
+    """The reads the reference's ReadLoader (read_loader.hpp) delivers for a
+    file, in order: (reads uint8, offs uint64)."""
+    lib = C.CDLL(REF_LOADER_SO)
+    lib.ref_load_reads.argtypes = [C.c_char_p, C.c_int, C.c_uint64, u64p, C.POINTER(C.c_void_p),
+                                   C.POINTER(C.c_void_p)]
+    lib.ref_free_reads.argtypes = [C.c_void_p, C.c_void_p]
+    n = np.zeros(1, np.uint64)
+    r, o = C.c_void_p(), C.c_void_p()
+    assert lib.ref_load_reads(os.fsencode(path), n_threads, buffer_size, _ptr(n, u64p), C.byref(r), C.byref(o)) == 0
+    nr = int(n[0])
+    offs = np.ctypeslib.as_array(C.cast(o, u64p), shape=(nr + 1,)).copy()
+    reads = (np.ctypeslib.as_array(C.cast(r, u8p), shape=(int(offs[-1]),)).copy() if offs[-1]
+             else np.zeros(0, np.uint8))
+    lib.ref_free_reads(r, o)
+    return reads, offs
