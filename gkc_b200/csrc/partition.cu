@@ -51,7 +51,7 @@ struct PartSmem {
     uint32_t smm[PT_T + 1];        // minimizer of each core superkmer (after the window pass)
   } b;
   uint32_t pk[PT_NLOC / 16 + 1];   // the tile's bases, 2 bits each, first base in the top bits
-  uint8_t stg[PT_STG];             // the tile's packed superkmers before they are written out
+  alignas(16) uint8_t stg[PT_STG]; // the tile's packed superkmers before they are written out (read as uint4)
   uint8_t code_tab[256];           // byte -> 2-bit code or 255
   uint16_t brk[PT_NW + 1];         // local positions of breaks, ascending
   uint16_t skm[PT_T + 1];          // break index of each core superkmer start

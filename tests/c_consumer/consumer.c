@@ -25,7 +25,13 @@ int main(int argc, char **argv) {
 
   char *reads = NULL;
   uint64_t *offs = NULL, n_reads = 0;
-  CHECK(gkc_fastx_load(argv[1], 2, 0, &reads, &offs, &n_reads) == GKC_OK, "fastx load");
+  /* the reference's rule: the line after each header */
+  CHECK(gkc_fastx_load(argv[1], 2, 0, &reads, &offs, &n_reads) == GKC_OK && n_reads == 2 && offs[2] == 16 &&
+            memcmp(reads, "ACGTACGTGGGGCCCC", 16) == 0,
+        "fastx load");
+  gkc_fastx_free(reads, offs, 0);
+  /* the lines of a record joined */
+  CHECK(gkc_fastx_load_ex(argv[1], 2, 0, GKC_FASTX_JOIN_LINES, &reads, &offs, &n_reads) == GKC_OK, "fastx joined");
   CHECK(n_reads == 2 && offs[0] == 0 && offs[1] == 8 && offs[2] == 20, "fastx offsets");
   CHECK(memcmp(reads, "ACGTACGTGGGGCCCCAAAA", 20) == 0, "fastx bytes");
   gkc_fastx_free(reads, offs, 0);

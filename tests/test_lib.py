@@ -109,7 +109,7 @@ def test_c_consumer_of_the_header(tmp_path):
             np.array([2, 9, 300], np.uint32), 1, 1000)
     r = subprocess.run([str(exe), str(fa), str(tmp_path / "db")], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.count("ok ") == 11
+    assert r.stdout.count("ok ") == 12
 
 
 def test_cpp_nccl_sharding_example_compiles(tmp_path):
