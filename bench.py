@@ -267,6 +267,70 @@ def reference_parity(ctx, G, prm, reads, offs, wl, threads):
             "compared": "per-bin sorted (k-mer, count) lists of the CPU-baseline sample"}
 
 
+def time_minimizer_emit(ctx, G, torch, stream, reads, offs, n_reads, n_bases, wl, reps=3):
+    """HPC (gkc_hpc_device) then every window's minimizer, position and
+    strand (gkc_minimizers_device) over the compressed reads; bytes moved at
+    least: the reads and offsets in, the compressed reads, their offsets and
+    original positions out and back in, 6 bytes per window out."""
+    d_h = torch.empty(n_bases + 64, dtype=torch.uint8, device="cuda")
+    d_ho = torch.empty(n_reads + 1, dtype=torch.int64, device="cuda")
+    d_orig = torch.empty(n_bases + 16, dtype=torch.int32, device="cuda")
+    d_mm = torch.empty(n_bases + 16, dtype=torch.int32, device="cuda")
+    d_pos = torch.empty(n_bases + 16, dtype=torch.uint8, device="cuda")
+    d_str = torch.empty(n_bases + 16, dtype=torch.int8, device="cuda")
+    prm = G.params(wl["k"], wl["p"], wl["nbins"], False)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    t_hpc, t_mm = [], []
+    for r in range(reps + 1):
+        ev[0].record(stream)
+        ctx.hpc_device(reads, n_bases, offs, n_reads, d_h, d_ho, d_orig)
+        ev[1].record(stream)
+        nb = int(d_ho[n_reads].item())
+        ctx.minimizers_device(d_h, nb, d_ho, n_reads, prm, d_mm, d_pos, d_str)
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+        if r:
+            t_hpc.append(ev[0].elapsed_time(ev[1]))
+            t_mm.append(ev[1].elapsed_time(ev[2]))
+    peak, kind = peaks()
+    hpc_ms, mm_ms = float(np.median(t_hpc)), float(np.median(t_mm))
+    b_hpc = n_bases + 8 * (n_reads + 1) + nb + 8 * (n_reads + 1) + 4 * nb
+    b_mm = nb + 8 * (n_reads + 1) + 6 * nb
+    return {"windows": nb, "hpc_ms": hpc_ms, "minimizer_ms": mm_ms,
+            "windows_per_s": nb / ((hpc_ms + mm_ms) / 1000.0),
+            "roofline": {"bound": "hbm", "kernel": "k_window_minimizers", "achieved": b_mm / (mm_ms / 1000.0) / 1e9,
+                         "peak": peak, "peak_kind": kind, "unit": "GB/s",
+                         "frac": b_mm / (mm_ms / 1000.0) / 1e9 / peak,
+                         "model": "reads + offsets in, 4 + 1 + 1 bytes per window out"},
+            "hpc_gbs": b_hpc / (hpc_ms / 1000.0) / 1e9}
+
+
+def time_subsample(ctx, G, torch, stream, reads, offs, n_reads, n_bases, wl, reps=3, mod=4):
+    """k-mers whose window minimizer % 4 == 0 with their position lists
+    (gkc_subsample_positions_device)."""
+    prm = G.params(wl["k"], wl["p"], wl["nbins"], False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ts = []
+    for r in range(reps + 1):
+        e0.record(stream)
+        v = ctx.subsample_positions_device(reads, n_bases, offs, n_reads, prm, mod)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if r:
+            ts.append(e0.elapsed_time(e1))
+    ms = float(np.median(ts))
+    n_pos, nd = int(v.n_positions), int(v.n_distinct)
+    w = 16
+    P = math.ceil(2 * wl["k"] / 8)
+    # model: reads in, selected (key, position) pairs sorted by LSD radix passes, keys + offsets + positions out
+    model = n_bases + 8 * (n_reads + 1) + (w + 4) * n_pos * (1 + 2 * P) + w * nd + 8 * (nd + 1) + 4 * n_pos
+    peak, kind = peaks()
+    return {"positions": n_pos, "distinct": nd, "ms": ms, "positions_per_s": n_pos / (ms / 1000.0),
+            "roofline": {"bound": "hbm", "achieved": model / (ms / 1000.0) / 1e9, "peak": peak, "peak_kind": kind,
+                         "unit": "GB/s", "frac": model / (ms / 1000.0) / 1e9 / peak,
+                         "model": "reads in; (key, position) pairs through 2k/8 LSD passes; lists out"}}
+
+
 # ------------------------------------------------------------ reference arm
 
 def run_reference(args, wl):
@@ -308,25 +372,56 @@ def run_reference(args, wl):
     }))
 
 
-def serve_mix(G, device, n_jobs, loads, seed, max_running=4, lo=1e5, hi=1e9, calib_jobs=40):
+def host_read_pool(G, seed, n_bases):
+    """Config-2 short reads (150 bp, 30x of a genome) made on the host, for
+    the serving mix's host-read jobs: a job of b bases takes the first b // 150
+    reads."""
+    L = G.lib()
+    n = n_bases // 150
+    glen = max(n * 150 // 30, 1 << 16)
+    genome = np.zeros(glen, np.uint8)
+    assert L.gkc_synth_genome(0, seed, glen, 0.05, 0.01, genome.ctypes.data) == 0
+    reads = np.zeros(n * 150 + 64, np.uint8)
+    offs = np.zeros(n + 1, np.uint64)
+    assert L.gkc_synth_short_reads(0, seed, genome.ctypes.data, glen, 0, n, 150, 0.005, reads.ctypes.data,
+                                   offs.ctypes.data) == 0
+    return reads, offs
+
+
+def serve_mix(G, device, n_jobs, loads, seed, max_running=4, lo=1e5, hi=1e9, calib_jobs=40, host_frac=0.25,
+              host_pool_bases=200_000_000):
     """The serving mix: jobs of log-uniform size in [lo, hi] bases, each from
     the config-2 (short reads of a genome, 30x) or config-3 (long reads, 20x,
     HPC) generator at random, k in {25, 31}, Poisson arrivals at each load
     (a fraction of the capacity measured by a burst of calib_jobs jobs).
-    Latency = job end - submission, on the server's clock; reads are
-    generated on the device when a job starts, inside its latency."""
+    Latency = job end - submission, on the server's clock.  A host_frac share
+    of the config-2 jobs hands the server reads in host memory (taken from a
+    pool made on the host, at most host_pool_bases bases), so their latency
+    includes the upload; the others' reads are generated on the device when
+    the job starts, inside its latency."""
     import threading
     rng = np.random.default_rng(seed)
+    pool_reads, pool_offs = host_read_pool(G, seed + 17, host_pool_bases)
 
     def draw(n):
         sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), n)).astype(np.int64)
-        return list(zip(sizes.tolist(), rng.choice([2, 3], n).tolist(), rng.choice([25, 31], n).tolist()))
+        gens = rng.choice([2, 3], n)
+        gens = np.where((gens == 2) & (rng.random(n) < host_frac), 0, gens)  # 0: host reads (config-2 shape)
+        return list(zip(sizes.tolist(), gens.tolist(), rng.choice([25, 31], n).tolist()))
+
+    def submit(srv, sz, g, k, job_seed):
+        if g == 0:
+            nr = max(1, min(int(sz) // 150, len(pool_offs) - 1))
+            return srv.submit(pool_reads[:int(pool_offs[nr])], pool_offs[:nr + 1], prm_for(2, k))
+        return srv.submit_synth(prm_for(g, k), g, job_seed, sz)
 
     def prm_for(gen, k):
         return G.params(k, 15, 256, True) if gen == 3 else G.params(k, 11, 256)
 
     out = {"generators": "config-2 short reads 30x (p=11) / config-3 long reads 20x HPC (p=15)",
-           "sizes_bases": [lo, hi], "k": [25, 31], "slots": max_running}
+           "sizes_bases": [lo, hi], "k": [25, 31], "slots": max_running,
+           "host_read_jobs": f"{host_frac:.0%} of the config-2 jobs, reads in host memory "
+                             f"(at most {host_pool_bases:.0e} bases), upload inside the latency"}
     with G.Server(device, max_running=max_running) as srv:
         def collect(ids, infos):
             for j in ids:
@@ -335,7 +430,7 @@ def serve_mix(G, device, n_jobs, loads, seed, max_running=4, lo=1e5, hi=1e9, cal
 
         cal = draw(calib_jobs)
         t0 = time.perf_counter()
-        ids = [srv.submit_synth(prm_for(g, k), g, seed * 7919 + i, sz) for i, (sz, g, k) in enumerate(cal)]
+        ids = [submit(srv, sz, g, k, seed * 7919 + i) for i, (sz, g, k) in enumerate(cal)]
         infos = []
         collect(ids, infos)
         wall = time.perf_counter() - t0
@@ -373,7 +468,7 @@ def serve_mix(G, device, n_jobs, loads, seed, max_running=4, lo=1e5, hi=1e9, cal
                 dt = start + t - time.perf_counter()
                 if dt > 0:
                     time.sleep(dt)
-                jid = srv.submit_synth(prm_for(g, k), g, seed * 100003 + li * 10007 + i, sz)
+                jid = submit(srv, sz, g, k, seed * 100003 + li * 10007 + i)
                 with lock:
                     ids.append(jid)
             done.set()
@@ -609,6 +704,14 @@ def run_ours(args, wl):
         if wide:
             assert G.lib().gkc_ctx_release_workspace(ctx.h) == 0
         step()
+
+    # the workload's application outputs, each timed on its own: config 3's
+    # per-window (minimizer, position, strand) emit after HPC, config 4's
+    # sub-sampled k-mers with position lists (minimizer % 4 == 0)
+    if rank == 0 and wl["gen"] == "long":
+        result["minimizer_emit"] = time_minimizer_emit(ctx, G, torch, stream, reads, offs, n_reads, n_bases, wl)
+    if rank == 0 and wl["k"] > 32:
+        result["subsample_positions"] = time_subsample(ctx, G, torch, stream, reads, offs, n_reads, n_bases, wl)
 
     # the CPU baseline's reads: the workload's first reads, copied from the
     # device (at most 10 M reads, enough for about 10 s of reference CPU work)
