@@ -129,8 +129,8 @@ template <typename K>
 static gkc_status db_write_t(gkc_ctx *c, const char *path, uint32_t min_count, uint32_t max_count, int lut_len,
                              uint64_t n) {
   const int k = c->ck;
-  const K *keys = (const K *)c->bufs["out_keys"].p;
-  const uint32_t *counts = (const uint32_t *)c->bufs["out_counts"].p;
+  const K *keys = (const K *)c->bufs["flt_keys"].p;
+  const uint32_t *counts = (const uint32_t *)c->bufs["flt_counts"].p;
   const unsigned grid = c->n_sms * 16;
   // counter width: the smallest that holds the largest count
   WS(stats, unsigned long long, "db_stats", 2);

@@ -68,17 +68,17 @@ using namespace gkc;
   } while (0)
 
 // Keeps the entries of (keys, counts, bin_off) whose count is in [lo, hi];
-// returns the kept list in the "out_*" workspaces.
+// returns the kept list in the "flt_*" workspaces.
 template <typename K>
 static gkc_status keep_range(gkc_ctx *c, const K *keys, const uint32_t *counts, const uint64_t *bin_off,
                              uint32_t nbins, uint64_t n, uint32_t lo, uint32_t hi, uint64_t *n_out) {
   const unsigned grid = c->n_sms * 8;
-  WS(flags, unsigned long long, "out_flags", n + 1);
-  WS(pos, uint64_t, "out_pos", n + 2);
-  WS(stmp, uint64_t, "out_scan_tmp", scan_u64_tmp_words(n + 1) + 8);
-  WS(ok, K, "out_keys", n + 1);
-  WS(oc, uint32_t, "out_counts", n + 1);
-  WS(ob, uint64_t, "out_bin_off", nbins + 1);
+  WS(flags, unsigned long long, "flt_flags", n + 1);
+  WS(pos, uint64_t, "flt_pos", n + 2);
+  WS(stmp, uint64_t, "flt_scan_tmp", scan_u64_tmp_words(n + 1) + 8);
+  WS(ok, K, "flt_keys", n + 1);
+  WS(oc, uint32_t, "flt_counts", n + 1);
+  WS(ob, uint64_t, "flt_bin_off", nbins + 1);
   k_keep_flags<<<grid, 256, 0, c->st>>>(counts, n, lo, hi, flags);
   scan_u64(flags, pos, n, stmp, c->st);
   k_keep_copy<K><<<grid, 256, 0, c->st>>>(keys, counts, pos, n, lo, hi, ok, oc);
@@ -170,8 +170,8 @@ gkc_status gkc_count_output(gkc_ctx *c, uint32_t min_count, uint32_t max_count, 
   }
   *n_out = c->out_n;
   const uint64_t n = c->out_n;
-  if (bin_off) CK(cudaMemcpy(bin_off, c->bufs["out_bin_off"].p, 8 * (c->out_nbins + 1), cudaMemcpyDeviceToHost));
-  if (keys && n) CK(cudaMemcpy(keys, c->bufs["out_keys"].p, 8 * kw * n, cudaMemcpyDeviceToHost));
-  if (counts && n) CK(cudaMemcpy(counts, c->bufs["out_counts"].p, 4 * n, cudaMemcpyDeviceToHost));
+  if (bin_off) CK(cudaMemcpy(bin_off, c->bufs["flt_bin_off"].p, 8 * (c->out_nbins + 1), cudaMemcpyDeviceToHost));
+  if (keys && n) CK(cudaMemcpy(keys, c->bufs["flt_keys"].p, 8 * kw * n, cudaMemcpyDeviceToHost));
+  if (counts && n) CK(cudaMemcpy(counts, c->bufs["flt_counts"].p, 4 * n, cudaMemcpyDeviceToHost));
   return GKC_OK;
 }
