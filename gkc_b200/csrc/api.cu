@@ -231,9 +231,7 @@ gkc_status gkc_ctx_create(int device_id, uint64_t hbm_budget_bytes, gkc_ctx **ou
   if (set_dyn_smem_limit((const void *)k_partition, c->max_smem_optin) != cudaSuccess ||
       set_dyn_smem_limit((const void *)k_bin_place, c->max_smem_optin) != cudaSuccess ||
       set_dyn_smem_limit((const void *)k_bucket_count<uint64_t>, c->max_smem_optin) != cudaSuccess ||
-      set_dyn_smem_limit((const void *)k_bucket_count<u128>, c->max_smem_optin) != cudaSuccess ||
-      set_dyn_smem_limit((const void *)k_bucket_scatter<uint64_t>, c->max_smem_optin) != cudaSuccess ||
-      set_dyn_smem_limit((const void *)k_bucket_scatter<u128>, c->max_smem_optin) != cudaSuccess) {
+      set_dyn_smem_limit((const void *)k_bucket_count<u128>, c->max_smem_optin) != cudaSuccess) {
     cudaGetLastError();
     delete c;
     return GKC_ERR_CUDA;
@@ -383,9 +381,9 @@ uint64_t gkc_job_hbm_estimate(const gkc_params *prm, uint64_t n_bases, uint64_t 
   while (max_bits > 0 && ((uint64_t)prm->nbins << max_bits) > (1ull << 20)) max_bits--;
   const uint64_t chunks = kc / 32768 + prm->nbins + 1;  // the smallest chunk the tuner picks
   e += 4 * (chunks << max_bits) + 8 * chunks;                            // chunk matrix, first superkmers
-  e += w * kc * 2 + 4 * kc;                                              // keys, output keys, counts
+  e += w * kc * 2 + 4 * kc * 2;                                          // keys, output keys, staged and output counts
   e += w * std::max<uint64_t>(kc / 16, 1 << 16);                         // oversized-bucket scratch
-  e += ((uint64_t)prm->nbins << max_bits) * 8 * 3;                       // bucket starts, sizes, look-back
+  e += ((uint64_t)prm->nbins << max_bits) * 8 * 5;                       // bucket starts, sizes, distinct counts, offsets, scan
   return e + (64ull << 20);
 }
 
@@ -678,21 +676,20 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   k_bucket_scan<<<std::min<uint32_t>(nbins, 65535), kBucketScanThreads, 0, c->st>>>(ea, bstart, bsize);
   LAUNCHED(c);
   stage_mark(c, 4);
-  const size_t sct_smem = bucket_scatter_smem_bytes<K>();
-  if ((int)sct_smem > c->max_smem_optin) return ctx_fail(c, GKC_ERR_INTERNAL, "scatter stage exceeds shared memory");
-  k_bucket_scatter<K><<<c->n_sms * 2, kBucketScatterThreads, sct_smem, c->st>>>(ea);
+  k_bucket_scatter<K><<<c->n_sms * 6, kBucketScatterThreads, 0, c->st>>>(ea);
   LAUNCHED(c);
 
-  // counting: one look-back word per bucket; oversized buckets go through the scratch area
-  WS(out_keys, K, slot_name(c, "out_keys").c_str(), keys_cap);
-  WS(out_counts, uint32_t, slot_name(c, "counts").c_str(), keys_cap);
-  WS(lookback, unsigned long long, "lookback", max_buckets + 1);
-  WS(ticket, unsigned long long, "lb_ticket", 4);
+  // counting: buckets independently, each bucket's runs staged over its own
+  // keys (counts beside them), then moved to the scan of the distinct counts;
+  // oversized buckets go through the scratch area
+  WS(stage_counts, uint32_t, "stage_counts", keys_cap);
+  WS(bucket_d, unsigned long long, "bucket_d", max_buckets + 1);
+  WS(bucket_out, uint64_t, "bucket_out", max_buckets + 2);
+  WS(dtmp, uint64_t, "scan_tmp3", scan_u64_tmp_words(max_buckets + 1) + 8);
+  WS(ticket, unsigned long long, "count_ticket", 4);
   scratch_keys = std::max<uint64_t>(scratch_keys, 1 << 16);
   WS(scratch, K, "sort_scratch", scratch_keys);
-  WS(bin_out, uint64_t, slot_name(c, "bin_out").c_str(), nbins + 1);
   CK(cudaMemsetAsync(ticket, 0, 32, c->st));
-  CK(cudaMemsetAsync(lookback, 0, (max_buckets + 1) * 8, c->st));
   SortCountArgs sa;
   memset(&sa, 0, sizeof(sa));
   sa.nbins = nbins;
@@ -705,11 +702,10 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   sa.scratch = scratch;
   sa.scratch_keys = scratch_keys;
   sa.scratch_cursor = ticket + 1;
-  sa.out_keys = out_keys;
-  sa.out_counts = out_counts;
-  sa.out_cap = keys_cap;
-  sa.bin_out = bin_out;
-  sa.lookback = lookback;
+  sa.stage_keys = keys;
+  sa.stage_counts = stage_counts;
+  sa.stage_cap = keys_cap;
+  sa.bucket_d = bucket_d;
   sa.ticket = ticket;
   sa.err = err;
   const size_t smem = bucket_count_smem_bytes<K>();
@@ -717,12 +713,20 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   int occ = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bucket_count<K>, kBucketCountThreads, smem));
   stage_mark(c, 5);
-  // persistent: every CTA resident at once (the look-back waits only on
-  // buckets taken earlier, by CTAs that are running)
+  // persistent, buckets taken by ticket
   const int ctas = std::max(1, std::min(occ, c->tune.count_ctas ? (int)c->tune.count_ctas : 2));
   k_bucket_count<K><<<c->n_sms * ctas, kBucketCountThreads, smem, c->st>>>(sa);
   LAUNCHED(c);
   stage_mark(c, 6);
+  // final offsets: the exclusive scan of the distinct counts (the bucket count is read on the device)
+  scan_u64_dev(bucket_d, bucket_out, max_buckets, bucket_base + nbins, dtmp, c->st);
+  c->launches += 4;
+  WS(out_keys, K, slot_name(c, "out_keys").c_str(), keys_cap);
+  WS(out_counts, uint32_t, slot_name(c, "counts").c_str(), keys_cap);
+  WS(bin_out, uint64_t, slot_name(c, "bin_out").c_str(), nbins + 1);
+  k_compact_runs<K><<<c->n_sms * 8, 256, 0, c->st>>>(keys, stage_counts, bstart, bucket_d, bucket_out, bucket_base,
+                                                      nbins, out_keys, out_counts, bin_out, err);
+  LAUNCHED(c);
   c->count_keys_cap = keys_cap;
   return GKC_OK;
 }

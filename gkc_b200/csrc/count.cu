@@ -16,15 +16,16 @@
 //   2. k_bucket_scan    - one CTA per bin turns the (chunk, digit) counts
 //                         into each chunk's write offset per digit and each
 //                         bucket's start and size;
-//   3. k_bucket_scatter - expands every k-mer once; each round of a chunk is
-//                         grouped by digit in shared memory and leaves as
-//                         runs of consecutive keys at the chunk's offsets;
+//   3. k_bucket_scatter - expands every k-mer once and writes it at its
+//                         chunk's offset for its digit plus its rank there
+//                         (a shared-memory atomic);
 //   4. k_bucket_count   - persistent, one bucket per ticket: counting sort by
 //                         sub-bucket in shared memory, each thread sorting and
 //                         run-length encoding a few sub-buckets, a block scan,
-//                         and the bucket's output offset by decoupled
-//                         look-back over the buckets before it, so the runs
-//                         are written once, to their final place.  A bucket
+//                         the runs staged at the bucket's own key range and
+//                         its distinct count recorded (buckets are counted
+//                         independently of one another); k_compact_runs then
+//                         moves them to the scan of the counts.  A bucket
 //                         larger than shared memory is placed by sub-bucket in
 //                         a scratch area and counted in slices; a single
 //                         sub-bucket too large for a slice is aggregated in a
@@ -130,59 +131,31 @@ __global__ void k_chunk_first(ExpandArgs a) {
   }
 }
 
-// -------------------------------------------------------- superkmer rounds
+// ------------------------------------------------------- k-mer runs
 
-// The superkmers of one round of a chunk, staged in shared memory: k-mer
-// starts relative to the round's first k-mer (clamped above) and packed byte
-// offsets.  At most MAXS superkmers: a round ends early where they run out.
-template <int MAXS>
-struct SkmRound {
-  int32_t koff[MAXS + 1];
-  uint64_t off[MAXS];
-  uint32_t ns, m;    // staged superkmers; k-mers in the round
-  uint64_t s_first;  // first staged superkmer (global index)
-  uint64_t s_next;   // first superkmer of the next round
-};
-
-// Stages the round that starts at k-mer r0 inside superkmer s_first and
-// sets R.m (<= rmax).  All threads call; ends with a barrier.
-template <int NT, int MAXS>
-GKC_DEV void stage_round(SkmRound<MAXS> &R, const ExpandArgs &a, uint64_t s_first, uint64_t s_hi,
-                         uint64_t r0, uint64_t q1, uint32_t rmax) {
-  const uint32_t ns = (uint32_t)min((uint64_t)(s_hi - s_first), (uint64_t)MAXS);
-  for (uint32_t i = threadIdx.x; i <= ns; i += NT) {
-    const int64_t d = (int64_t)a.koff[s_first + i] - (int64_t)r0;
-    R.koff[i] = (int32_t)min((int64_t)d, (int64_t)rmax + 1);
-    if (i < ns) R.off[i] = a.desc[s_first + i] >> 24;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    R.ns = ns;
-    R.s_first = s_first;
-    int64_t m = min((int64_t)(q1 - r0), (int64_t)rmax);
-    m = min((int64_t)m, (int64_t)R.koff[ns]);
-    R.m = (uint32_t)max(m, (int64_t)0);
-  }
-  __syncthreads();
-}
-
-// Staged superkmer holding local k-mer q: the last with koff <= q.
-template <int MAXS>
-GKC_DEV uint32_t round_find(const SkmRound<MAXS> &R, int32_t q) {
-  uint32_t lo = 0, hi = R.ns - 1;
+// The superkmer of the bin holding k-mer q: the last one in [lo, hi] whose
+// k-mer prefix is at most q.
+GKC_DEV uint64_t skm_of_kmer(const uint64_t *koff, uint64_t lo, uint64_t hi, uint64_t q) {
   while (lo < hi) {
-    const uint32_t mid = (lo + hi + 1) >> 1;
-    if (R.koff[mid] <= q) lo = mid; else hi = mid - 1;
+    const uint64_t mid = (lo + hi + 1) >> 1;
+    if (__ldg(koff + mid) <= q) lo = mid; else hi = mid - 1;
   }
   return lo;
 }
 
-// Thread 0, after a round: the next round's first superkmer (the last staged
-// one starting at or before the round's end; past all staged ones when the
-// round held no k-mers, as they all were empty).
-template <int MAXS>
-GKC_DEV void round_advance(SkmRound<MAXS> &R) {
-  R.s_next = R.m == 0 ? R.s_first + R.ns : R.s_first + round_find<MAXS>(R, (int32_t)R.m);
+// Thread tid's k-mers of chunk c: a contiguous run [*q, *qe) of about
+// chunk_kmers / nt k-mers, and the superkmer holding its first k-mer
+// (searched between the chunk's first superkmer and the next chunk's).
+GKC_DEV uint64_t thread_run(const ExpandArgs &a, uint64_t c, uint32_t b, uint64_t j, int nt, uint64_t *q,
+                            uint64_t *qe) {
+  const uint64_t q0 = a.bin_kstart[b] + j * a.chunk_kmers;
+  const uint64_t q1 = min(q0 + a.chunk_kmers, a.bin_kstart[b + 1]);
+  const uint64_t per = (q1 - q0 + nt - 1) / nt;
+  *q = min(q0 + per * threadIdx.x, q1);
+  *qe = min(*q + per, q1);
+  const uint64_t lo = a.chunk_s0[c];
+  const uint64_t hi = (c + 1 < a.chunk_base[b + 1]) ? a.chunk_s0[c + 1] : a.bin_start[b + 1] - 1;
+  return skm_of_kmer(a.koff, lo, hi, *q);
 }
 
 // 16 bases of a packed superkmer from base index pos, first base in the top
@@ -248,17 +221,18 @@ struct BaseStream {
 // ----------------------------------------------------------- 1. histogram
 
 constexpr int HS_NT = 256;
-constexpr int HS_PER = 16;
-constexpr int HS_R = HS_NT * HS_PER;  // k-mers per round
-constexpr int HS_MAXS = 1024;
 
+// Per chunk of a bin's k-mers, the histogram of coarse digits.  Each thread
+// walks a contiguous run of about chunk_kmers / 256 k-mers through its
+// superkmers; the digit needs only the top 32 bits of the canonical key,
+// min(first 16 bases, reverse complement of the last 16), from two 32-bit
+// rolling windows (h = min(k, 16) bases each).
 __global__ void __launch_bounds__(HS_NT) k_bucket_hist(ExpandArgs a) {
-  __shared__ SkmRound<HS_MAXS> R;
   __shared__ uint32_t hist[1 << kCoarseMaxBits];
   if (*a.err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
   const uint64_t n_chunks = a.chunk_base[a.nbins];
   const int k = a.k;
-  const int h = k < 16 ? k : 16;  // bases in each 32-bit window
+  const int h = k < 16 ? k : 16;
   const uint32_t hmask = h == 16 ? 0xFFFFFFFFu : ((1u << (2 * h)) - 1u);
   const int hsh = 32 - 2 * h;
   for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
@@ -266,52 +240,35 @@ __global__ void __launch_bounds__(HS_NT) k_bucket_hist(ExpandArgs a) {
     const uint64_t j = c - a.chunk_base[b];
     const int cb = (int)a.bin_bits[b];
     const uint32_t nd = 1u << cb;
-    const uint64_t q0 = a.bin_kstart[b] + j * a.chunk_kmers;
-    const uint64_t q1 = min(q0 + a.chunk_kmers, a.bin_kstart[b + 1]);
-    const uint64_t s_hi = a.bin_start[b + 1];
     for (uint32_t d = threadIdx.x; d < nd; d += HS_NT) hist[d] = 0;
-    uint64_t s_first = a.chunk_s0[c], r0 = q0;
-    while (r0 < q1) {
-      stage_round<HS_NT, HS_MAXS>(R, a, s_first, s_hi, r0, q1, HS_R);
-      if (R.ns == 0) {  // k-mers left but no superkmer: inconsistent offsets
-        if (threadIdx.x == 0) atomicOr(a.err, ERR_BOUNDS);
-        break;
+    __syncthreads();
+    uint64_t q, qe;
+    uint64_t s = thread_run(a, c, b, j, HS_NT, &q, &qe);
+    while (q < qe) {
+      const uint64_t ks = __ldg(a.koff + s), ke = __ldg(a.koff + s + 1);
+      if (ke <= q) {  // a superkmer without k-mers, or one already passed
+        s++;
+        continue;
       }
-      const uint32_t m = R.m;
-      const uint32_t q = threadIdx.x * HS_PER;
-      if (q < m) {
-        const uint32_t qe = min(q + HS_PER, m);
-        uint32_t si = round_find<HS_MAXS>(R, (int32_t)q);
-        uint32_t t = q;
-        while (t < qe) {
-          // k-mers [t, te) lie in superkmer si
-          const uint64_t off = R.off[si];
-          const uint32_t o = (uint32_t)((int32_t)t - R.koff[si]);
-          const uint32_t te = min(qe, (uint32_t)R.koff[si + 1]);
-          uint32_t fw = bases16(a.packed, off, o) >> hsh;
-          uint32_t rc = revcomp16(bases16(a.packed, off, o + k - h)) & hmask;
-          BaseStream sf, sr;
-          sf.init(a.packed + off, o + h);
-          sr.init(a.packed + off, o + k);
-          while (true) {
-            atomicAdd(&hist[coarse_of(eq_map(min(fw, rc) << hsh), cb)], 1u);
-            if (++t >= te) break;
-            fw = ((fw << 2) | sf.next()) & hmask;
-            rc = (rc >> 2) | ((3u - sr.next()) << (2 * h - 2));
-          }
-          si++;
-          while (si < R.ns && R.koff[si + 1] <= (int32_t)t) si++;  // superkmers without k-mers
-        }
+      const uint64_t off = __ldg(a.desc + s) >> 24;
+      const uint32_t o = (uint32_t)(q - ks);
+      uint32_t cnt = (uint32_t)(min(qe, ke) - q);
+      uint32_t fw = bases16(a.packed, off, o) >> hsh;
+      uint32_t rc = revcomp16(bases16(a.packed, off, o + k - h)) & hmask;
+      BaseStream sf, sr;
+      sf.init(a.packed + off, o + h);
+      sr.init(a.packed + off, o + k);
+      q += cnt;
+      s++;
+      while (true) {
+        atomicAdd(&hist[coarse_of(eq_map(min(fw, rc) << hsh), cb)], 1u);
+        if (--cnt == 0) break;
+        fw = ((fw << 2) | sf.next()) & hmask;
+        rc = (rc >> 2) | ((3u - sr.next()) << (2 * h - 2));
       }
-      __syncthreads();
-      if (threadIdx.x == 0) round_advance<HS_MAXS>(R);
-      __syncthreads();
-      s_first = R.s_next;
-      r0 += m;
     }
     __syncthreads();
-    // the chunk's row, digits contiguous
-    uint32_t *row = a.hist + a.hist_base[b] + j * nd;
+    uint32_t *row = a.hist + a.hist_base[b] + j * nd;  // the chunk's row, digits contiguous
     for (uint32_t d = threadIdx.x; d < nd; d += HS_NT) row[d] = hist[d];
     __syncthreads();
   }
@@ -382,145 +339,65 @@ __global__ void __launch_bounds__(BS_NT) k_bucket_scan(ExpandArgs a, uint64_t *b
 
 // -------------------------------------------------------------- 3. scatter
 
-template <typename K> struct ScatterShape;
-template <> struct ScatterShape<uint64_t> { static constexpr int NT = 512, PER = 8, MAXS = 1024; };
-template <> struct ScatterShape<u128> { static constexpr int NT = 512, PER = 4, MAXS = 512; };
+constexpr int SC_THREADS = 256;
 
+// Expands every k-mer once and writes it to its bucket: the chunk's write
+// offset per digit (from the scan) plus the key's rank among the chunk's keys
+// of that digit, taken with a shared-memory atomic.  Threads walk contiguous
+// runs as in the histogram; the first k-mer of each superkmer segment is
+// extracted whole, the rest rolled in (kmer_counting.cu:99-112, canonical
+// form :33-44).
 template <typename K>
-struct ScatterSmem {
-  static constexpr int RR = ScatterShape<K>::NT * ScatterShape<K>::PER;  // k-mers per round
-  static constexpr int ND = 1 << kCoarseMaxBits;
-  K stage[RR];
-  K sorted[RR];
-  uint32_t cnt[ND / 2 + 1];  // two 16-bit counters per word (counts, then cursors)
-  uint16_t lstart[ND];       // digit starts inside the round
-  uint32_t gbase[ND];        // next write position per digit, from the bin's first key
-  uint32_t tmp[64];
-  SkmRound<ScatterShape<K>::MAXS> R;
-};
-
-template <typename K> size_t bucket_scatter_smem_bytes() { return sizeof(ScatterSmem<K>); }
-template size_t bucket_scatter_smem_bytes<uint64_t>();
-template size_t bucket_scatter_smem_bytes<u128>();
-
-// 16-bit counters in pairs: returns the counter's value before the increment.
-GKC_DEV uint32_t cnt16_add(uint32_t *cnt, uint32_t d) {
-  const uint32_t sh = 16 * (d & 1u);
-  return (atomicAdd(&cnt[d >> 1], 1u << sh) >> sh) & 0xFFFFu;
-}
-GKC_DEV uint32_t cnt16_get(const uint32_t *cnt, uint32_t d) { return (cnt[d >> 1] >> (16 * (d & 1u))) & 0xFFFFu; }
-
-template <typename K>
-__global__ void __launch_bounds__(ScatterShape<K>::NT, 2) k_bucket_scatter(ExpandArgs a) {
-  constexpr int NT = ScatterShape<K>::NT, PER = ScatterShape<K>::PER, MAXS = ScatterShape<K>::MAXS;
-  constexpr int RR = ScatterSmem<K>::RR;
-  static_assert(RR < 65536, "16-bit counters");
-  extern __shared__ __align__(16) uint8_t sct_raw[];
-  ScatterSmem<K> &S = *reinterpret_cast<ScatterSmem<K> *>(sct_raw);
-  SkmRound<MAXS> &R = S.R;
+__global__ void __launch_bounds__(SC_THREADS) k_bucket_scatter(ExpandArgs a) {
+  __shared__ uint32_t cnt[1 << kCoarseMaxBits];
+  __shared__ uint32_t gbase[1 << kCoarseMaxBits];
   if (*a.err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
   K *keys = reinterpret_cast<K *>(a.keys);
   const uint64_t n_chunks = a.chunk_base[a.nbins];
   const int k = a.k, key_bits = 2 * k, top = 2 * k - 2;
   const K mask = kmer_mask<K>(k);
-  const int tid = threadIdx.x;
   for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
     const uint32_t b = find_bin(a.chunk_base, a.nbins, c);
     const uint64_t j = c - a.chunk_base[b];
     const int cb = (int)a.bin_bits[b];
     const uint32_t nd = 1u << cb;
     const uint64_t kbase = a.bin_kstart[b];
-    const uint64_t q0 = kbase + j * a.chunk_kmers;
-    const uint64_t q1 = min(q0 + a.chunk_kmers, a.bin_kstart[b + 1]);
-    const uint64_t s_hi = a.bin_start[b + 1];
     const uint32_t *row = a.hist + a.hist_base[b] + j * nd;
-    for (uint32_t d = tid; d < nd; d += NT) S.gbase[d] = row[d];
-    uint64_t s_first = a.chunk_s0[c], r0 = q0;
-    while (r0 < q1) {
-      for (uint32_t w = tid; w <= nd / 2; w += NT) S.cnt[w] = 0;
-      stage_round<NT, MAXS>(R, a, s_first, s_hi, r0, q1, RR);
-      if (R.ns == 0) {  // k-mers left but no superkmer: inconsistent offsets
-        if (tid == 0) atomicOr(a.err, ERR_BOUNDS);
-        break;
-      }
-      const uint32_t m = R.m;
-      // expand: thread-contiguous k-mers, staged at e * NT + tid
-      const uint32_t q = tid * PER;
-      if (q < m) {
-        const uint32_t qe = min(q + PER, m);
-        uint32_t si = round_find<MAXS>(R, (int32_t)q);
-        uint32_t t = q, e = 0;
-        while (t < qe) {
-          const uint64_t off = R.off[si];
-          const uint32_t o = (uint32_t)((int32_t)t - R.koff[si]);
-          const uint32_t te = min(qe, (uint32_t)R.koff[si + 1]);
-          K x = extract_kmer<K>(a.packed, off, o, k);
-          K r = revcomp_k<K>(x, k);
-          BaseStream bs;
-          bs.init(a.packed + off, o + k);
-          while (true) {
-            const K key = x < r ? x : r;  // canonicalkmer, kmer_counting.cu:33-44
-            S.stage[e * NT + tid] = key;
-            cnt16_add(S.cnt, coarse_digit<K>(key, key_bits, cb));
-            e++;
-            if (++t >= te) break;
-            const uint32_t cc = bs.next();
-            x = ((x << 2) | (K)cc) & mask;
-            r = (r >> 2) | ((K)(3u - cc) << top);
-          }
-          si++;
-          while (si < R.ns && R.koff[si + 1] <= (int32_t)t) si++;
-        }
-      }
-      __syncthreads();
-      // digit starts inside the round
-      {
-        constexpr int DPT = (1 << kCoarseMaxBits) / NT;
-        uint32_t v[DPT], s = 0;
-#pragma unroll
-        for (int u = 0; u < DPT; u++) {
-          const uint32_t d = tid * DPT + u;
-          v[u] = d < nd ? cnt16_get(S.cnt, d) : 0u;
-          s += v[u];
-        }
-        uint32_t total;
-        uint32_t run = block_exclusive_scan<NT>(s, S.tmp, &total);
-#pragma unroll
-        for (int u = 0; u < DPT; u++) {
-          const uint32_t d = tid * DPT + u;
-          if (d < nd) S.lstart[d] = (uint16_t)run;
-          run += v[u];
-        }
-        __syncthreads();
-        // the counters become cursors, starting at the digit starts
-        for (uint32_t w = tid; w < (nd + 1) / 2; w += NT) {
-          const uint32_t lo = S.lstart[2 * w], hi = 2 * w + 1 < nd ? S.lstart[2 * w + 1] : 0u;
-          S.cnt[w] = lo | (hi << 16);
-        }
-      }
-      __syncthreads();
-      // local k-mer i sits in slot (i % PER) * NT + i / PER
-      for (uint32_t i = tid; i < m; i += NT) {
-        const K x = S.stage[(i % PER) * NT + i / PER];
-        S.sorted[cnt16_add(S.cnt, coarse_digit<K>(x, key_bits, cb))] = x;
-      }
-      __syncthreads();
-      for (uint32_t i = tid; i < m; i += NT) {
-        const K x = S.sorted[i];
-        const uint32_t d = coarse_digit<K>(x, key_bits, cb);
-        const uint64_t slot = kbase + S.gbase[d] + (i - S.lstart[d]);
-        if (slot < a.keys_cap) keys[slot] = x;
-        else atomicOr(a.err, ERR_CAPACITY);
-      }
-      __syncthreads();
-      // the cursors now hold each digit's end inside the round
-      for (uint32_t d = tid; d < nd; d += NT) S.gbase[d] += cnt16_get(S.cnt, d) - S.lstart[d];
-      if (tid == 0) round_advance<MAXS>(R);
-      __syncthreads();
-      s_first = R.s_next;
-      r0 += m;
-      __syncthreads();
+    for (uint32_t d = threadIdx.x; d < nd; d += SC_THREADS) {
+      gbase[d] = row[d];
+      cnt[d] = 0;
     }
+    __syncthreads();
+    uint64_t q, qe;
+    uint64_t s = thread_run(a, c, b, j, SC_THREADS, &q, &qe);
+    while (q < qe) {
+      const uint64_t ks = __ldg(a.koff + s), ke = __ldg(a.koff + s + 1);
+      if (ke <= q) {
+        s++;
+        continue;
+      }
+      const uint64_t off = __ldg(a.desc + s) >> 24;
+      const uint32_t o = (uint32_t)(q - ks);
+      uint32_t n = (uint32_t)(min(qe, ke) - q);
+      K x = extract_kmer<K>(a.packed, off, o, k);
+      K r = revcomp_k<K>(x, k);
+      BaseStream bs;
+      bs.init(a.packed + off, o + k);
+      q += n;
+      s++;
+      while (true) {
+        const K key = x < r ? x : r;
+        const uint32_t d = coarse_digit<K>(key, key_bits, cb);
+        const uint64_t slot = kbase + gbase[d] + atomicAdd(&cnt[d], 1u);
+        if (slot < a.keys_cap) keys[slot] = key;
+        else atomicOr(a.err, ERR_CAPACITY);
+        if (--n == 0) break;
+        const uint32_t cc = bs.next();
+        x = ((x << 2) | (K)cc) & mask;
+        r = (r >> 2) | ((K)(3u - cc) << top);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -569,51 +446,6 @@ struct CountSmem {
 template <typename K> size_t bucket_count_smem_bytes() { return sizeof(CountSmem<K>); }
 template size_t bucket_count_smem_bytes<uint64_t>();
 template size_t bucket_count_smem_bytes<u128>();
-
-GKC_DEV uint64_t globaltimer_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Look-back words: (flag << 62) | value; flag 1: the bucket's distinct count,
-// flag 2: the inclusive prefix through the bucket.
-constexpr uint64_t LB_AGG = 1ull << 62, LB_INC = 2ull << 62, LB_VAL = (1ull << 62) - 1;
-
-GKC_DEV void lb_publish(unsigned long long *st, uint64_t g, uint64_t word) {
-  __threadfence();
-  atomicExch(st + g, (unsigned long long)word);
-}
-
-// Exclusive prefix of bucket g (one thread): walks back over the published
-// words until an inclusive prefix.  The wait is bounded (about 10 s); when it
-// runs out, ERR_SPIN_TIMEOUT is set and the sum so far returned.
-GKC_DEV uint64_t lb_exclusive(unsigned long long *st, uint64_t g, uint32_t *err) {
-  uint64_t excl = 0;
-  int64_t i = (int64_t)g - 1;
-  const uint64_t t0 = globaltimer_ns();
-  uint32_t it = 0;
-  while (i >= 0) {
-    const uint64_t w = *(volatile unsigned long long *)(st + i);
-    const uint64_t f = w & ~LB_VAL;
-    if (f == LB_INC) {
-      excl += w & LB_VAL;
-      break;
-    }
-    if (f == LB_AGG) {
-      excl += w & LB_VAL;
-      i--;
-      continue;
-    }
-    if (++it > (1u << 26) || globaltimer_ns() - t0 > 10000000000ull) {
-      atomicOr(err, ERR_SPIN_TIMEOUT);
-      break;
-    }
-    nanosleep_backoff(it);
-  }
-  __threadfence();
-  return excl;
-}
 
 // In-place ascending sort of A[0, m) by one warp (bitonic network whose
 // comparators put the smaller key first, so indices >= m act as +infinity).
@@ -772,11 +604,12 @@ GKC_DEV uint32_t slice_runs(CountSmem<K> &S, uint32_t m, uint32_t jb, uint32_t n
   return D;
 }
 
-// Writes the D runs of the slice (S.seg_* from slice_runs) at out[ob, ob+D),
-// coalesced: output i comes from the thread whose runs cover it.
+// Writes the D runs of the slice (S.seg_* from slice_runs) to the staging
+// arrays at [ob, ob+D), coalesced: output i comes from the thread whose runs
+// cover it.
 template <typename K, int NT>
 GKC_DEV void write_runs(CountSmem<K> &S, const SortCountArgs &a, uint32_t D, uint64_t ob) {
-  K *out_keys = reinterpret_cast<K *>(a.out_keys);
+  K *out_keys = reinterpret_cast<K *>(a.stage_keys);
   for (uint32_t i = threadIdx.x; i < D; i += NT) {
     uint32_t lo = 0, hi = NT - 1;
     while (lo < hi) {
@@ -784,9 +617,9 @@ GKC_DEV void write_runs(CountSmem<K> &S, const SortCountArgs &a, uint32_t D, uin
       if (S.seg_pos[mid] <= i) lo = mid; else hi = mid - 1;
     }
     const uint32_t src = S.seg_src[lo] + (i - S.seg_pos[lo]);
-    if (ob + i < a.out_cap) {
+    if (ob + i < a.stage_cap) {
       out_keys[ob + i] = S.u.A[src];
-      a.out_counts[ob + i] = S.C[src];
+      a.stage_counts[ob + i] = S.C[src];
     } else {
       atomicOr(a.err, ERR_CAPACITY);
     }
@@ -796,12 +629,12 @@ GKC_DEV void write_runs(CountSmem<K> &S, const SortCountArgs &a, uint32_t D, uin
 // One sub-bucket of n keys at tmp[0, n), too many for shared memory: key
 // ranges are aggregated in the hash table; a range whose distinct keys fill
 // more than 3/4 of it is halved and both halves retried (lower first).  Runs
-// are appended at out[S.out_base + S.run].
+// are appended to the staging arrays at S.out_base + S.run.
 template <typename K, int NT>
 GKC_DEV void heavy_slice(CountSmem<K> &S, const SortCountArgs &a, const K *src, uint64_t n) {
   constexpr int HN = HeavyTab<K>::N;
   HeavyTab<K> &T = S.u.h;
-  K *out_keys = reinterpret_cast<K *>(a.out_keys);
+  K *out_keys = reinterpret_cast<K *>(a.stage_keys);
   const int tid = threadIdx.x;
   if (tid == 0) {
     S.sp = 1;
@@ -908,9 +741,9 @@ GKC_DEV void heavy_slice(CountSmem<K> &S, const SortCountArgs &a, const K *src, 
     block_sort_pairs<K, NT>(T.key, T.cnt, nd);
     const uint64_t ob = S.out_base + S.run;
     for (uint32_t i = tid; i < nd; i += NT) {
-      if (ob + i < a.out_cap) {
+      if (ob + i < a.stage_cap) {
         out_keys[ob + i] = T.key[i];
-        a.out_counts[ob + i] = T.cnt[i];
+        a.stage_counts[ob + i] = T.cnt[i];
       } else {
         atomicOr(a.err, ERR_CAPACITY);
       }
@@ -980,16 +813,11 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
       }
       __syncthreads();
       const uint32_t D = slice_runs<K, NT>(S, m, 0, nsub, 0);
-      if (tid == 0) {
-        lb_publish(a.lookback, g, LB_AGG | D);
-        const uint64_t ex = lb_exclusive(a.lookback, g, a.err);
-        lb_publish(a.lookback, g, LB_INC | (ex + D));
-        S.out_base = ex;
-        if (a.bucket_base[b] == g) a.bin_out[b] = ex;
-        if (g + 1 == n_buckets) a.bin_out[a.nbins] = ex + D;
-      }
-      __syncthreads();
-      write_runs<K, NT>(S, a, D, S.out_base);
+      // the runs go to the staging arrays at the bucket's own key range
+      // (its keys are all in registers or shared memory by now); a later
+      // pass moves them to their final place
+      if (tid == 0) a.bucket_d[g] = D;
+      write_runs<K, NT>(S, a, D, start);
       __syncthreads();
       continue;
     }
@@ -1010,12 +838,7 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
     for (uint32_t jj = tid; jj < nsub; jj += NT) S.cnt[jj] = 0;
     __syncthreads();
     if (S.flag) {  // no room: an empty result (the host re-runs with a larger area)
-      if (tid == 0) {
-        const uint64_t ex = lb_exclusive(a.lookback, g, a.err);
-        lb_publish(a.lookback, g, LB_INC | ex);
-        if (a.bucket_base[b] == g) a.bin_out[b] = ex;
-        if (g + 1 == n_buckets) a.bin_out[a.nbins] = ex;
-      }
+      if (tid == 0) a.bucket_d[g] = 0;
       __syncthreads();
       continue;
     }
@@ -1034,8 +857,7 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
     __threadfence_block();
     __syncthreads();
     if (tid == 0) {
-      S.out_base = lb_exclusive(a.lookback, g, a.err);
-      if (a.bucket_base[b] == g) a.bin_out[b] = S.out_base;
+      S.out_base = start;  // staged at the bucket's own key range (all its keys are in the scratch area)
       S.run = 0;
     }
     __syncthreads();
@@ -1066,14 +888,40 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
       }
       jlo = jhi;
     }
-    if (tid == 0) {
-      lb_publish(a.lookback, g, LB_INC | (S.out_base + S.run));
-      if (g + 1 == n_buckets) a.bin_out[a.nbins] = S.out_base + S.run;
-    }
+    if (tid == 0) a.bucket_d[g] = S.run;
     __syncthreads();
   }
 }
 
+// Moves each bucket's staged runs to its final offset (the exclusive scan of
+// the buckets' distinct counts), one warp per bucket; bin_out[b] is the
+// offset of the bin's first bucket.
+template <typename K>
+__global__ void k_compact_runs(const K *stage_keys, const uint32_t *stage_counts, const uint64_t *bucket_start,
+                               const unsigned long long *bucket_d, const uint64_t *bucket_out,
+                               const uint64_t *bucket_base, uint32_t nbins, K *out_keys, uint32_t *out_counts,
+                               uint64_t *bin_out, const uint32_t *err) {
+  if (*err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
+  const uint64_t nb = bucket_base[nbins];
+  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t nt = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t b = t; b <= nbins; b += nt) bin_out[b] = bucket_out[bucket_base[b]];
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint64_t g = t >> 5; g < nb; g += nt >> 5) {
+    const uint64_t s = bucket_start[g], d = bucket_d[g], o = bucket_out[g];
+    for (uint64_t i = lane; i < d; i += 32) {
+      out_keys[o + i] = stage_keys[s + i];
+      out_counts[o + i] = stage_counts[s + i];
+    }
+  }
+}
+
+template __global__ void k_compact_runs<uint64_t>(const uint64_t *, const uint32_t *, const uint64_t *,
+                                                  const unsigned long long *, const uint64_t *, const uint64_t *,
+                                                  uint32_t, uint64_t *, uint32_t *, uint64_t *, const uint32_t *);
+template __global__ void k_compact_runs<u128>(const u128 *, const uint32_t *, const uint64_t *,
+                                              const unsigned long long *, const uint64_t *, const uint64_t *,
+                                              uint32_t, u128 *, uint32_t *, uint64_t *, const uint32_t *);
 template __global__ void k_bucket_scatter<uint64_t>(ExpandArgs);
 template __global__ void k_bucket_scatter<u128>(ExpandArgs);
 template __global__ void k_bucket_count<uint64_t>(SortCountArgs);

@@ -90,10 +90,9 @@ __global__ void k_chunk_first(ExpandArgs a);
 __global__ void k_bucket_hist(ExpandArgs a);
 __global__ void k_bucket_scan(ExpandArgs a, uint64_t *bucket_start, uint64_t *bucket_size);
 template <typename K> __global__ void k_bucket_scatter(ExpandArgs a);
-template <typename K> size_t bucket_scatter_smem_bytes();
 constexpr int kBucketScanThreads = 1024;
 constexpr int kBucketHistThreads = 256;
-constexpr int kBucketScatterThreads = 512;
+constexpr int kBucketScatterThreads = 256;
 __global__ void k_skm_nk(const uint64_t *desc, const unsigned long long *n_skm_dev, int k,
                          unsigned long long *nk);
 
@@ -108,16 +107,20 @@ struct SortCountArgs {
   void *scratch;                  // oversized buckets, placed by sub-bucket
   uint64_t scratch_keys;
   unsigned long long *scratch_cursor;  // zeroed
-  void *out_keys;                 // per-bin sorted distinct keys
-  uint32_t *out_counts;
-  uint64_t out_cap;
-  uint64_t *bin_out;              // nbins + 1 output offsets
-  unsigned long long *lookback;   // one word per bucket, zeroed
+  void *stage_keys;               // runs of bucket g at [bucket_start[g], + its distinct count)
+  uint32_t *stage_counts;
+  uint64_t stage_cap;
+  unsigned long long *bucket_d;   // distinct keys of each bucket
   unsigned long long *ticket;     // zeroed
   uint32_t *err;
 };
 template <typename K> __global__ void k_bucket_count(SortCountArgs a);
 template <typename K> size_t bucket_count_smem_bytes();
+template <typename K>
+__global__ void k_compact_runs(const K *stage_keys, const uint32_t *stage_counts, const uint64_t *bucket_start,
+                               const unsigned long long *bucket_d, const uint64_t *bucket_out,
+                               const uint64_t *bucket_base, uint32_t nbins, K *out_keys, uint32_t *out_counts,
+                               uint64_t *bin_out, const uint32_t *err);
 constexpr int kBucketCountThreads = 512;
 constexpr uint32_t kCoarseTarget = 4096;
 constexpr uint32_t kCoarseMaxBits = 12;
