@@ -44,8 +44,9 @@ WORKLOADS = {
                     hpc=0),
     "config4": dict(gen="genome", genome_len=100_000_000, coverage=30, read_len=250, err=0.005,
                     k=63, p=13, nbins=256, hpc=0),
-    # a small case of the config-2 generator (5x of a 10 Mbp genome, 50 M bases) for profiler captures
-    "small": dict(gen="genome", genome_len=10_000_000, coverage=5, read_len=150, err=0.005,
+    # a small case of the config-2 generator for profiler captures: 30x of a 3 Mbp genome (90 M bases,
+    # 72 M k-mers), the same copies per k-mer as the 30x workloads
+    "small": dict(gen="genome", genome_len=3_000_000, coverage=30, read_len=150, err=0.005,
                   k=31, p=11, nbins=256, hpc=0),
     # long reads: lognormal lengths (median 8 kbp, sigma 0.5, clipped to 1-50 kbp), 20x
     "config3": dict(gen="long", genome_len=100_000_000, coverage=20, median=8000.0, sigma=0.5,
@@ -512,7 +513,7 @@ def run_serve(args):
 def wl_name(args):
     return {"ns": "ns-100Mbp-30x-150bp-k31", "config2": "config2-10Mbp-30x-150bp-k31",
             "config1": "config1-iid-20000x150bp-k31", "config4": "config4-100Mbp-30x-250bp-k63",
-            "config3": "config3-100Mbp-20x-long-hpc-k25", "small": "small-10Mbp-5x-150bp-k31"}[args.workload]
+            "config3": "config3-100Mbp-20x-long-hpc-k25", "small": "small-3Mbp-30x-150bp-k31"}[args.workload]
 
 
 def scaled_sample(wl, n_cal, kmers_cal, rate, seconds):

@@ -231,7 +231,9 @@ gkc_status gkc_ctx_create(int device_id, uint64_t hbm_budget_bytes, gkc_ctx **ou
   if (set_dyn_smem_limit((const void *)k_partition, c->max_smem_optin) != cudaSuccess ||
       set_dyn_smem_limit((const void *)k_bin_place, c->max_smem_optin) != cudaSuccess ||
       set_dyn_smem_limit((const void *)k_bucket_count<uint64_t>, c->max_smem_optin) != cudaSuccess ||
-      set_dyn_smem_limit((const void *)k_bucket_count<u128>, c->max_smem_optin) != cudaSuccess) {
+      set_dyn_smem_limit((const void *)k_bucket_count<u128>, c->max_smem_optin) != cudaSuccess ||
+      set_dyn_smem_limit((const void *)k_bucket_scatter<uint64_t>, c->max_smem_optin) != cudaSuccess ||
+      set_dyn_smem_limit((const void *)k_bucket_scatter<u128>, c->max_smem_optin) != cudaSuccess) {
     cudaGetLastError();
     delete c;
     return GKC_ERR_CUDA;
@@ -648,6 +650,8 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   WS(chunk_s0, uint64_t, "chunk_s0", max_chunks);
   WS(hist, uint32_t, "bucket_hist", max_chunks << max_bits);
   WS(keys, K, "keys", keys_cap);
+  // the result's key array holds the k-mer-order keys until the count stage is done with them
+  WS(out_keys, K, slot_name(c, "out_keys").c_str(), keys_cap);
   WS(bstart, uint64_t, "bucket_start", max_buckets + 1);
   WS(bsize, uint64_t, "bucket_size", max_buckets + 1);
   ExpandArgs ea;
@@ -667,16 +671,20 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   ea.chunk_s0 = chunk_s0;
   ea.hist = hist;
   ea.keys = keys;
+  ea.flat = out_keys;
   ea.keys_cap = keys_cap;
   ea.err = err;
   k_chunk_first<<<(unsigned)std::min<uint64_t>((max_chunks + 255) / 256, 65535), 256, 0, c->st>>>(ea);
   LAUNCHED(c);
-  k_bucket_hist<<<c->n_sms * 8, kBucketHistThreads, 0, c->st>>>(ea);
+  k_bucket_hist<K><<<c->n_sms * 8, kBucketHistThreads, 0, c->st>>>(ea);
   LAUNCHED(c);
-  k_bucket_scan<<<std::min<uint32_t>(nbins, 65535), kBucketScanThreads, 0, c->st>>>(ea, bstart, bsize);
+  WS(bbin, uint32_t, "bucket_bin", max_buckets + 1);
+  k_bucket_scan<<<std::min<uint32_t>(nbins, 65535), kBucketScanThreads, 0, c->st>>>(ea, bstart, bsize, bbin);
   LAUNCHED(c);
   stage_mark(c, 4);
-  k_bucket_scatter<K><<<c->n_sms * 6, kBucketScatterThreads, 0, c->st>>>(ea);
+  const size_t sct_smem = bucket_scatter_smem_bytes<K>();
+  if ((int)sct_smem > c->max_smem_optin) return ctx_fail(c, GKC_ERR_INTERNAL, "scatter tile exceeds shared memory");
+  k_bucket_scatter<K><<<c->n_sms, kBucketScatterThreads, sct_smem, c->st>>>(ea);
   LAUNCHED(c);
 
   // counting: buckets independently, each bucket's runs staged over its own
@@ -698,6 +706,7 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   sa.bin_bits = bin_bits;
   sa.bucket_start = bstart;
   sa.bucket_size = bsize;
+  sa.bucket_bin = bbin;
   sa.keys = keys;
   sa.scratch = scratch;
   sa.scratch_keys = scratch_keys;
@@ -721,7 +730,6 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   // final offsets: the exclusive scan of the distinct counts (the bucket count is read on the device)
   scan_u64_dev(bucket_d, bucket_out, max_buckets, bucket_base + nbins, dtmp, c->st);
   c->launches += 4;
-  WS(out_keys, K, slot_name(c, "out_keys").c_str(), keys_cap);
   WS(out_counts, uint32_t, slot_name(c, "counts").c_str(), keys_cap);
   WS(bin_out, uint64_t, slot_name(c, "bin_out").c_str(), nbins + 1);
   k_compact_runs<K><<<c->n_sms * 8, 256, 0, c->st>>>(keys, stage_counts, bstart, bucket_d, bucket_out, bucket_base,

@@ -8,29 +8,31 @@
 // order-preserving map of the key (eq_map), so a bin's sorted list is the
 // concatenation of its buckets' sorted lists.  Device stages:
 //   1. k_bucket_hist    - per chunk of a bin's k-mers, a histogram of coarse
-//                         digits.  A canonical key's digit depends only on its
-//                         top 32 bits, which are min(top of x, top of
-//                         revcomp x): the first 16 bases and the reverse
-//                         complement of the last 16, two 32-bit rolling
-//                         windows (no 64-bit expansion);
+//                         digits.  Warps take 32 consecutive k-mers at a time,
+//                         one per lane: each lane finds its superkmer by a
+//                         search over the next 32 superkmers' k-mer ends and
+//                         extracts its k-mer from aligned 8-byte words;
 //   2. k_bucket_scan    - one CTA per bin turns the (chunk, digit) counts
 //                         into each chunk's write offset per digit and each
-//                         bucket's start and size;
-//   3. k_bucket_scatter - expands every k-mer once and writes it at its
-//                         chunk's offset for its digit plus its rank there
-//                         (a shared-memory atomic);
-//   4. k_bucket_count   - persistent, one bucket per ticket: counting sort by
-//                         sub-bucket in shared memory, each thread sorting and
-//                         run-length encoding a few sub-buckets, a block scan,
-//                         the runs staged at the bucket's own key range and
-//                         its distinct count recorded (buckets are counted
-//                         independently of one another); k_compact_runs then
-//                         moves them to the scan of the counts.  A bucket
-//                         larger than shared memory is placed by sub-bucket in
-//                         a scratch area and counted in slices; a single
-//                         sub-bucket too large for a slice is aggregated in a
-//                         shared-memory hash table over key ranges that are
-//                         halved until a range's distinct keys fit.
+//                         bucket's start, size and bin;
+//   3. k_bucket_scatter - expands every k-mer once the same way and writes
+//                         it at its chunk's offset for its digit plus its
+//                         rank there (a shared-memory atomic);
+//   4. k_bucket_count   - persistent, buckets taken by ticket, each counted
+//                         on its own: its keys aggregated in a shared-memory
+//                         hash table and the distinct (key, count) pairs
+//                         sorted by a bitonic network; a bucket with too many
+//                         distinct keys is counting-sorted by sub-bucket
+//                         instead, each sub-bucket reduced by its thread or a
+//                         warp.  The runs are staged at the bucket's own key
+//                         range and its distinct count recorded;
+//                         k_compact_runs then moves them to the scan of the
+//                         counts.  A bucket larger than shared memory is
+//                         placed by sub-bucket in a scratch area and counted
+//                         in slices; a single sub-bucket too large for a slice
+//                         is aggregated in a shared-memory hash table over key
+//                         ranges that are halved until a range's distinct keys
+//                         fit.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -143,36 +145,22 @@ GKC_DEV uint64_t skm_of_kmer(const uint64_t *koff, uint64_t lo, uint64_t hi, uin
   return lo;
 }
 
-// Thread tid's k-mers of chunk c: a contiguous run [*q, *qe) of about
-// chunk_kmers / nt k-mers, and the superkmer holding its first k-mer
-// (searched between the chunk's first superkmer and the next chunk's).
-GKC_DEV uint64_t thread_run(const ExpandArgs &a, uint64_t c, uint32_t b, uint64_t j, int nt, uint64_t *q,
-                            uint64_t *qe) {
-  const uint64_t q0 = a.bin_kstart[b] + j * a.chunk_kmers;
-  const uint64_t q1 = min(q0 + a.chunk_kmers, a.bin_kstart[b + 1]);
-  const uint64_t per = (q1 - q0 + nt - 1) / nt;
-  *q = min(q0 + per * threadIdx.x, q1);
-  *qe = min(*q + per, q1);
-  const uint64_t lo = a.chunk_s0[c];
-  const uint64_t hi = (c + 1 < a.chunk_base[b + 1]) ? a.chunk_s0[c + 1] : a.bin_start[b + 1] - 1;
-  return skm_of_kmer(a.koff, lo, hi, *q);
+// Packed bases are read as aligned 8-byte words, byte-swapped so that the
+// stream's first base is in the top bits (2 bits per base, MSB first within
+// a byte).  A word is loaded only when it holds a wanted base, so reads end
+// within 7 bytes past the last superkmer.
+GKC_DEV uint64_t be_word(const uint8_t *packed, uint64_t w) {
+  const uint64_t x = __ldg(reinterpret_cast<const unsigned long long *>(packed) + w);
+  return ((uint64_t)__byte_perm((uint32_t)x, 0, 0x0123) << 32) | __byte_perm((uint32_t)(x >> 32), 0, 0x0123);
 }
 
-// 16 bases of a packed superkmer from base index pos, first base in the top
-// bits (2 bits per base, MSB first; bytes past the end read as padding).
-GKC_DEV uint32_t bases16(const uint8_t *packed, uint64_t off, uint32_t pos) {
-  const uint8_t *p = packed + off + (pos >> 2);
-  const uint32_t sh = 2 * (pos & 3u);
-  uint32_t v = ((uint32_t)__ldg(p) << 24) | ((uint32_t)__ldg(p + 1) << 16) | ((uint32_t)__ldg(p + 2) << 8) |
-               (uint32_t)__ldg(p + 3);
-  if (sh) v = (v << sh) | ((uint32_t)__ldg(p + 4) >> (8 - sh));
+// nb <= 64 bits of the stream from bit position pos, left-aligned.
+GKC_DEV uint64_t stream_bits(const uint8_t *packed, uint64_t pos, int nb) {
+  const uint64_t w = pos >> 6;
+  const int r = (int)(pos & 63);
+  uint64_t v = be_word(packed, w) << r;
+  if (r + nb > 64) v |= be_word(packed, w + 1) >> (64 - r);
   return v;
-}
-
-// Reverse complement of the 16 bases of w.
-GKC_DEV uint32_t revcomp16(uint32_t w) {
-  const uint32_t y = __brev(~w);
-  return ((y >> 1) & 0x55555555u) | ((y & 0x55555555u) << 1);
 }
 
 // The 2k bits of bases [o, o+k) of a packed superkmer at byte `off`.
@@ -181,60 +169,93 @@ GKC_DEV K extract_kmer(const uint8_t *packed, uint64_t off, uint32_t o, int k);
 
 template <>
 GKC_DEV uint64_t extract_kmer<uint64_t>(const uint8_t *packed, uint64_t off, uint32_t o, int k) {
-  const uint8_t *p = packed + off + (o >> 2);
-  const int sh = 2 * (o & 3);
-  uint64_t hi = 0;
-#pragma unroll
-  for (int i = 0; i < 8; i++) hi = (hi << 8) | __ldg(p + i);
-  const uint64_t v = sh ? ((hi << sh) | (uint64_t)(__ldg(p + 8) >> (8 - sh))) : hi;
-  return v >> (64 - 2 * k);
+  return stream_bits(packed, 8 * off + 2 * (uint64_t)o, 2 * k) >> (64 - 2 * k);
 }
 
 template <>
 GKC_DEV u128 extract_kmer<u128>(const uint8_t *packed, uint64_t off, uint32_t o, int k) {
-  const uint8_t *p = packed + off + (o >> 2);
-  const int sh = 2 * (o & 3);
-  u128 hi = 0;
-#pragma unroll
-  for (int i = 0; i < 16; i++) hi = (hi << 8) | (u128)__ldg(p + i);
-  const u128 v = sh ? ((hi << sh) | (u128)(__ldg(p + 16) >> (8 - sh))) : hi;
-  return v >> (128 - 2 * k);
+  const uint64_t pos = 8 * off + 2 * (uint64_t)o;
+  const int nb = 2 * k;  // 66 .. 128
+  const uint64_t hi = stream_bits(packed, pos, 64);
+  const uint64_t lo = stream_bits(packed, pos + 64, nb - 64);
+  const u128 v = ((u128)hi << 64) | lo;
+  return v >> (128 - nb);
 }
 
-// Bases of a packed superkmer from index j on, each byte read once.
-struct BaseStream {
-  const uint8_t *p;
-  uint32_t j, byte;
-  GKC_DEV void init(const uint8_t *src, uint32_t j0) {
-    p = src;
-    j = j0;
-    byte = __ldg(p + (j >> 2));
+// The k-mers [qa, qb) of one bin, taken by the calling warp 32 at a time,
+// lane i the i-th of each group: each lane finds its superkmer among the 32
+// after the group's first one (a search over their k-mer ends, held one per
+// lane), extracts its k-mer and passes the canonical key to emit(key, valid)
+// (called by every lane; valid is false past qb).  s0 is the superkmer
+// holding k-mer qa, s_end the bin's end (k-mer offsets up to koff[s_end] are
+// read).
+template <typename K, typename Emit>
+GKC_DEV void warp_kmers(const ExpandArgs &a, uint64_t qa, uint64_t qb, uint64_t s0, uint64_t s_end, Emit &&emit) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const int k = a.k;
+  uint64_t base = s0;
+  for (uint64_t q0 = qa; q0 < qb; q0 += 32) {
+    const uint64_t q = q0 + lane;
+    const uint64_t jx = base + 1 + lane;
+    const uint64_t e = jx <= s_end ? __ldg(a.koff + jx) : ~0ull;  // end of superkmer base + lane
+    uint32_t cnt = 0;  // superkmers from `base` on that end at or before q
+#pragma unroll
+    for (uint32_t st = 16; st > 0; st >>= 1) {
+      const uint64_t v = __shfl_sync(0xffffffffu, e, cnt + st - 1);
+      if (v <= q) cnt += st;
+    }
+    const uint64_t prev = __shfl_sync(0xffffffffu, e, cnt == 0 ? 0 : cnt - 1);
+    const uint64_t e31 = __shfl_sync(0xffffffffu, e, 31);
+    const bool valid = q < qb;
+    uint64_t s = base + cnt;
+    uint64_t ks = cnt == 0 ? __ldg(a.koff + base) : prev;
+    if (valid && q >= e31) {  // 32 superkmers (some without k-mers) end before q
+      s = skm_of_kmer(a.koff, base + 32, s_end - 1, q);
+      ks = __ldg(a.koff + s);
+    }
+    K key = 0;
+    if (valid) {
+      const uint64_t off = __ldg(a.desc + s) >> 24;
+      const K x = extract_kmer<K>(a.packed, off, (uint32_t)(q - ks), k);
+      const K r = revcomp_k<K>(x, k);
+      key = x < r ? x : r;
+    }
+    emit(key, valid);
+    base = __shfl_sync(0xffffffffu, s, 31);  // every lane valid unless this was the last group
   }
-  GKC_DEV uint32_t next() {
-    if ((j & 3u) == 0) byte = __ldg(p + (j >> 2));
-    const uint32_t c = (byte >> (6 - 2 * (j & 3u))) & 3u;
-    j++;
-    return c;
-  }
-};
+}
+
+// The k-mers of chunk c (bin b, j-th chunk of the bin) taken by warp w of W:
+// [*qa, *qb) and the superkmer holding *qa.
+GKC_DEV uint64_t warp_run(const ExpandArgs &a, uint64_t c, uint32_t b, uint64_t j, int w, int W, uint64_t *qa,
+                          uint64_t *qb) {
+  const uint64_t q0 = a.bin_kstart[b] + j * a.chunk_kmers;
+  const uint64_t q1 = min(q0 + a.chunk_kmers, a.bin_kstart[b + 1]);
+  const uint64_t per = ((q1 - q0 + W - 1) / W + 31) & ~31ull;
+  *qa = min(q0 + per * w, q1);
+  *qb = min(*qa + per, q1);
+  const uint64_t lo = a.chunk_s0[c];
+  const uint64_t hi = (c + 1 < a.chunk_base[b + 1]) ? a.chunk_s0[c + 1] : a.bin_start[b + 1] - 1;
+  return skm_of_kmer(a.koff, lo, hi, *qa);
+}
 
 // ----------------------------------------------------------- 1. histogram
 
 constexpr int HS_NT = 256;
 
-// Per chunk of a bin's k-mers, the histogram of coarse digits.  Each thread
-// walks a contiguous run of about chunk_kmers / 256 k-mers through its
-// superkmers; the digit needs only the top 32 bits of the canonical key,
-// min(first 16 bases, reverse complement of the last 16), from two 32-bit
-// rolling windows (h = min(k, 16) bases each).
+// Expands every k-mer once (k-mer extraction and canonical form:
+// kmer_counting.cu:99-112, 33-44) into `flat`, in k-mer order, and counts
+// the coarse digits of each chunk of a bin's k-mers; each warp takes a
+// contiguous share of the chunk, 32 consecutive k-mers at a time, so the
+// writes are coalesced.
+template <typename K>
 __global__ void __launch_bounds__(HS_NT) k_bucket_hist(ExpandArgs a) {
   __shared__ uint32_t hist[1 << kCoarseMaxBits];
   if (*a.err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
+  K *flat = reinterpret_cast<K *>(a.flat);
   const uint64_t n_chunks = a.chunk_base[a.nbins];
-  const int k = a.k;
-  const int h = k < 16 ? k : 16;
-  const uint32_t hmask = h == 16 ? 0xFFFFFFFFu : ((1u << (2 * h)) - 1u);
-  const int hsh = 32 - 2 * h;
+  const int key_bits = 2 * a.k;
+  const int w = threadIdx.x >> 5;
   for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
     const uint32_t b = find_bin(a.chunk_base, a.nbins, c);
     const uint64_t j = c - a.chunk_base[b];
@@ -242,30 +263,19 @@ __global__ void __launch_bounds__(HS_NT) k_bucket_hist(ExpandArgs a) {
     const uint32_t nd = 1u << cb;
     for (uint32_t d = threadIdx.x; d < nd; d += HS_NT) hist[d] = 0;
     __syncthreads();
-    uint64_t q, qe;
-    uint64_t s = thread_run(a, c, b, j, HS_NT, &q, &qe);
-    while (q < qe) {
-      const uint64_t ks = __ldg(a.koff + s), ke = __ldg(a.koff + s + 1);
-      if (ke <= q) {  // a superkmer without k-mers, or one already passed
-        s++;
-        continue;
-      }
-      const uint64_t off = __ldg(a.desc + s) >> 24;
-      const uint32_t o = (uint32_t)(q - ks);
-      uint32_t cnt = (uint32_t)(min(qe, ke) - q);
-      uint32_t fw = bases16(a.packed, off, o) >> hsh;
-      uint32_t rc = revcomp16(bases16(a.packed, off, o + k - h)) & hmask;
-      BaseStream sf, sr;
-      sf.init(a.packed + off, o + h);
-      sr.init(a.packed + off, o + k);
-      q += cnt;
-      s++;
-      while (true) {
-        atomicAdd(&hist[coarse_of(eq_map(min(fw, rc) << hsh), cb)], 1u);
-        if (--cnt == 0) break;
-        fw = ((fw << 2) | sf.next()) & hmask;
-        rc = (rc >> 2) | ((3u - sr.next()) << (2 * h - 2));
-      }
+    uint64_t qa, qb;
+    const uint64_t s0 = warp_run(a, c, b, j, w, HS_NT / 32, &qa, &qb);
+    if (qa < qb && qb <= a.keys_cap) {
+      uint64_t q = qa + (threadIdx.x & 31u);
+      warp_kmers<K>(a, qa, qb, s0, a.bin_start[b + 1], [&](K key, bool valid) {
+        if (valid) {
+          flat[q] = key;
+          atomicAdd(&hist[coarse_digit<K>(key, key_bits, cb)], 1u);
+        }
+        q += 32;
+      });
+    } else if (qa < qb && (threadIdx.x & 31u) == 0) {
+      atomicOr(a.err, ERR_CAPACITY);
     }
     __syncthreads();
     uint32_t *row = a.hist + a.hist_base[b] + j * nd;  // the chunk's row, digits contiguous
@@ -282,7 +292,7 @@ __global__ void __launch_bounds__(HS_NT) k_bucket_hist(ExpandArgs a) {
 // bin's first key.
 constexpr int BS_NT = 1024;
 __global__ void __launch_bounds__(BS_NT) k_bucket_scan(ExpandArgs a, uint64_t *bucket_start,
-                                                       uint64_t *bucket_size) {
+                                                       uint64_t *bucket_size, uint32_t *bucket_bin) {
   __shared__ uint32_t tmp[64];
   constexpr int DPT = (1 << kCoarseMaxBits) / BS_NT;
   if (*a.err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
@@ -319,6 +329,7 @@ __global__ void __launch_bounds__(BS_NT) k_bucket_scan(ExpandArgs a, uint64_t *b
       if (d < nd) {
         bucket_start[g0 + d] = a.bin_kstart[b] + run;
         bucket_size[g0 + d] = col[u];
+        bucket_bin[g0 + d] = b;
       }
       run += col[u];
     }
@@ -339,67 +350,108 @@ __global__ void __launch_bounds__(BS_NT) k_bucket_scan(ExpandArgs a, uint64_t *b
 
 // -------------------------------------------------------------- 3. scatter
 
-constexpr int SC_THREADS = 256;
+constexpr int SC_THREADS = 1024;
+// keys per scatter tile: the tile, its digits and three digit tables fill
+// most of the shared memory of one CTA per SM
+template <typename K> constexpr int sc_tile() { return sizeof(K) == 8 ? 16384 : 8192; }
 
-// Expands every k-mer once and writes it to its bucket: the chunk's write
-// offset per digit (from the scan) plus the key's rank among the chunk's keys
-// of that digit, taken with a shared-memory atomic.  Threads walk contiguous
-// runs as in the histogram; the first k-mer of each superkmer segment is
-// extracted whole, the rest rolled in (kmer_counting.cu:99-112, canonical
-// form :33-44).
+// Moves every key of `flat` to its bucket.  Each CTA takes whole chunks, a
+// tile of SC_TILE keys at a time: the tile is counting-sorted by digit in
+// shared memory (a key's rank within its digit from a shared-memory atomic),
+// then written out in that order, so the keys of one digit leave as a
+// contiguous run at the chunk's write offset for the digit (from the scan)
+// plus the digit's keys of the chunk's earlier tiles.
 template <typename K>
-__global__ void __launch_bounds__(SC_THREADS) k_bucket_scatter(ExpandArgs a) {
-  __shared__ uint32_t cnt[1 << kCoarseMaxBits];
-  __shared__ uint32_t gbase[1 << kCoarseMaxBits];
+__global__ void __launch_bounds__(SC_THREADS, 1) k_bucket_scatter(ExpandArgs a) {
+  constexpr int SC_TILE = sc_tile<K>(), KPT = SC_TILE / SC_THREADS;
+  constexpr int ND = 1 << kCoarseMaxBits;
+  extern __shared__ __align__(16) uint8_t sc_smem[];
+  K *S = reinterpret_cast<K *>(sc_smem);                      // the tile, by digit
+  uint16_t *Sd = reinterpret_cast<uint16_t *>(S + SC_TILE);   // digits of S
+  uint32_t *gbase = reinterpret_cast<uint32_t *>(Sd + SC_TILE);  // chunk's write offsets
+  uint32_t *done = gbase + ND;                                // digit's keys of the chunk's earlier tiles
+  uint32_t *toff = done + ND;                                 // tile counts, then tile offsets (ND + 1)
+  uint32_t *tmp = toff + ND + 1;                              // block scan
   if (*a.err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
   K *keys = reinterpret_cast<K *>(a.keys);
+  const K *flat = reinterpret_cast<const K *>(a.flat);
   const uint64_t n_chunks = a.chunk_base[a.nbins];
-  const int k = a.k, key_bits = 2 * k, top = 2 * k - 2;
-  const K mask = kmer_mask<K>(k);
+  const int key_bits = 2 * a.k;
+  const int tid = threadIdx.x;
   for (uint64_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
     const uint32_t b = find_bin(a.chunk_base, a.nbins, c);
     const uint64_t j = c - a.chunk_base[b];
     const int cb = (int)a.bin_bits[b];
     const uint32_t nd = 1u << cb;
     const uint64_t kbase = a.bin_kstart[b];
+    const uint64_t q0 = kbase + j * a.chunk_kmers;
+    const uint64_t q1 = min(q0 + a.chunk_kmers, a.bin_kstart[b + 1]);
     const uint32_t *row = a.hist + a.hist_base[b] + j * nd;
-    for (uint32_t d = threadIdx.x; d < nd; d += SC_THREADS) {
+    for (uint32_t d = tid; d < nd; d += SC_THREADS) {
       gbase[d] = row[d];
-      cnt[d] = 0;
+      done[d] = 0;
     }
-    __syncthreads();
-    uint64_t q, qe;
-    uint64_t s = thread_run(a, c, b, j, SC_THREADS, &q, &qe);
-    while (q < qe) {
-      const uint64_t ks = __ldg(a.koff + s), ke = __ldg(a.koff + s + 1);
-      if (ke <= q) {
-        s++;
-        continue;
+    for (uint64_t t0 = q0; t0 < q1; t0 += SC_TILE) {
+      const uint32_t tn = (uint32_t)min((uint64_t)SC_TILE, q1 - t0);
+      for (uint32_t d = tid; d < nd; d += SC_THREADS) toff[d] = 0;
+      __syncthreads();
+      K xs[KPT];
+      uint32_t rk[KPT / 2];  // ranks within the digit, two 16-bit halves (< SC_TILE)
+#pragma unroll
+      for (int u = 0; u < KPT / 2; u++) rk[u] = 0;
+#pragma unroll
+      for (int u = 0; u < KPT; u++) {
+        const uint32_t i = u * SC_THREADS + tid;
+        if (i < tn) {
+          xs[u] = flat[t0 + i];
+          rk[u / 2] |= atomicAdd(&toff[coarse_digit<K>(xs[u], key_bits, cb)], 1u) << (16 * (u & 1));
+        }
       }
-      const uint64_t off = __ldg(a.desc + s) >> 24;
-      const uint32_t o = (uint32_t)(q - ks);
-      uint32_t n = (uint32_t)(min(qe, ke) - q);
-      K x = extract_kmer<K>(a.packed, off, o, k);
-      K r = revcomp_k<K>(x, k);
-      BaseStream bs;
-      bs.init(a.packed + off, o + k);
-      q += n;
-      s++;
-      while (true) {
-        const K key = x < r ? x : r;
-        const uint32_t d = coarse_digit<K>(key, key_bits, cb);
-        const uint64_t slot = kbase + gbase[d] + atomicAdd(&cnt[d], 1u);
-        if (slot < a.keys_cap) keys[slot] = key;
+      __syncthreads();
+      // exclusive scan of the tile counts, thread-contiguous digits
+      const uint32_t per = (nd + SC_THREADS - 1) / SC_THREADS, d0 = tid * per;
+      uint32_t sum = 0;
+      for (uint32_t d = d0; d < d0 + per && d < nd; d++) sum += toff[d];
+      uint32_t total;
+      uint32_t run = block_exclusive_scan<SC_THREADS>(sum, tmp, &total);
+      for (uint32_t d = d0; d < d0 + per && d < nd; d++) {
+        const uint32_t v = toff[d];
+        toff[d] = run;
+        run += v;
+      }
+      if (tid == 0) toff[nd] = total;
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < KPT; u++) {
+        const uint32_t i = u * SC_THREADS + tid;
+        if (i < tn) {
+          const uint32_t d = coarse_digit<K>(xs[u], key_bits, cb);
+          const uint32_t at = toff[d] + ((rk[u / 2] >> (16 * (u & 1))) & 0xFFFFu);
+          S[at] = xs[u];
+          Sd[at] = (uint16_t)d;
+        }
+      }
+      __syncthreads();
+      for (uint32_t i = tid; i < tn; i += SC_THREADS) {
+        const uint32_t d = Sd[i];
+        const uint64_t slot = kbase + gbase[d] + done[d] + (i - toff[d]);
+        if (slot < a.keys_cap) keys[slot] = S[i];
         else atomicOr(a.err, ERR_CAPACITY);
-        if (--n == 0) break;
-        const uint32_t cc = bs.next();
-        x = ((x << 2) | (K)cc) & mask;
-        r = (r >> 2) | ((K)(3u - cc) << top);
       }
+      __syncthreads();
+      for (uint32_t d = tid; d < nd; d += SC_THREADS) done[d] += toff[d + 1] - toff[d];
+      __syncthreads();  // before the next tile clears toff
     }
-    __syncthreads();
   }
 }
+
+template <typename K> size_t bucket_scatter_smem_bytes() {
+  constexpr int ND = 1 << kCoarseMaxBits;
+  static_assert(sc_tile<K>() <= 65536 && sc_tile<K>() % SC_THREADS == 0, "16-bit ranks, whole rounds");
+  return (size_t)sc_tile<K>() * (sizeof(K) + 2) + 4 * (3 * ND + 1 + 64);
+}
+template size_t bucket_scatter_smem_bytes<uint64_t>();
+template size_t bucket_scatter_smem_bytes<u128>();
 
 // ---------------------------------------------------------------- 4. count
 
@@ -408,8 +460,9 @@ template <> struct CountShape<uint64_t> { static constexpr int NT = 512, CAP = 8
 template <> struct CountShape<u128> { static constexpr int NT = 512, CAP = 4096; };
 constexpr int CC_SB_MAX = 12;        // sub-bucket bits
 constexpr int CC_NSUB_MAX = 1 << CC_SB_MAX;
-constexpr uint32_t CC_SEG_MAX = 64;  // longer per-thread segments are sorted by warps
-constexpr int CC_BIG_LIST = 128;
+constexpr uint32_t CC_THREAD_MAX = 8;  // larger sub-buckets are reduced by warps
+constexpr int CC_BIG_LIST = 1024;      // > CAP / (CC_THREAD_MAX + 1): every larger sub-bucket fits
+constexpr uint32_t CC_TICKETS = 4;     // buckets taken per ticket
 constexpr int CC_STACK = 2 * 129 + 2;  // key-range halving: at most 128 levels, two entries each
 
 // Heavy-slice hash table: keys, counts and a slot state (0 free, 1 being
@@ -434,14 +487,22 @@ struct CountSmem {
   uint32_t cnt[CC_NSUB_MAX + 1];  // sub-bucket counts, then starts
   uint32_t seg_pos[NT];           // output position of each thread's runs (exclusive scan)
   uint32_t seg_src[NT];           // first run of each thread's segment in A
-  uint32_t big[CC_BIG_LIST];      // threads whose segments are sorted by warps
+  uint16_t big[CC_BIG_LIST];      // sub-buckets reduced by warps
   uint32_t tmp[64];
   uint32_t nbig, hfill, nsub;
   int flag, sp;
   uint64_t g, start, n, out_base, run, tbase;
   uint32_t b;
-  K stk_lo[CC_STACK], stk_hi[CC_STACK];
+  union {
+    struct {
+      K lo[CC_STACK], hi[CC_STACK];
+    } stk;                       // key-range stack of the heavy path
+    uint16_t dc[CC_NSUB_MAX];    // distinct keys of each sub-bucket of a slice
+  } w;
 };
+
+static_assert(CountShape<uint64_t>::CAP / (CC_THREAD_MAX + 1) < CC_BIG_LIST, "big list holds every large sub-bucket");
+static_assert(CountShape<u128>::CAP / (CC_THREAD_MAX + 1) < CC_BIG_LIST, "big list holds every large sub-bucket");
 
 template <typename K> size_t bucket_count_smem_bytes() { return sizeof(CountSmem<K>); }
 template size_t bucket_count_smem_bytes<uint64_t>();
@@ -539,62 +600,265 @@ GKC_DEV void scan_sub(CountSmem<K> &S, uint32_t nsub) {
   __syncthreads();
 }
 
+template <typename K>
+GKC_DEV void insertion_sort(K *A, uint32_t b0, uint32_t b1) {
+  for (uint32_t p = b0 + 1; p < b1; p++) {
+    const K x = A[p];
+    uint32_t q = p;
+    while (q > b0 && x < A[q - 1]) {
+      A[q] = A[q - 1];
+      q--;
+    }
+    A[q] = x;
+  }
+}
+
+// Run-length encodes the sorted A[b0, b1) in place (keys in A, counts in C
+// from b0); returns the number of runs.
+template <typename K>
+GKC_DEV uint32_t rle_in_place(K *A, uint16_t *C, uint32_t b0, uint32_t b1) {
+  uint32_t u = 0;
+  for (uint32_t i = b0; i < b1;) {
+    const K x = A[i];
+    uint32_t c = 1;
+    i++;
+    while (i < b1 && A[i] == x) {
+      c++;
+      i++;
+    }
+    A[b0 + u] = x;
+    C[b0 + u] = (uint16_t)c;  // c <= m <= CAP < 2^16
+    u++;
+  }
+  return u;
+}
+
+template <typename K> GKC_DEV K shfl_xor_k(K v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+template <> GKC_DEV u128 shfl_xor_k<u128>(u128 v, int m) {
+  const uint64_t lo = __shfl_xor_sync(0xffffffffu, (uint64_t)v, m);
+  const uint64_t hi = __shfl_xor_sync(0xffffffffu, (uint64_t)(v >> 64), m);
+  return ((u128)hi << 64) | lo;
+}
+template <typename K> GKC_DEV K shfl_up_k(K v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+template <> GKC_DEV u128 shfl_up_k<u128>(u128 v, int d) {
+  const uint64_t lo = __shfl_up_sync(0xffffffffu, (uint64_t)v, d);
+  const uint64_t hi = __shfl_up_sync(0xffffffffu, (uint64_t)(v >> 64), d);
+  return ((u128)hi << 64) | lo;
+}
+
+GKC_DEV uint32_t warp_exclusive_scan(uint32_t c, uint32_t *total) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t inc = c;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= (uint32_t)d) inc += t;
+  }
+  *total = __shfl_sync(0xffffffffu, inc, 31);
+  return inc - c;
+}
+
+// Sorts A[b0, b0 + n), n <= 32 R, with the calling warp: lane l holds
+// positions l R .. l R + R - 1 in registers (positions past n hold the
+// largest key, so the first n sorted positions are A's keys), a bitonic
+// network over 32 R positions; then run-length encodes the sorted keys in
+// place (keys in A, counts in C from b0).  Returns the number of runs.
+template <typename K, int R>
+GKC_DEV uint32_t warp_sort_rle(K *A, uint16_t *C, uint32_t b0, uint32_t n) {
+  constexpr uint32_t N = 32 * R;
+  const uint32_t lane = threadIdx.x & 31u;
+  K v[R];
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const uint32_t e = lane * R + r;
+    v[r] = e < n ? A[b0 + e] : ~(K)0;
+  }
+#pragma unroll
+  for (uint32_t size = 2; size <= N; size <<= 1) {
+#pragma unroll
+    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride < (uint32_t)R) {
+#pragma unroll
+        for (int r = 0; r < R; r++)
+          if ((r & stride) == 0) {
+            const bool asc = ((lane * R + r) & size) == 0;
+            const K x = v[r], y = v[r + stride];
+            const bool sw = asc ? (y < x) : (x < y);
+            v[r] = sw ? y : x;
+            v[r + stride] = sw ? x : y;
+          }
+      } else {
+        const int lm = (int)(stride / R);
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const K y = shfl_xor_k<K>(v[r], lm);
+          const bool asc = ((lane * R + r) & size) == 0;
+          const bool low = (lane & (uint32_t)lm) == 0;  // the lower position of the pair
+          const bool keep_min = low == asc;
+          v[r] = keep_min ? (y < v[r] ? y : v[r]) : (v[r] < y ? y : v[r]);
+        }
+      }
+    }
+  }
+  // run heads among the first n positions
+  const K before = shfl_up_k<K>(v[R - 1], 1);
+  uint32_t hb = 0;
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const uint32_t e = lane * R + r;
+    const K p = r == 0 ? before : v[r > 0 ? r - 1 : 0];
+    if (e < n && (e == 0 || p != v[r])) hb |= 1u << r;
+  }
+  uint32_t D;
+  const uint32_t rank0 = warp_exclusive_scan(__popc(hb), &D);
+  __syncwarp();
+  uint32_t rank = rank0;
+#pragma unroll
+  for (int r = 0; r < R; r++)
+    if ((hb >> r) & 1u) {
+      A[b0 + rank] = v[r];
+      C[b0 + rank] = (uint16_t)(lane * R + r);  // the run's first position, < 32 R
+      rank++;
+    }
+  __syncwarp();
+  uint32_t nxt[R];
+  rank = rank0;
+#pragma unroll
+  for (int r = 0; r < R; r++)
+    if ((hb >> r) & 1u) {
+      nxt[r] = rank + 1 < D ? C[b0 + rank + 1] : n;
+      rank++;
+    }
+  __syncwarp();
+  rank = rank0;
+#pragma unroll
+  for (int r = 0; r < R; r++)
+    if ((hb >> r) & 1u) {
+      C[b0 + rank] = (uint16_t)(nxt[r] - (lane * R + r));
+      rank++;
+    }
+  __syncwarp();
+  return D;
+}
+
+template <typename K> GKC_DEV K warp_min_k(K v) {
+#pragma unroll
+  for (int m = 16; m > 0; m >>= 1) {
+    const K y = shfl_xor_k<K>(v, m);
+    v = y < v ? y : v;
+  }
+  return v;
+}
+
+// Run-length encodes A[b0, b0 + n) with the calling warp when it holds at
+// most 32 distinct keys: each round takes the smallest key above the last
+// one and counts its copies.  Returns the number of runs, or 0 (A untouched)
+// when there are more.
+template <typename K>
+GKC_DEV uint32_t warp_select_rle(K *A, uint16_t *C, uint32_t b0, uint32_t n) {
+  const uint32_t lane = threadIdx.x & 31u;
+  K mine = 0;
+  uint32_t mine_c = 0, d = 0, seen = 0;
+  K last = 0;
+  while (seen < n) {
+    if (d == 32) return 0;
+    K lo = ~(K)0;
+    bool any = false;
+    for (uint32_t i = lane; i < n; i += 32) {
+      const K x = A[b0 + i];
+      if ((d == 0 || last < x) && (!any || x < lo)) {
+        lo = x;
+        any = true;
+      }
+    }
+    // lanes with nothing above `last` offer the largest key, which is only
+    // taken when no lane has a smaller one; the copies counted below decide
+    const K key = warp_min_k<K>(lo);
+    uint32_t c = 0;
+    for (uint32_t i = lane; i < n; i += 32) c += A[b0 + i] == key ? 1u : 0u;
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) c += __shfl_xor_sync(0xffffffffu, c, m);
+    if (lane == d) {
+      mine = key;
+      mine_c = c;
+    }
+    last = key;
+    seen += c;
+    d++;
+  }
+  __syncwarp();
+  if (lane < d) {
+    A[b0 + lane] = mine;
+    C[b0 + lane] = (uint16_t)mine_c;
+  }
+  __syncwarp();
+  return d;
+}
+
 // The m keys in S.u.A are grouped by sub-bucket: sub-bucket jb + jj starts at
 // S.cnt[jb + jj] - s0 for jj in [0, nsl) (the last one ends at m).  Each
-// thread sorts the sub-buckets it owns and run-length encodes them in place
-// (keys in A, counts in C); longer segments are sorted by warps first.  Sets
+// sub-bucket is reduced to its runs in place: by the thread that owns it
+// (insertion sort) when it holds at most CC_THREAD_MAX keys, else by a warp
+// (a register bitonic sort up to 128 keys; above that, rounds that take the
+// next smallest key while there are at most 32 distinct ones; else a bitonic
+// sort in shared memory).  A k-mer seen many times fills a sub-bucket with
+// copies of itself and of its sequencing-error variants, which share its
+// leading bases.  Each thread then packs the runs of the sub-buckets it owns
+// together from their first key on (keys in A, counts in C).  Sets
 // S.seg_src / S.seg_pos (exclusive scan of the run counts) and returns the
 // slice's distinct keys.
 template <typename K, int NT>
 GKC_DEV uint32_t slice_runs(CountSmem<K> &S, uint32_t m, uint32_t jb, uint32_t nsl, uint32_t s0) {
   const int tid = threadIdx.x;
   K *A = S.u.A;
+  uint16_t *dc = S.w.dc;
   auto start_of = [&](uint32_t jj) -> uint32_t { return jj < nsl ? S.cnt[jb + jj] - s0 : m; };
   const uint32_t j0 = (uint32_t)(((uint64_t)tid * nsl) / NT), j1 = (uint32_t)(((uint64_t)(tid + 1) * nsl) / NT);
-  const uint32_t s = start_of(j0), e = start_of(j1);
   if (tid == 0) S.nbig = 0;
   __syncthreads();
-  bool big = e - s > CC_SEG_MAX;
-  if (big) {
-    const uint32_t t = atomicAdd(&S.nbig, 1u);
-    if (t < (uint32_t)CC_BIG_LIST) S.big[t] = (uint32_t)tid;
-    else big = false;  // list full: sorted by its own thread
+  for (uint32_t jj = j0; jj < j1; jj++) {
+    const uint32_t b0 = start_of(jj), b1 = start_of(jj + 1);
+    if (b1 - b0 <= CC_THREAD_MAX) {
+      insertion_sort<K>(A, b0, b1);
+      dc[jj] = (uint16_t)rle_in_place<K>(A, S.C, b0, b1);
+    } else {
+      S.big[atomicAdd(&S.nbig, 1u)] = (uint16_t)jj;  // fewer than CC_BIG_LIST (static_assert)
+    }
   }
-  if (!big) {
-    for (uint32_t jj = j0; jj < j1; jj++) {
-      const uint32_t b0 = start_of(jj), b1 = start_of(jj + 1);
-      for (uint32_t p = b0 + 1; p < b1; p++) {
-        const K x = A[p];
-        uint32_t q = p;
-        while (q > b0 && x < A[q - 1]) {
-          A[q] = A[q - 1];
-          q--;
-        }
-        A[q] = x;
+  __syncthreads();
+  const uint32_t nbig = S.nbig, lane = threadIdx.x & 31u;
+  for (uint32_t t = threadIdx.x >> 5; t < nbig; t += NT / 32) {
+    const uint32_t jj = S.big[t];
+    const uint32_t b0 = start_of(jj), n = start_of(jj + 1) - b0;
+    uint32_t d;
+    if (n <= 32) {
+      d = warp_sort_rle<K, 1>(A, S.C, b0, n);
+    } else if (n <= 64) {
+      d = warp_sort_rle<K, 2>(A, S.C, b0, n);
+    } else if (n <= 128) {
+      d = warp_sort_rle<K, 4>(A, S.C, b0, n);
+    } else {
+      d = warp_select_rle<K>(A, S.C, b0, n);
+      if (d == 0) {
+        warp_sort<K>(A + b0, n);
+        if (lane == 0) d = rle_in_place<K>(A, S.C, b0, b0 + n);
+        d = __shfl_sync(0xffffffffu, d, 0);
       }
     }
+    if (lane == 0) dc[jj] = (uint16_t)d;
+    __syncwarp();
   }
   __syncthreads();
-  const uint32_t nbig = min(S.nbig, (uint32_t)CC_BIG_LIST);
-  for (uint32_t t = threadIdx.x >> 5; t < nbig; t += NT / 32) {
-    const uint32_t ow = S.big[t];
-    const uint32_t oj0 = (uint32_t)(((uint64_t)ow * nsl) / NT), oj1 = (uint32_t)(((uint64_t)(ow + 1) * nsl) / NT);
-    const uint32_t os = start_of(oj0);
-    warp_sort<K>(A + os, start_of(oj1) - os);
-  }
-  __syncthreads();
+  const uint32_t s = start_of(j0);
   uint32_t u = 0;
-  for (uint32_t i = s; i < e;) {
-    const K x = A[i];
-    uint32_t c = 1;
-    i++;
-    while (i < e && A[i] == x) {
-      c++;
-      i++;
-    }
-    A[s + u] = x;
-    S.C[s + u] = (uint16_t)c;  // c <= m <= CAP < 2^16
-    u++;
+  for (uint32_t jj = j0; jj < j1; jj++) {
+    const uint32_t b0 = start_of(jj), d = dc[jj];
+    if (b0 != s + u)
+      for (uint32_t i = 0; i < d; i++) {
+        A[s + u + i] = A[b0 + i];
+        S.C[s + u + i] = S.C[b0 + i];
+      }
+    u += d;
   }
   uint32_t D;
   const uint32_t pos = block_exclusive_scan<NT>(u, S.tmp, &D);
@@ -638,13 +902,13 @@ GKC_DEV void heavy_slice(CountSmem<K> &S, const SortCountArgs &a, const K *src, 
   const int tid = threadIdx.x;
   if (tid == 0) {
     S.sp = 1;
-    S.stk_lo[0] = (K)0;
-    S.stk_hi[0] = ~(K)0;
+    S.w.stk.lo[0] = (K)0;
+    S.w.stk.hi[0] = ~(K)0;
   }
   __syncthreads();
   while (true) {
     if (S.sp == 0) break;
-    const K lo = S.stk_lo[S.sp - 1], hi = S.stk_hi[S.sp - 1];
+    const K lo = S.w.stk.lo[S.sp - 1], hi = S.w.stk.hi[S.sp - 1];
     for (int s = tid; s < HN; s += NT) {
       T.cnt[s] = 0;
       T.state[s] = 0;
@@ -701,10 +965,10 @@ GKC_DEV void heavy_slice(CountSmem<K> &S, const SortCountArgs &a, const K *src, 
       if (tid == 0) {
         const K mid = lo + ((hi - lo) >> 1);
         if (S.sp + 2 <= CC_STACK) {
-          S.stk_lo[S.sp] = mid + 1;  // upper half below the lower half
-          S.stk_hi[S.sp] = hi;
-          S.stk_lo[S.sp + 1] = lo;
-          S.stk_hi[S.sp + 1] = mid;
+          S.w.stk.lo[S.sp] = mid + 1;  // upper half below the lower half
+          S.w.stk.hi[S.sp] = hi;
+          S.w.stk.lo[S.sp + 1] = lo;
+          S.w.stk.hi[S.sp + 1] = mid;
           S.sp += 2;
         } else {
           atomicOr(a.err, ERR_BOUNDS);
@@ -754,6 +1018,128 @@ GKC_DEV void heavy_slice(CountSmem<K> &S, const SortCountArgs &a, const K *src, 
   }
 }
 
+// ---- hash path (8-byte keys): a bucket's keys aggregated in a shared-memory
+// table first, so that only its distinct keys are sorted, by a bitonic
+// network (keys of a minimizer bin are far from uniform in their leading
+// bases: those holding the minimizer near their start share them, so digit
+// splits of a bucket can be very uneven).  The keys are read from global
+// memory, so a bucket of any size with few enough distinct keys takes this
+// path.  The table lives in the upper half of the key area (keys) and in the
+// run-count area (counts); the distinct keys go to the lower half of the key
+// area, their counts to the sub-bucket counters.
+constexpr uint32_t HT_SLOTS = 4096;
+constexpr uint32_t HT_MAX_DISTINCT = 3072;  // 3/4 full: beyond it the bucket takes the sub-bucket path
+constexpr uint64_t HT_EMPTY = ~0ull;        // never a canonical key: the reverse complement of all-T is all-A
+
+GKC_DEV uint32_t ht_slot(uint64_t x) { return (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> 52); }
+
+template <int NT, typename K>
+GKC_DEV bool hash_count(CountSmem<K> &, const SortCountArgs &, const K *, uint64_t, uint64_t, uint64_t) {
+  return false;  // 16-byte keys: no 128-bit compare-and-swap in shared memory here
+}
+
+// Counts the n keys src[0, n) (read from global memory, any n) through the
+// table and writes the bucket's sorted runs to the staging arrays at
+// `start`.  Returns false, with nothing written, when the bucket has more
+// than HT_MAX_DISTINCT distinct keys (the caller then takes the sub-bucket
+// or the scratch path).  Not inlined: its registers are then not added to
+// the count kernel's.
+template <int NT>
+__device__ __noinline__ bool hash_count(CountSmem<uint64_t> &S, const SortCountArgs &a, const uint64_t *src,
+                                        uint64_t n, uint64_t start, uint64_t g) {
+  static_assert(2 * HT_SLOTS <= (uint32_t)CountShape<uint64_t>::CAP, "table and sorted keys share the key area");
+  static_assert(sizeof(S.C) >= HT_SLOTS * 4, "table counts fit the run-count area");
+  static_assert(sizeof(S.cnt) >= HT_SLOTS * 4, "sorted counts fit the sub-bucket counters");
+  constexpr uint32_t SPT = HT_SLOTS / NT;
+  constexpr int U = 4;  // keys in flight per thread
+  volatile uint64_t *T = S.u.A + HT_SLOTS;
+  uint32_t *TC = reinterpret_cast<uint32_t *>(S.C);
+  uint64_t *B = S.u.A;
+  uint32_t *BC = S.cnt;
+  const int tid = threadIdx.x;
+  for (uint32_t i = tid; i < HT_SLOTS; i += NT) {
+    T[i] = HT_EMPTY;
+    TC[i] = 0;
+  }
+  if (tid == 0) {
+    S.hfill = 0;
+    S.flag = 0;
+  }
+  __syncthreads();
+  for (uint64_t i0 = tid; i0 < n; i0 += (uint64_t)U * NT) {
+    if (*(volatile int *)&S.flag) break;
+    uint64_t xs[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const uint64_t i = i0 + (uint64_t)u * NT;
+      xs[u] = i < n ? __ldg(reinterpret_cast<const unsigned long long *>(src) + i) : HT_EMPTY;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const uint64_t x = xs[u];
+      if (i0 + (uint64_t)u * NT >= n) break;
+      uint32_t h = ht_slot(x);
+      for (uint32_t probe = 0; probe < HT_SLOTS; probe++) {
+        uint64_t cur = T[h];
+        if (cur == HT_EMPTY) {
+          cur = atomicCAS((unsigned long long *)(S.u.A + HT_SLOTS + h), (unsigned long long)HT_EMPTY,
+                          (unsigned long long)x);
+          if (cur == HT_EMPTY) {
+            atomicAdd(&TC[h], 1u);
+            if (atomicAdd(&S.hfill, 1u) + 1 > HT_MAX_DISTINCT) S.flag = 1;
+            break;
+          }
+        }
+        if (cur == x) {
+          atomicAdd(&TC[h], 1u);
+          break;
+        }
+        h = (h + 1) & (HT_SLOTS - 1);
+      }
+    }
+  }
+  __syncthreads();
+  if (S.flag) return false;
+  const uint32_t D = S.hfill;
+  // the distinct keys, in slot order, to B[0, D), their counts to BC; the
+  // rest of the power of two above D holds the largest key
+  uint32_t own = 0;
+#pragma unroll
+  for (int q = 0; q < (int)SPT; q++) own += T[q * NT + tid] != HT_EMPTY ? 1u : 0u;
+  uint32_t tot;
+  uint32_t pos = block_exclusive_scan<NT>(own, S.tmp, &tot);
+#pragma unroll
+  for (int q = 0; q < (int)SPT; q++) {
+    const uint32_t slot = q * NT + tid;
+    const uint64_t x = T[slot];
+    if (x != HT_EMPTY) {
+      B[pos] = x;
+      BC[pos] = TC[slot];
+      pos++;
+    }
+  }
+  uint32_t P = 1;
+  while (P < D) P <<= 1;
+  for (uint32_t i = D + tid; i < P; i += NT) {
+    B[i] = HT_EMPTY;
+    BC[i] = 0;
+  }
+  __syncthreads();
+  block_sort_pairs<uint64_t, NT>(B, BC, P);
+  uint64_t *out = reinterpret_cast<uint64_t *>(a.stage_keys);
+  for (uint32_t i = tid; i < D; i += NT) {
+    if (start + i < a.stage_cap) {
+      out[start + i] = B[i];
+      a.stage_counts[start + i] = BC[i];
+    } else {
+      atomicOr(a.err, ERR_CAPACITY);
+    }
+  }
+  if (tid == 0) a.bucket_d[g] = D;
+  __syncthreads();
+  return true;
+}
+
 template <typename K>
 __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCountArgs a) {
   constexpr int NT = CountShape<K>::NT, CAP = CountShape<K>::CAP, KPT = CAP / NT;
@@ -766,13 +1152,20 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
   const int tid = threadIdx.x;
   if (*a.err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
   const uint64_t n_buckets = a.bucket_base[a.nbins];
+  int hash_skip = 0;                // the same in every thread of the block
+  uint64_t t_next = 0, t_end = 0;   // thread 0: the rest of its batch of tickets
   while (true) {
     if (tid == 0) {
-      S.g = atomicAdd(a.ticket, 1ull);
-      if (S.g < n_buckets) {
-        S.b = find_bin(a.bucket_base, a.nbins, S.g);
-        S.start = a.bucket_start[S.g];
-        S.n = a.bucket_size[S.g];
+      if (t_next == t_end) {
+        t_next = atomicAdd(a.ticket, (unsigned long long)CC_TICKETS);
+        t_end = t_next + CC_TICKETS;
+      }
+      const uint64_t gg = t_next++;
+      S.g = gg;
+      if (gg < n_buckets) {
+        S.b = a.bucket_bin[gg];
+        S.start = a.bucket_start[gg];
+        S.n = a.bucket_size[gg];
       }
     }
     __syncthreads();
@@ -781,16 +1174,29 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
     const uint64_t start = S.start, n = S.n;
     const uint32_t b = S.b;
     const int cb = (int)a.bin_bits[b];
+    // distinct keys through the table first, unless the last bucket that
+    // tried it had too many (then skip it for a few buckets)
+    if (hash_skip == 0) {
+      if (hash_count<NT>(S, a, keys + start, n, start, g)) continue;
+      hash_skip = 8;
+    } else {
+      hash_skip--;
+    }
     if (n <= (uint64_t)CAP) {
       // ---- the whole bucket in shared memory
       const uint32_t m = (uint32_t)n;
+      K xs[KPT];
+#pragma unroll
+      for (int u = 0; u < KPT; u++) {
+        const uint32_t i = u * NT + tid;
+        if (i < m) xs[u] = keys[start + i];
+      }
       int sb = 0;
-      while (sb < CC_SB_MAX && (2u << sb) <= m) sb++;
+      while (sb < CC_SB_MAX && (1u << sb) < 2 * m) sb++;
       sb = min(sb, room - cb);
       const uint32_t nsub = 1u << sb;
       for (uint32_t jj = tid; jj < nsub; jj += NT) S.cnt[jj] = 0;
       __syncthreads();
-      K xs[KPT];
       uint32_t rk[(KPT + 1) / 2];
 #pragma unroll
       for (int u = 0; u < (KPT + 1) / 2; u++) rk[u] = 0;
@@ -798,7 +1204,6 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
       for (int u = 0; u < KPT; u++) {
         const uint32_t i = u * NT + tid;
         if (i < m) {
-          xs[u] = keys[start + i];
           const uint32_t r = atomicAdd(&S.cnt[sub_digit<K>(xs[u], key_bits, cb, sb)], 1u);
           rk[u / 2] |= r << (16 * (u & 1));
         }
@@ -922,6 +1327,8 @@ template __global__ void k_compact_runs<uint64_t>(const uint64_t *, const uint32
 template __global__ void k_compact_runs<u128>(const u128 *, const uint32_t *, const uint64_t *,
                                               const unsigned long long *, const uint64_t *, const uint64_t *,
                                               uint32_t, u128 *, uint32_t *, uint64_t *, const uint32_t *);
+template __global__ void k_bucket_hist<uint64_t>(ExpandArgs);
+template __global__ void k_bucket_hist<u128>(ExpandArgs);
 template __global__ void k_bucket_scatter<uint64_t>(ExpandArgs);
 template __global__ void k_bucket_scatter<u128>(ExpandArgs);
 template __global__ void k_bucket_count<uint64_t>(SortCountArgs);

@@ -83,16 +83,18 @@ struct ExpandArgs {
   uint64_t *chunk_s0;          // first superkmer of each chunk
   uint32_t *hist;              // (bin, chunk, digit) counts, then write offsets in the bin
   void *keys;                  // scatter output (uint64 or u128)
-  uint64_t keys_cap;
+  void *flat;                  // the keys in k-mer order (written by the histogram, read by the scatter)
+  uint64_t keys_cap;          // of keys and flat
   uint32_t *err;
 };
 __global__ void k_chunk_first(ExpandArgs a);
-__global__ void k_bucket_hist(ExpandArgs a);
-__global__ void k_bucket_scan(ExpandArgs a, uint64_t *bucket_start, uint64_t *bucket_size);
+template <typename K> __global__ void k_bucket_hist(ExpandArgs a);
+__global__ void k_bucket_scan(ExpandArgs a, uint64_t *bucket_start, uint64_t *bucket_size, uint32_t *bucket_bin);
 template <typename K> __global__ void k_bucket_scatter(ExpandArgs a);
 constexpr int kBucketScanThreads = 1024;
 constexpr int kBucketHistThreads = 256;
-constexpr int kBucketScatterThreads = 256;
+constexpr int kBucketScatterThreads = 1024;
+template <typename K> size_t bucket_scatter_smem_bytes();
 __global__ void k_skm_nk(const uint64_t *desc, const unsigned long long *n_skm_dev, int k,
                          unsigned long long *nk);
 
@@ -103,6 +105,7 @@ struct SortCountArgs {
   const uint32_t *bin_bits;
   const uint64_t *bucket_start;   // first key of each bucket
   const uint64_t *bucket_size;
+  const uint32_t *bucket_bin;     // bin of each bucket
   const void *keys;               // bucketed keys
   void *scratch;                  // oversized buckets, placed by sub-bucket
   uint64_t scratch_keys;
