@@ -679,6 +679,13 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   k_bucket_hist<K><<<c->n_sms * 8, kBucketHistThreads, 0, c->st>>>(ea);
   LAUNCHED(c);
   WS(bbin, uint32_t, "bucket_bin", max_buckets + 1);
+  WS(big_list, uint32_t, "big_list", max_buckets + 1);
+  // [0] bucket ticket, [1] scratch cursor, [2] large buckets listed, [3] their ticket
+  WS(ticket, unsigned long long, "count_ticket", 4);
+  CK(cudaMemsetAsync(ticket, 0, 32, c->st));
+  ea.big_list = big_list;
+  ea.big_count = ticket + 2;
+  ea.big_min = bucket_count_cap<K>();
   k_bucket_scan<<<std::min<uint32_t>(nbins, 65535), kBucketScanThreads, 0, c->st>>>(ea, bstart, bsize, bbin);
   LAUNCHED(c);
   stage_mark(c, 4);
@@ -694,10 +701,8 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   WS(bucket_d, unsigned long long, "bucket_d", max_buckets + 1);
   WS(bucket_out, uint64_t, "bucket_out", max_buckets + 2);
   WS(dtmp, uint64_t, "scan_tmp3", scan_u64_tmp_words(max_buckets + 1) + 8);
-  WS(ticket, unsigned long long, "count_ticket", 4);
   scratch_keys = std::max<uint64_t>(scratch_keys, 1 << 16);
   WS(scratch, K, "sort_scratch", scratch_keys);
-  CK(cudaMemsetAsync(ticket, 0, 32, c->st));
   SortCountArgs sa;
   memset(&sa, 0, sizeof(sa));
   sa.nbins = nbins;
@@ -716,6 +721,10 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   sa.stage_cap = keys_cap;
   sa.bucket_d = bucket_d;
   sa.ticket = ticket;
+  sa.big_list = big_list;
+  sa.big_count = ticket + 2;
+  sa.big_ticket = ticket + 3;
+  sa.big_min = ea.big_min;
   sa.err = err;
   const size_t smem = bucket_count_smem_bytes<K>();
   if ((int)smem > c->max_smem_optin) return ctx_fail(c, GKC_ERR_INTERNAL, "count tables exceed shared memory");

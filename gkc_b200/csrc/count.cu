@@ -330,6 +330,7 @@ __global__ void __launch_bounds__(BS_NT) k_bucket_scan(ExpandArgs a, uint64_t *b
         bucket_start[g0 + d] = a.bin_kstart[b] + run;
         bucket_size[g0 + d] = col[u];
         bucket_bin[g0 + d] = b;
+        if (col[u] >= a.big_min) a.big_list[atomicAdd(a.big_count, 1ull)] = (uint32_t)(g0 + d);
       }
       run += col[u];
     }
@@ -505,6 +506,9 @@ static_assert(CountShape<uint64_t>::CAP / (CC_THREAD_MAX + 1) < CC_BIG_LIST, "bi
 static_assert(CountShape<u128>::CAP / (CC_THREAD_MAX + 1) < CC_BIG_LIST, "big list holds every large sub-bucket");
 
 template <typename K> size_t bucket_count_smem_bytes() { return sizeof(CountSmem<K>); }
+template <typename K> uint64_t bucket_count_cap() { return CountShape<K>::CAP; }
+template uint64_t bucket_count_cap<uint64_t>();
+template uint64_t bucket_count_cap<u128>();
 template size_t bucket_count_smem_bytes<uint64_t>();
 template size_t bucket_count_smem_bytes<u128>();
 
@@ -1018,44 +1022,160 @@ GKC_DEV void heavy_slice(CountSmem<K> &S, const SortCountArgs &a, const K *src, 
   }
 }
 
+// Sorts the 32 R keys (with counts) at Kb / Cb by the calling warp in
+// registers: lane l holds positions r 32 + l, a bitonic network (strides
+// below 32 across lanes by shuffles, larger ones across a lane's registers).
+template <int R, typename CT>
+GKC_DEV void warp_sort_run(uint64_t *Kb, CT *Cb) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint64_t v[R];
+  uint32_t c[R];
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    v[r] = Kb[r * 32 + lane];
+    c[r] = Cb[r * 32 + lane];
+  }
+#pragma unroll
+  for (uint32_t size = 2; size <= 32u * R; size <<= 1) {
+#pragma unroll
+    for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride >= 32) {
+        const int rs = (int)(stride / 32);
+#pragma unroll
+        for (int r = 0; r < R; r++)
+          if ((r & rs) == 0) {
+            const bool asc = ((r * 32 + lane) & size) == 0;
+            const uint64_t x = v[r], y = v[r + rs];
+            if (asc ? (y < x) : (x < y)) {
+              v[r] = y;
+              v[r + rs] = x;
+              const uint32_t t = c[r];
+              c[r] = c[r + rs];
+              c[r + rs] = t;
+            }
+          }
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const bool asc = ((r * 32 + lane) & size) == 0;
+          const uint64_t y = __shfl_xor_sync(0xffffffffu, v[r], stride);
+          const uint32_t cy = __shfl_xor_sync(0xffffffffu, c[r], stride);
+          const bool keep_min = ((lane & stride) == 0) == asc;
+          if (keep_min ? (y < v[r]) : (v[r] < y)) {
+            v[r] = y;
+            c[r] = cy;
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    Kb[r * 32 + lane] = v[r];
+    Cb[r * 32 + lane] = (CT)c[r];
+  }
+}
+
+// Merges the sorted runs of length L of (sk, sc) pairwise into (dk, dc): each
+// thread writes P / NT consecutive outputs (at least one), starting from a
+// merge-path search of its first one.
+template <int NT, typename CT>
+GKC_DEV void merge_round(const uint64_t *sk, const CT *sc, uint64_t *dk, CT *dc, uint32_t P, uint32_t L) {
+  const uint32_t per = P >= (uint32_t)NT ? P / NT : 1u;
+  const uint32_t o0 = threadIdx.x * per;
+  if (o0 < P) {
+    const uint32_t a0 = o0 & ~(2 * L - 1);
+    const uint64_t *A = sk + a0, *Bk = sk + a0 + L;
+    const uint32_t o = o0 - a0;
+    uint32_t lo = o > L ? o - L : 0u, hi = o < L ? o : L;
+    while (lo < hi) {  // i = outputs before o taken from A (ties from A first)
+      const uint32_t mid = (lo + hi) >> 1;
+      if (A[mid] <= Bk[o - mid - 1]) lo = mid + 1; else hi = mid;
+    }
+    uint32_t i = lo, j = o - lo;
+    for (uint32_t t = 0; t < per; t++) {
+      if (j >= L || (i < L && A[i] <= Bk[j])) {
+        dk[o0 + t] = A[i];
+        dc[o0 + t] = sc[a0 + i];
+        i++;
+      } else {
+        dk[o0 + t] = Bk[j];
+        dc[o0 + t] = sc[a0 + L + j];
+        j++;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Sorts P keys with counts (P a power of two in [32, 4096]) held in buffer 0
+// (k0, c0), using buffer 1 (k1, c1) as well: runs of P / W keys sorted by W
+// warps in registers, then merged pairwise.  Returns the buffer that holds
+// the result.
+template <int NT, typename CT>
+GKC_DEV int block_merge_sort(uint64_t *k0, CT *c0, uint64_t *k1, CT *c1, uint32_t P) {
+  const uint32_t W = min((uint32_t)NT / 32, P / 32), C = P / W, w = threadIdx.x >> 5;
+  if (w < W) {
+    switch (C / 32) {
+      case 1: warp_sort_run<1, CT>(k0 + w * C, c0 + w * C); break;
+      case 2: warp_sort_run<2, CT>(k0 + w * C, c0 + w * C); break;
+      case 4: warp_sort_run<4, CT>(k0 + w * C, c0 + w * C); break;
+      default: warp_sort_run<8, CT>(k0 + w * C, c0 + w * C); break;
+    }
+  }
+  __syncthreads();
+  int src = 0;
+  for (uint32_t L = C; L < P; L <<= 1) {
+    if (src == 0) merge_round<NT, CT>(k0, c0, k1, c1, P, L);
+    else merge_round<NT, CT>(k1, c1, k0, c0, P, L);
+    src ^= 1;
+  }
+  return src;
+}
+
 // ---- hash path (8-byte keys): a bucket's keys aggregated in a shared-memory
-// table first, so that only its distinct keys are sorted, by a bitonic
-// network (keys of a minimizer bin are far from uniform in their leading
-// bases: those holding the minimizer near their start share them, so digit
-// splits of a bucket can be very uneven).  The keys are read from global
-// memory, so a bucket of any size with few enough distinct keys takes this
-// path.  The table lives in the upper half of the key area (keys) and in the
-// run-count area (counts); the distinct keys go to the lower half of the key
-// area, their counts to the sub-bucket counters.
+// table first, so that only its distinct keys are sorted, by comparisons
+// (keys of a minimizer bin are far from uniform in their leading bases:
+// those holding the minimizer near their start share them, so digit splits
+// of a bucket can be very uneven).  The keys are read from global memory, so
+// a bucket of any size with few enough distinct keys takes this path.  The
+// table lives in the upper half of the key area (keys) and in the run-count
+// area (counts); the distinct keys go to the lower half of the key area,
+// their counts to the per-sub-bucket array, and are merge-sorted with the
+// table's two areas as the second buffer.  The slices of a bucket too large
+// for the table are counted the same way.
 constexpr uint32_t HT_SLOTS = 4096;
 constexpr uint32_t HT_MAX_DISTINCT = 3072;  // 3/4 full: beyond it the bucket takes the sub-bucket path
+constexpr uint64_t HT_MAX_KEYS = 65535;     // counts of the sorted pairs are 16-bit
 constexpr uint64_t HT_EMPTY = ~0ull;        // never a canonical key: the reverse complement of all-T is all-A
 
 GKC_DEV uint32_t ht_slot(uint64_t x) { return (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> 52); }
 
 template <int NT, typename K>
-GKC_DEV bool hash_count(CountSmem<K> &, const SortCountArgs &, const K *, uint64_t, uint64_t, uint64_t) {
+GKC_DEV bool hash_count(CountSmem<K> &, const SortCountArgs &, const K *, uint64_t, uint64_t) {
   return false;  // 16-byte keys: no 128-bit compare-and-swap in shared memory here
 }
 
-// Counts the n keys src[0, n) (read from global memory, any n) through the
-// table and writes the bucket's sorted runs to the staging arrays at
-// `start`.  Returns false, with nothing written, when the bucket has more
-// than HT_MAX_DISTINCT distinct keys (the caller then takes the sub-bucket
-// or the scratch path).  Not inlined: its registers are then not added to
-// the count kernel's.
+// Counts the n keys src[0, n) (read from global memory; n < 2^16, so counts
+// fit 16 bits) through the table and writes their sorted runs to the staging
+// arrays at `out_at`; their number is left in S.hfill.  Returns false, with
+// nothing written, when there are more than HT_MAX_DISTINCT distinct keys
+// (the caller then takes another path).  Uses the key area, the run-count
+// area and the per-sub-bucket array only (S.cnt is left as it is).  Not
+// inlined: its registers are then not added to the count kernel's.
 template <int NT>
 __device__ __noinline__ bool hash_count(CountSmem<uint64_t> &S, const SortCountArgs &a, const uint64_t *src,
-                                        uint64_t n, uint64_t start, uint64_t g) {
+                                        uint64_t n, uint64_t out_at) {
   static_assert(2 * HT_SLOTS <= (uint32_t)CountShape<uint64_t>::CAP, "table and sorted keys share the key area");
   static_assert(sizeof(S.C) >= HT_SLOTS * 4, "table counts fit the run-count area");
-  static_assert(sizeof(S.cnt) >= HT_SLOTS * 4, "sorted counts fit the sub-bucket counters");
+  static_assert(sizeof(S.w.dc) >= HT_SLOTS * 2, "sorted counts fit the per-sub-bucket array");
   constexpr uint32_t SPT = HT_SLOTS / NT;
-  constexpr int U = 4;  // keys in flight per thread
+  constexpr int U = 8;  // keys in flight per thread
+  if (n > HT_MAX_KEYS) return false;
   volatile uint64_t *T = S.u.A + HT_SLOTS;
   uint32_t *TC = reinterpret_cast<uint32_t *>(S.C);
   uint64_t *B = S.u.A;
-  uint32_t *BC = S.cnt;
+  uint16_t *BC = S.w.dc;
   const int tid = threadIdx.x;
   for (uint32_t i = tid; i < HT_SLOTS; i += NT) {
     T[i] = HT_EMPTY;
@@ -1114,28 +1234,32 @@ __device__ __noinline__ bool hash_count(CountSmem<uint64_t> &S, const SortCountA
     const uint64_t x = T[slot];
     if (x != HT_EMPTY) {
       B[pos] = x;
-      BC[pos] = TC[slot];
+      BC[pos] = (uint16_t)TC[slot];  // <= n < 2^16
       pos++;
     }
   }
-  uint32_t P = 1;
+  uint32_t P = 32;
   while (P < D) P <<= 1;
   for (uint32_t i = D + tid; i < P; i += NT) {
     B[i] = HT_EMPTY;
     BC[i] = 0;
   }
   __syncthreads();
-  block_sort_pairs<uint64_t, NT>(B, BC, P);
+  // the table is free now: its two areas are the sort's second buffer
+  uint64_t *B1 = S.u.A + HT_SLOTS;
+  uint16_t *BC1 = S.C;
+  const int res = block_merge_sort<NT, uint16_t>(B, BC, B1, BC1, P);
+  const uint64_t *RK = res ? B1 : B;
+  const uint16_t *RC = res ? BC1 : BC;
   uint64_t *out = reinterpret_cast<uint64_t *>(a.stage_keys);
   for (uint32_t i = tid; i < D; i += NT) {
-    if (start + i < a.stage_cap) {
-      out[start + i] = B[i];
-      a.stage_counts[start + i] = BC[i];
+    if (out_at + i < a.stage_cap) {
+      out[out_at + i] = RK[i];
+      a.stage_counts[out_at + i] = RC[i];
     } else {
       atomicOr(a.err, ERR_CAPACITY);
     }
   }
-  if (tid == 0) a.bucket_d[g] = D;
   __syncthreads();
   return true;
 }
@@ -1154,13 +1278,25 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
   const uint64_t n_buckets = a.bucket_base[a.nbins];
   int hash_skip = 0;                // the same in every thread of the block
   uint64_t t_next = 0, t_end = 0;   // thread 0: the rest of its batch of tickets
+  bool big_phase = true;            // thread 0: the large buckets first, so none is left for the end
   while (true) {
     if (tid == 0) {
-      if (t_next == t_end) {
-        t_next = atomicAdd(a.ticket, (unsigned long long)CC_TICKETS);
-        t_end = t_next + CC_TICKETS;
+      uint64_t gg = n_buckets;
+      if (big_phase) {
+        const unsigned long long bi = atomicAdd(a.big_ticket, 1ull);
+        if (bi < *a.big_count) gg = a.big_list[bi];
+        else big_phase = false;
       }
-      const uint64_t gg = t_next++;
+      if (!big_phase) {
+        while (true) {
+          if (t_next == t_end) {
+            t_next = atomicAdd(a.ticket, (unsigned long long)CC_TICKETS);
+            t_end = t_next + CC_TICKETS;
+          }
+          gg = t_next++;
+          if (gg >= n_buckets || a.bucket_size[gg] < a.big_min) break;  // a large one: taken from the list
+        }
+      }
       S.g = gg;
       if (gg < n_buckets) {
         S.b = a.bucket_bin[gg];
@@ -1176,11 +1312,17 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
     const int cb = (int)a.bin_bits[b];
     // distinct keys through the table first, unless the last bucket that
     // tried it had too many (then skip it for a few buckets)
-    if (hash_skip == 0) {
-      if (hash_count<NT>(S, a, keys + start, n, start, g)) continue;
-      hash_skip = 8;
-    } else {
-      hash_skip--;
+    if (n <= HT_MAX_KEYS) {
+      if (hash_skip == 0) {
+        if (hash_count<NT>(S, a, keys + start, n, start)) {
+          if (tid == 0) a.bucket_d[g] = S.hfill;
+          __syncthreads();
+          continue;
+        }
+        hash_skip = 8;
+      } else {
+        hash_skip--;
+      }
     }
     if (n <= (uint64_t)CAP) {
       // ---- the whole bucket in shared memory
@@ -1280,11 +1422,16 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
       const uint64_t se = jhi < nsub ? S.cnt[jhi] : n;
       const uint64_t ns = se - s0;
       if (ns <= (uint64_t)CAP) {
-        const uint32_t m = (uint32_t)ns;
-        for (uint32_t i = tid; i < m; i += NT) S.u.A[i] = place[s0 + i];
-        __syncthreads();
-        const uint32_t D = slice_runs<K, NT>(S, m, jlo, jhi - jlo, s0);
-        write_runs<K, NT>(S, a, D, S.out_base + S.run);
+        uint32_t D;
+        if (hash_count<NT>(S, a, place + s0, ns, S.out_base + S.run)) {
+          D = S.hfill;
+        } else {
+          const uint32_t m = (uint32_t)ns;
+          for (uint32_t i = tid; i < m; i += NT) S.u.A[i] = place[s0 + i];
+          __syncthreads();
+          D = slice_runs<K, NT>(S, m, jlo, jhi - jlo, s0);
+          write_runs<K, NT>(S, a, D, S.out_base + S.run);
+        }
         __syncthreads();
         if (tid == 0) S.run += D;
         __syncthreads();

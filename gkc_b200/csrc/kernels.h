@@ -85,6 +85,9 @@ struct ExpandArgs {
   void *keys;                  // scatter output (uint64 or u128)
   void *flat;                  // the keys in k-mer order (written by the histogram, read by the scatter)
   uint64_t keys_cap;          // of keys and flat
+  uint32_t *big_list;          // buckets of at least big_min keys (listed by the scan, counted first)
+  unsigned long long *big_count;  // zeroed
+  uint64_t big_min;
   uint32_t *err;
 };
 __global__ void k_chunk_first(ExpandArgs a);
@@ -115,10 +118,15 @@ struct SortCountArgs {
   uint64_t stage_cap;
   unsigned long long *bucket_d;   // distinct keys of each bucket
   unsigned long long *ticket;     // zeroed
+  const uint32_t *big_list;       // buckets of at least big_min keys, taken before the others
+  const unsigned long long *big_count;
+  unsigned long long *big_ticket;  // zeroed
+  uint64_t big_min;
   uint32_t *err;
 };
 template <typename K> __global__ void k_bucket_count(SortCountArgs a);
 template <typename K> size_t bucket_count_smem_bytes();
+template <typename K> uint64_t bucket_count_cap();  // keys of the largest bucket counted in shared memory
 template <typename K>
 __global__ void k_compact_runs(const K *stage_keys, const uint32_t *stage_counts, const uint64_t *bucket_start,
                                const unsigned long long *bucket_d, const uint64_t *bucket_out,
