@@ -385,7 +385,8 @@ uint64_t gkc_job_hbm_estimate(const gkc_params *prm, uint64_t n_bases, uint64_t 
   e += 4 * (chunks << max_bits) + 8 * chunks;                            // chunk matrix, first superkmers
   e += w * kc * 2 + 4 * kc * 2;                                          // keys, output keys, staged and output counts
   e += w * std::max<uint64_t>(kc / 16, 1 << 16);                         // oversized-bucket scratch
-  e += ((uint64_t)prm->nbins << max_bits) * 8 * 5;                       // bucket starts, sizes, distinct counts, offsets, scan
+  e += ((uint64_t)prm->nbins << max_bits) * (8 * 5 + 4 * 2);             // bucket starts, sizes, distinct counts,
+                                                                         // offsets, scan; bins, large-bucket list
   return e + (64ull << 20);
 }
 

@@ -184,44 +184,53 @@ GKC_DEV u128 extract_kmer<u128>(const uint8_t *packed, uint64_t off, uint32_t o,
 
 // The k-mers [qa, qb) of one bin, taken by the calling warp 32 at a time,
 // lane i the i-th of each group: each lane finds its superkmer among the 32
-// after the group's first one (a search over their k-mer ends, held one per
-// lane), extracts its k-mer and passes the canonical key to emit(key, valid)
-// (called by every lane; valid is false past qb).  s0 is the superkmer
-// holding k-mer qa, s_end the bin's end (k-mer offsets up to koff[s_end] are
-// read).
+// from the group's first one (a search over their k-mer ends relative to the
+// group's first k-mer, held one per lane), extracts its k-mer and passes the
+// canonical key to emit(key, valid) (called by every lane; valid is false
+// past qb).  s0 is the superkmer holding k-mer qa, s_end the bin's end
+// (k-mer offsets up to koff[s_end] are read).  The next group's offsets are
+// loaded before this group's k-mers are extracted.
 template <typename K, typename Emit>
 GKC_DEV void warp_kmers(const ExpandArgs &a, uint64_t qa, uint64_t qb, uint64_t s0, uint64_t s_end, Emit &&emit) {
   const uint32_t lane = threadIdx.x & 31u;
   const int k = a.k;
   uint64_t base = s0;
+  uint64_t e = base + 1 + lane <= s_end ? __ldg(a.koff + base + 1 + lane) : ~0ull;  // end of superkmer base + lane
+  uint64_t kb = __ldg(a.koff + base);                                                // start of superkmer base
   for (uint64_t q0 = qa; q0 < qb; q0 += 32) {
-    const uint64_t q = q0 + lane;
-    const uint64_t jx = base + 1 + lane;
-    const uint64_t e = jx <= s_end ? __ldg(a.koff + jx) : ~0ull;  // end of superkmer base + lane
-    uint32_t cnt = 0;  // superkmers from `base` on that end at or before q
+    // superkmer `base` holds q0 or ends at it, so e >= q0
+    const uint32_t rel = (uint32_t)min(e - q0, (uint64_t)64);
+    uint32_t cnt = 0;  // superkmers from `base` on that end at or before q0 + lane
 #pragma unroll
-    for (uint32_t st = 16; st > 0; st >>= 1) {
-      const uint64_t v = __shfl_sync(0xffffffffu, e, cnt + st - 1);
-      if (v <= q) cnt += st;
-    }
-    const uint64_t prev = __shfl_sync(0xffffffffu, e, cnt == 0 ? 0 : cnt - 1);
-    const uint64_t e31 = __shfl_sync(0xffffffffu, e, 31);
-    const bool valid = q < qb;
+    for (uint32_t st = 16; st > 0; st >>= 1)
+      if (__shfl_sync(0xffffffffu, rel, cnt + st - 1) <= lane) cnt += st;
+    const uint32_t prev = __shfl_sync(0xffffffffu, rel, cnt ? cnt - 1 : 0);
+    const uint32_t r31 = __shfl_sync(0xffffffffu, rel, 31);
+    const bool valid = q0 + lane < qb;
     uint64_t s = base + cnt;
-    uint64_t ks = cnt == 0 ? __ldg(a.koff + base) : prev;
-    if (valid && q >= e31) {  // 32 superkmers (some without k-mers) end before q
+    uint64_t o = cnt ? (uint64_t)(lane - prev) : q0 - kb + lane;  // the k-mer's index in its superkmer
+    if (valid && lane >= r31) {  // 32 superkmers (some without k-mers) end before this k-mer
+      const uint64_t q = q0 + lane;
       s = skm_of_kmer(a.koff, base + 32, s_end - 1, q);
-      ks = __ldg(a.koff + s);
+      o = q - __ldg(a.koff + s);
+    }
+    const uint64_t nbase = __shfl_sync(0xffffffffu, s, 31);  // holds the next group's first k-mer or precedes it
+    uint64_t ne = e, nkb = kb;
+    if (q0 + 32 < qb) {
+      ne = nbase + 1 + lane <= s_end ? __ldg(a.koff + nbase + 1 + lane) : ~0ull;
+      nkb = __ldg(a.koff + nbase);
     }
     K key = 0;
     if (valid) {
       const uint64_t off = __ldg(a.desc + s) >> 24;
-      const K x = extract_kmer<K>(a.packed, off, (uint32_t)(q - ks), k);
+      const K x = extract_kmer<K>(a.packed, off, (uint32_t)o, k);
       const K r = revcomp_k<K>(x, k);
       key = x < r ? x : r;
     }
     emit(key, valid);
-    base = __shfl_sync(0xffffffffu, s, 31);  // every lane valid unless this was the last group
+    base = nbase;
+    e = ne;
+    kb = nkb;
   }
 }
 

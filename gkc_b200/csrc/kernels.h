@@ -133,7 +133,7 @@ __global__ void k_compact_runs(const K *stage_keys, const uint32_t *stage_counts
                                const uint64_t *bucket_base, uint32_t nbins, K *out_keys, uint32_t *out_counts,
                                uint64_t *bin_out, const uint32_t *err);
 constexpr int kBucketCountThreads = 512;
-constexpr uint32_t kCoarseTarget = 4096;
+constexpr uint32_t kCoarseTarget = 8192;
 constexpr uint32_t kCoarseMaxBits = 12;
 constexpr uint64_t kChunkKmers = 65536;
 

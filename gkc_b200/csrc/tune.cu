@@ -8,8 +8,12 @@
 // and the count kernel's CTAs per SM.  A search times the count stages of the
 // graph-captured pipeline on a sample of the caller's reads for each
 // candidate, one dimension at a time from the defaults, and keeps the
-// fastest; choices are cached per (SM count, key width, read-length class,
-// bin count) for the process and can be saved to and loaded from a file.
+// fastest.  The sample runs with its bin count scaled down so that its bins
+// hold as many bases as the full run's (digit counts, bucket sizes and the
+// scatter's working set follow the bin size).  Choices are cached per (SM
+// count, key width, read-length class, bin count, bin-size class: bases per
+// bin in factors of 4) for the process and can be saved to and loaded from a
+// file.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,9 +33,10 @@
 namespace {
 
 struct TuneKey {
-  int sms, key_words, long_reads, nbins;
+  int sms, key_words, long_reads, nbins, bin_class;
   bool operator<(const TuneKey &o) const {
-    return std::tie(sms, key_words, long_reads, nbins) < std::tie(o.sms, o.key_words, o.long_reads, o.nbins);
+    return std::tie(sms, key_words, long_reads, nbins, bin_class) <
+           std::tie(o.sms, o.key_words, o.long_reads, o.nbins, o.bin_class);
   }
 };
 
@@ -40,7 +45,10 @@ std::map<TuneKey, gkc_tune_params> g_cache;
 
 TuneKey key_for(int sms, const gkc_params *prm, uint64_t n_bases, uint64_t n_reads) {
   const uint64_t mean = n_reads ? n_bases / n_reads : 0;
-  return TuneKey{sms, prm->k <= 32 ? 1 : 2, mean > 1000 ? 1 : 0, prm->nbins};
+  const uint64_t per_bin = std::max<uint64_t>(1, n_bases / (uint64_t)std::max(prm->nbins, 1));
+  int lg = 0;
+  while ((per_bin >> lg) > 1) lg++;
+  return TuneKey{sms, prm->k <= 32 ? 1 : 2, mean > 1000 ? 1 : 0, prm->nbins, lg / 2};
 }
 
 gkc_tune_params defaults() {
@@ -111,15 +119,17 @@ void gkc_tune_cache_clear(void) {
   g_cache.clear();
 }
 
-// One line per entry: "gkc-tune 1 sms key_words long_reads nbins coarse_target chunk_kmers ctas".
+// One line per entry:
+// "gkc-tune 2 sms key_words long_reads nbins bin_class coarse_target chunk_kmers ctas".
 gkc_status gkc_tune_cache_save(const char *path) {
   if (!path) return GKC_ERR_INVALID_ARG;
   FILE *f = fopen(path, "w");
   if (!f) return GKC_ERR_NOT_FOUND;
   std::lock_guard<std::mutex> lk(g_mu);
   for (auto &kv : g_cache)
-    fprintf(f, "gkc-tune 1 %d %d %d %d %u %u %u\n", kv.first.sms, kv.first.key_words, kv.first.long_reads,
-            kv.first.nbins, kv.second.coarse_target, kv.second.chunk_kmers, kv.second.count_ctas_per_sm);
+    fprintf(f, "gkc-tune 2 %d %d %d %d %d %u %u %u\n", kv.first.sms, kv.first.key_words, kv.first.long_reads,
+            kv.first.nbins, kv.first.bin_class, kv.second.coarse_target, kv.second.chunk_kmers,
+            kv.second.count_ctas_per_sm);
   return fclose(f) == 0 ? GKC_OK : GKC_ERR_INTERNAL;
 }
 
@@ -134,9 +144,9 @@ gkc_status gkc_tune_cache_load(const char *path) {
     TuneKey k{};
     gkc_tune_params p{};
     int ver = 0;
-    if (sscanf(line, "gkc-tune %d %d %d %d %d %u %u %u", &ver, &k.sms, &k.key_words, &k.long_reads, &k.nbins,
-               &p.coarse_target, &p.chunk_kmers, &p.count_ctas_per_sm) != 8 ||
-        ver != 1 || !valid(p)) {
+    if (sscanf(line, "gkc-tune %d %d %d %d %d %d %u %u %u", &ver, &k.sms, &k.key_words, &k.long_reads, &k.nbins,
+               &k.bin_class, &p.coarse_target, &p.chunk_kmers, &p.count_ctas_per_sm) != 9 ||
+        ver != 2 || !valid(p)) {
       st = GKC_ERR_INVALID_ARG;
       break;
     }
@@ -189,6 +199,10 @@ gkc_status gkc_autotune_device(gkc_ctx *c, const gkc_params *prm, const char *d_
       return ctx_cuda(c, cudaGetLastError(), "reading the sample's size");
   }
   rep.sample_bases = nb;
+  // bins of the sample as large as the full run's
+  gkc_params ps = *prm;
+  if (nb < n_bytes)
+    ps.nbins = std::max(1, (int)((double)prm->nbins * (double)nb / (double)n_bytes + 0.5));
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &occ, prm->k <= 32 ? (const void *)gkc::k_bucket_count<uint64_t> : (const void *)gkc::k_bucket_count<u128>,
@@ -199,7 +213,7 @@ gkc_status gkc_autotune_device(gkc_ctx *c, const gkc_params *prm, const char *d_
   const gkc_tune_params saved = {c->tune.coarse_target, c->tune.chunk_kmers, c->tune.count_ctas, 0};
   float best_ms = 0;
   gkc_status s = gkc_tune_set(c, &cur);
-  if (s == GKC_OK) s = time_count_stages(c, prm, d_reads, nb, d_offs, ns, 3, &best_ms);
+  if (s == GKC_OK) s = time_count_stages(c, &ps, d_reads, nb, d_offs, ns, 3, &best_ms);
   if (s != GKC_OK) {
     gkc_tune_set(c, &saved);
     return s;
@@ -207,11 +221,11 @@ gkc_status gkc_autotune_device(gkc_ctx *c, const gkc_params *prm, const char *d_
   rep.default_ms = best_ms;
   rep.candidates = 1;
   const uint32_t ctas[] = {1, 2};
-  const uint32_t targets[] = {2048, 3072, 4096, 6144};
+  const uint32_t targets[] = {4096, 8192, 16384};
   const uint32_t chunks[] = {32768, 65536, 131072};
   for (int dim = 0; dim < 3; dim++) {
     const uint32_t *vals = dim == 0 ? ctas : dim == 1 ? targets : chunks;
-    const int nv = dim == 0 ? 2 : dim == 1 ? 4 : 3;
+    const int nv = dim == 0 ? 2 : dim == 1 ? 3 : 3;
     gkc_tune_params best = cur;
     for (int i = 0; i < nv; i++) {
       gkc_tune_params cand = cur;
@@ -221,7 +235,7 @@ gkc_status gkc_autotune_device(gkc_ctx *c, const gkc_params *prm, const char *d_
       *field = vals[i];
       float ms = 0;
       s = gkc_tune_set(c, &cand);
-      if (s == GKC_OK) s = time_count_stages(c, prm, d_reads, nb, d_offs, ns, 3, &ms);
+      if (s == GKC_OK) s = time_count_stages(c, &ps, d_reads, nb, d_offs, ns, 3, &ms);
       if (s != GKC_OK) {
         gkc_tune_set(c, &saved);
         return s;

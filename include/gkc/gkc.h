@@ -280,7 +280,7 @@ gkc_status gkc_db_read(const gkc_db *db, uint64_t first, uint64_t n, uint64_t *k
  *      (a power of two) and the count kernel's CTAs per SM.  Zero fields
  *      mean the default. ---- */
 typedef struct gkc_tune_params {
-  uint32_t coarse_target;      /* 256 .. 65536; default 4096 */
+  uint32_t coarse_target;      /* 256 .. 65536; default 8192 */
   uint32_t chunk_kmers;        /* 4096 .. 2^22, a power of two; default 65536 */
   uint32_t count_ctas_per_sm;  /* 1 .. 4; default 2 */
   uint32_t reserved;
@@ -296,11 +296,13 @@ gkc_status gkc_tune_get(const gkc_ctx *ctx, gkc_tune_params *out);
 /* NULL restores the defaults.  Applies to the context's later calls. */
 gkc_status gkc_tune_set(gkc_ctx *ctx, const gkc_tune_params *p);
 /* Chooses the shapes for this input's class by timing candidates on a sample
- * of the reads (the first ones, about 2^28 bases), one dimension at a time
- * from the defaults, and sets them on the context.  The choice is cached per
- * (SM count, key width, read-length class: mean above 1 kbp or not, bin
- * count); a cached choice is used without timing unless force != 0.  The
- * context's partition and count results are replaced by the sample's. */
+ * of the reads (the first ones, about 2^28 bases; run with the bin count
+ * scaled down so its bins hold as many bases as the full input's), one
+ * dimension at a time from the defaults, and sets them on the context.  The
+ * choice is cached per (SM count, key width, read-length class: mean above
+ * 1 kbp or not, bin count, bases per bin in factors of 4); a cached choice is
+ * used without timing unless force != 0.  The context's partition and count
+ * results are replaced by the sample's. */
 gkc_status gkc_autotune_device(gkc_ctx *ctx, const gkc_params *prm, const char *d_reads, uint64_t n_bytes,
                                const uint64_t *d_offs, uint64_t n_reads, int force, gkc_tune_report *out);
 /* The process-wide cache (host only, needs no GPU). */

@@ -1,5 +1,6 @@
 """The launch-shape tuner's cache and parameter checks (host only, no GPU):
-entries are keyed by SM count, key width, read-length class and bin count;
+entries are keyed by SM count, key width, read-length class, bin count and
+bases per bin (in factors of 4);
 they round-trip through the text file; out-of-range shapes are refused."""
 import ctypes as C
 
@@ -31,9 +32,11 @@ def test_store_and_lookup_by_class():
     L = G.lib()
     short = G.params(31, 11, 256)
     assert L.gkc_tune_cache_store(148, C.byref(short), 3_000_000_000, 20_000_000, C.byref(tp(3072, 32768, 1))) == OK
-    # same class: any size with 150 bp reads, same key width and bins
-    st, out = lookup(148, short, 300_000_000, 2_000_000)
+    # same class: 150 bp reads, same key width and bins, bases per bin within the same factor of 4
+    st, out = lookup(148, short, 4_000_000_000, 26_000_000)
     assert st == OK and out.as_dict() == {"coarse_target": 3072, "chunk_kmers": 32768, "count_ctas_per_sm": 1}
+    # ten times fewer bases per bin: another size class
+    assert lookup(148, short, 300_000_000, 2_000_000)[0] == NOT_FOUND
     # another class each: long reads, 128-bit keys, other bins, other SM count
     assert lookup(148, short, 2_000_000_000, 250_000)[0] == NOT_FOUND
     assert lookup(148, G.params(63, 13, 256), 3_000_000_000, 12_000_000)[0] == NOT_FOUND
@@ -66,7 +69,7 @@ def test_cache_file_round_trip(tmp_path):
                                                                   "count_ctas_per_sm": 1}
     # a damaged file is refused whole
     with open(path, "a") as f:
-        f.write("gkc-tune 1 148 1 0 256 9 99 2\n")
+        f.write("gkc-tune 2 148 1 0 256 11 9 99 2\n")  # coarse target 9: out of range
     L.gkc_tune_cache_clear()
     assert L.gkc_tune_cache_load(path) == INVALID
     assert lookup(148, a, 3 * 10**9, 2 * 10**7)[0] == NOT_FOUND
