@@ -626,9 +626,14 @@ def run_ours(args, wl):
     model = algorithmic_bytes(B, R, S, N, D, wl["k"])
     peak, peak_kind = peaks()
 
-    # dominant kernel and its model bytes per launch
-    kernel_bytes = {"partition": model["partition"], "coarse_scatter": model["expand"],
-                    "coarse_count": model["sort"] + model["count"]}
+    # dominant stage and its model bytes per launch: the partition kernel; the
+    # expansion (the histogram kernel walks the superkmers and writes every
+    # canonical key); sort + count (the bucket scatter, the count kernel and
+    # the compaction of its runs)
+    stages["sort_count"] = stages.get("coarse_scatter", 0.0) + stages.get("coarse_count", 0.0) + \
+        stages.get("finish", 0.0)
+    kernel_bytes = {"partition": model["partition"], "coarse_hist": model["expand"],
+                    "sort_count": model["sort"] + model["count"]}
     dom = max(kernel_bytes, key=lambda s: stages.get(s, 0.0))
     dom_ms = stages[dom]
     achieved = kernel_bytes[dom] / (dom_ms / 1000.0) / 1e9
@@ -649,6 +654,9 @@ def run_ours(args, wl):
                 "model_bytes_per_launch": kernel_bytes[dom], "ms_per_launch": dom_ms}
     if traffic:
         roofline["frac_dram_traffic"] = traffic / (dom_ms / 1000.0) / 1e9 / peak
+    roofline["stages"] = {n: {"model_bytes": b, "ms": stages.get(n, 0.0),
+                              "frac": (b / (stages[n] / 1000.0) / 1e9 / peak) if stages.get(n) else None}
+                          for n, b in kernel_bytes.items()}
     pipeline = {"model_bytes": model["total"], "ms": ms_step,
                 "achieved_gbs": model["total"] / (ms_step / 1000.0) / 1e9,
                 "frac_of_hbm_roofline": model["total"] / (ms_step / 1000.0) / 1e9 / peak,

@@ -1016,29 +1016,30 @@ __global__ void k_rebase_offs(uint64_t *offs, uint64_t n) {
   __syncthreads();
   if (threadIdx.x == 0) offs[0] = 0;
 }
-
-// The slot's count result into host memory the device can write (page-locked
-// buffers): bin offsets, then at most `capacity` keys and counts, in 16-byte
-// pieces where both sides allow it.  The totals' n_distinct (copied to the
-// host inside the pipeline) tells the waiter how much is valid.
-__global__ void k_copy_out(const uint64_t *bin_out, uint32_t nbins, const uint8_t *keys, const uint8_t *counts,
-                           int key_words, uint64_t capacity, uint64_t *h_bin_off, uint8_t *h_keys,
-                           uint8_t *h_counts) {
-  const uint64_t nd = min(bin_out[nbins], capacity);
-  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  const uint64_t nt = (uint64_t)gridDim.x * blockDim.x;
-  if (h_bin_off)
-    for (uint64_t i = tid; i <= nbins; i += nt) h_bin_off[i] = bin_out[i];
-  auto copy = [&](const uint8_t *src, uint8_t *dst, uint64_t bytes) {
-    if (!dst) return;
-    const bool vec = (((uintptr_t)src | (uintptr_t)dst) & 15) == 0;
-    const uint64_t n16 = vec ? bytes / 16 : 0;
-    for (uint64_t i = tid; i < n16; i += nt)
-      reinterpret_cast<uint4 *>(dst)[i] = reinterpret_cast<const uint4 *>(src)[i];
-    for (uint64_t i = n16 * 16 + tid; i < bytes; i += nt) dst[i] = src[i];
-  };
-  copy(keys, h_keys, nd * 8 * (uint64_t)key_words);
-  copy(counts, h_counts, nd * 4);
+// The download of a streaming call: once its pipeline is done, its totals
+// (copied to page-locked memory inside the captured pipeline) give the exact
+// sizes, and three DMA copies on the download stream move the bin offsets,
+// keys and counts into the caller's page-locked buffers while the next call
+// computes.  Blocks until the call's pipeline is done.
+static gkc_status issue_download(gkc_ctx *c, int slot) {
+  StreamCall &sc = c->calls[slot];
+  if (sc.dl_issued) return GKC_OK;
+  CK(cudaEventSynchronize(c->ev_comp[slot]));
+  const DevTotals *h = c->h_tots[slot];
+  const bool bad = (h->err & (ERR_CAPACITY | ERR_OVERSIZE_SCRATCH | ERR_BIN_TOO_LARGE | ERR_SPIN_TIMEOUT | ERR_BOUNDS |
+                              ERR_BAD_READ)) != 0;
+  if (!bad) {
+    const uint64_t nd = std::min<uint64_t>(h->n_distinct, sc.capacity);
+    if (sc.h_bin_off)
+      CK(cudaMemcpyAsync(sc.h_bin_off, sc.d_bin_off, 8 * ((uint64_t)sc.nbins + 1), cudaMemcpyDeviceToHost, c->st_dl));
+    if (sc.h_keys && nd)
+      CK(cudaMemcpyAsync(sc.h_keys, sc.d_keys, nd * 8 * (uint64_t)sc.key_words, cudaMemcpyDeviceToHost, c->st_dl));
+    if (sc.h_counts && nd)
+      CK(cudaMemcpyAsync(sc.h_counts, sc.d_counts, nd * 4, cudaMemcpyDeviceToHost, c->st_dl));
+  }
+  CK(cudaEventRecord(c->ev_dl[slot], c->st_dl));
+  sc.dl_issued = true;
+  return GKC_OK;
 }
 
 static bool host_visible(const void *p) {
@@ -1072,6 +1073,12 @@ gkc_status gkc_stream_submit(gkc_ctx *c, const gkc_params *prm, const char *read
   }
   const uint64_t t = c->next_ticket;
   const int slot = (int)(t & 1);
+  // the slot's previous call must have its download enqueued (ev_dl) before
+  // its buffers are reused
+  if (t >= 2) {
+    s = issue_download(c, slot);
+    if (s != GKC_OK) return s;
+  }
   // the slot's input buffers; growing them waits for everything in flight
   const uint64_t base = n_reads ? offs[0] : 0, nb = n_reads ? offs[n_reads] - base : 0;
   c->slot = slot;
@@ -1111,17 +1118,27 @@ gkc_status gkc_stream_submit(gkc_ctx *c, const gkc_params *prm, const char *read
   s = pipeline_batched(c, prm, dr, nb, doffs, n_reads, true);
   if (s != GKC_OK) return s;
   CK(cudaEventRecord(c->ev_comp[slot], c->st));
-  CK(cudaStreamWaitEvent(c->st_dl, c->ev_comp[slot], 0));
-  const int kw = prm->k <= 32 ? 1 : 2;
-  k_copy_out<<<64, 256, 0, c->st_dl>>>((const uint64_t *)c->bufs[slot_name(c, "bin_out")].p, (uint32_t)prm->nbins,
-                                      (const uint8_t *)c->bufs[slot_name(c, "out_keys")].p,
-                                      (const uint8_t *)c->bufs[slot_name(c, "counts")].p, kw, capacity, bin_off,
-                                      reinterpret_cast<uint8_t *>(keys), reinterpret_cast<uint8_t *>(counts));
-  LAUNCHED(c);
-  CK(cudaEventRecord(c->ev_dl[slot], c->st_dl));
-  c->calls[slot] = StreamCall{t, capacity, (uint32_t)prm->nbins, kw};
+  StreamCall sc;
+  sc.ticket = t;
+  sc.capacity = capacity;
+  sc.nbins = (uint32_t)prm->nbins;
+  sc.key_words = prm->k <= 32 ? 1 : 2;
+  sc.h_bin_off = bin_off;
+  sc.h_keys = keys;
+  sc.h_counts = counts;
+  sc.d_bin_off = c->bufs[slot_name(c, "bin_out")].p;
+  sc.d_keys = c->bufs[slot_name(c, "out_keys")].p;
+  sc.d_counts = c->bufs[slot_name(c, "counts")].p;
+  sc.dl_issued = false;
+  c->calls[slot] = sc;
   c->next_ticket = t + 1;
   *ticket = t;
+  // the other slot's call, if its pipeline is already done: start its download now
+  const int other = slot ^ 1;
+  if (!c->calls[other].dl_issued && cudaEventQuery(c->ev_comp[other]) == cudaSuccess) {
+    s = issue_download(c, other);
+    if (s != GKC_OK) return s;
+  }
   return GKC_OK;
 }
 
@@ -1130,6 +1147,8 @@ gkc_status gkc_stream_wait(gkc_ctx *c, uint64_t ticket, uint64_t *n_distinct, ui
   const int slot = (int)(ticket & 1);
   if (c->calls[slot].ticket != ticket) return ctx_fail(c, GKC_ERR_NOT_FOUND, "no call in flight with this ticket");
   cudaSetDevice(c->dev);
+  gkc_status s = issue_download(c, slot);
+  if (s != GKC_OK) return s;
   CK(cudaEventSynchronize(c->ev_dl[slot]));
   const DevTotals *h = c->h_tots[slot];
   if (n_distinct) *n_distinct = h->n_distinct;
@@ -1140,7 +1159,7 @@ gkc_status gkc_stream_wait(gkc_ctx *c, uint64_t ticket, uint64_t *n_distinct, ui
   if (h->err & ERR_SPIN_TIMEOUT) return ctx_fail(c, GKC_ERR_DEVICE_TIMEOUT, "device look-back wait timed out");
   if (h->err & (ERR_BOUNDS | ERR_BAD_READ)) return ctx_fail(c, GKC_ERR_INTERNAL, "device check failed");
   if (h->n_distinct > c->calls[slot].capacity)
-    return ctx_fail(c, GKC_ERR_CAPACITY, "result larger than the output capacity (first entries copied)");
+    return ctx_fail(c, GKC_ERR_CAPACITY, "result larger than the output capacity (bin offsets and the first entries copied)");
   return GKC_OK;
 }
 

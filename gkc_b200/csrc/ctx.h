@@ -52,6 +52,11 @@ struct StreamCall {
   uint64_t capacity = 0;
   uint32_t nbins = 0;
   int key_words = 1;
+  // the caller's page-locked outputs and the slot's device results
+  uint64_t *h_bin_off = nullptr, *h_keys = nullptr;
+  uint32_t *h_counts = nullptr;
+  const void *d_bin_off = nullptr, *d_keys = nullptr, *d_counts = nullptr;
+  bool dl_issued = true;  // the download has been enqueued (ev_dl recorded)
 };
 
 struct gkc_ctx {

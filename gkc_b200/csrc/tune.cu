@@ -189,10 +189,10 @@ gkc_status gkc_autotune_device(gkc_ctx *c, const gkc_params *prm, const char *d_
     if (out) *out = rep;
     return gkc_tune_set(c, &rep.chosen);
   }
-  // the sample: the first reads, up to about 2^28 bases
+  // the sample: the first reads, up to about 2^30 bases
   uint64_t ns = n_reads;
   uint64_t nb = n_bytes;
-  const uint64_t want = 1ull << 28;
+  const uint64_t want = 1ull << 30;
   if (n_bytes > want && n_reads > 1) {
     ns = std::max<uint64_t>(1, (uint64_t)((double)n_reads * ((double)want / (double)n_bytes)));
     if (cudaMemcpy(&nb, d_offs + ns, 8, cudaMemcpyDeviceToHost) != cudaSuccess)

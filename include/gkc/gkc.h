@@ -296,7 +296,7 @@ gkc_status gkc_tune_get(const gkc_ctx *ctx, gkc_tune_params *out);
 /* NULL restores the defaults.  Applies to the context's later calls. */
 gkc_status gkc_tune_set(gkc_ctx *ctx, const gkc_tune_params *p);
 /* Chooses the shapes for this input's class by timing candidates on a sample
- * of the reads (the first ones, about 2^28 bases; run with the bin count
+ * of the reads (the first ones, about 2^30 bases; run with the bin count
  * scaled down so its bins hold as many bases as the full input's), one
  * dimension at a time from the defaults, and sets them on the context.  The
  * choice is cached per (SM count, key width, read-length class: mean above
