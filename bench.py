@@ -678,14 +678,16 @@ def run_ours(args, wl):
     if not args.no_plain and rank == 0:
         kw = 1 if wl["k"] <= 32 else 2
         nd_b = int(cv.n_distinct)
-        batched_out = (torch.empty(wl["nbins"] + 1, dtype=torch.int64, device="cuda"),
-                       torch.empty(max(nd_b * kw, 1), dtype=torch.int64, device="cuda"),
-                       torch.empty(max(nd_b, 1), dtype=torch.int32, device="cuda"))
+        # the plain form allocates its own buffers: with 16-byte keys the
+        # batched ones are given back first (both key sets do not fit), and
+        # the two outputs are compared in host memory
+        wide = wl["k"] > 32
+        where = "cpu" if wide else "cuda"
+        batched_out = (torch.empty(wl["nbins"] + 1, dtype=torch.int64, device=where),
+                       torch.empty(max(nd_b * kw, 1), dtype=torch.int64, device=where),
+                       torch.empty(max(nd_b, 1), dtype=torch.int32, device=where))
         assert G.lib().gkc_count_copy_out(ctx.h, *(t.data_ptr() for t in batched_out)) == 0
         torch.cuda.synchronize()
-        # the plain form allocates its own buffers: with 16-byte keys the
-        # batched ones are given back first (both key sets do not fit)
-        wide = wl["k"] > 32
         if wide:
             assert G.lib().gkc_ctx_release_workspace(ctx.h) == 0
         pe0 = torch.cuda.Event(enable_timing=True)
@@ -710,7 +712,8 @@ def run_ours(args, wl):
         result["plain"] = {"value": N / (p_ms / 1000.0), "unit": "kmers/s", "ms_per_step": p_ms,
                            "steps": args.plain_steps, "batched_over_plain": p_ms / ms_step,
                            "same_output_as_batched": bool(same),
-                           "compared": "bin offsets, every key and every count, on the device",
+                           "compared": "bin offsets, every key and every count, " +
+                                       ("in host memory" if wide else "on the device"),
                            "launches_per_step": int(ctx.timings().launches)}
         # restore the batched result in the context
         if wide:
@@ -745,9 +748,11 @@ def run_ours(args, wl):
         h_offs.copy_(offs)
         kw = 1 if wl["k"] <= 32 else 2
         cap = D + D // 64 + 1024
+        # three host output sets: call i is submitted before call i - 2 is
+        # waited for, so its upload overlaps call i - 2's download
         outs = [(torch.empty(wl["nbins"] + 1, dtype=torch.int64, pin_memory=True),
                  torch.empty(cap * kw, dtype=torch.int64, pin_memory=True),
-                 torch.empty(cap, dtype=torch.int32, pin_memory=True)) for _ in range(2)]
+                 torch.empty(cap, dtype=torch.int32, pin_memory=True)) for _ in range(3)]
         nr = h_reads.numpy()
         no = h_offs.numpy().view(np.uint64)
         del reads  # the host path uploads its own copy
@@ -757,7 +762,7 @@ def run_ours(args, wl):
         assert G.lib().gkc_ctx_release_workspace(ctx.h) == 0
 
         def submit(i):
-            o = outs[i % 2]
+            o = outs[i % 3]
             return ctx.stream_submit(h_reads, h_offs, n_reads, prm, o[0], o[1], o[2], cap)
 
         for t in (submit(0), submit(1)):  # the first call of each slot captures its graph
@@ -767,9 +772,9 @@ def run_ours(args, wl):
         t0 = time.perf_counter()
         tickets = []
         for i in range(e_steps):
-            if i >= 2:
-                ctx.stream_wait(tickets[i - 2])  # its host buffers are reused now
             tickets.append(submit(i))
+            if i >= 2:
+                ctx.stream_wait(tickets[i - 2])
         for t in tickets[-2:]:
             nd, nk = ctx.stream_wait(t)
         torch.cuda.synchronize()

@@ -268,8 +268,9 @@ void gkc_ctx_destroy(gkc_ctx *c) {
   for (int i = 0; i < 2; i++) {
     if (c->ev_up[i]) cudaEventDestroy(c->ev_up[i]);
     if (c->ev_comp[i]) cudaEventDestroy(c->ev_comp[i]);
-    if (c->ev_dl[i]) cudaEventDestroy(c->ev_dl[i]);
   }
+  for (int i = 0; i < 4; i++)
+    if (c->ev_dl[i]) cudaEventDestroy(c->ev_dl[i]);
   if (c->own_stream && c->st) cudaStreamDestroy(c->st);
   delete c;
 }
@@ -1020,12 +1021,15 @@ __global__ void k_rebase_offs(uint64_t *offs, uint64_t n) {
 // (copied to page-locked memory inside the captured pipeline) give the exact
 // sizes, and three DMA copies on the download stream move the bin offsets,
 // keys and counts into the caller's page-locked buffers while the next call
-// computes.  Blocks until the call's pipeline is done.
-static gkc_status issue_download(gkc_ctx *c, int slot) {
-  StreamCall &sc = c->calls[slot];
+// computes.  Blocks until the call's pipeline is done.  rec: the call's
+// record (ticket & 3); its slot is ticket & 1.
+static gkc_status issue_download(gkc_ctx *c, int rec) {
+  StreamCall &sc = c->calls[rec];
   if (sc.dl_issued) return GKC_OK;
+  const int slot = (int)(sc.ticket & 1);
   CK(cudaEventSynchronize(c->ev_comp[slot]));
-  const DevTotals *h = c->h_tots[slot];
+  sc.tot = *c->h_tots[slot];  // the slot's next call overwrites them
+  const DevTotals *h = &sc.tot;
   const bool bad = (h->err & (ERR_CAPACITY | ERR_OVERSIZE_SCRATCH | ERR_BIN_TOO_LARGE | ERR_SPIN_TIMEOUT | ERR_BOUNDS |
                               ERR_BAD_READ)) != 0;
   if (!bad) {
@@ -1037,7 +1041,7 @@ static gkc_status issue_download(gkc_ctx *c, int slot) {
     if (sc.h_counts && nd)
       CK(cudaMemcpyAsync(sc.h_counts, sc.d_counts, nd * 4, cudaMemcpyDeviceToHost, c->st_dl));
   }
-  CK(cudaEventRecord(c->ev_dl[slot], c->st_dl));
+  CK(cudaEventRecord(c->ev_dl[rec], c->st_dl));
   sc.dl_issued = true;
   return GKC_OK;
 }
@@ -1068,15 +1072,18 @@ gkc_status gkc_stream_submit(gkc_ctx *c, const gkc_params *prm, const char *read
     for (int i = 0; i < 2; i++) {
       CK(cudaEventCreateWithFlags(&c->ev_up[i], cudaEventDisableTiming));
       CK(cudaEventCreateWithFlags(&c->ev_comp[i], cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&c->ev_dl[i], cudaEventDisableTiming));
     }
+    for (int i = 0; i < 4; i++) CK(cudaEventCreateWithFlags(&c->ev_dl[i], cudaEventDisableTiming));
   }
   const uint64_t t = c->next_ticket;
-  const int slot = (int)(t & 1);
-  // the slot's previous call must have its download enqueued (ev_dl) before
-  // its buffers are reused
+  const int slot = (int)(t & 1), rec = (int)(t & 3);
+  if (!c->calls[rec].waited)
+    return ctx_fail(c, GKC_ERR_INVALID_ARG, "four calls await their wait: wait for the oldest first");
+  // the slot's previous call must have its download enqueued before its
+  // buffers are reused
+  const int prev = (int)((t + 2) & 3);  // record of call t - 2
   if (t >= 2) {
-    s = issue_download(c, slot);
+    s = issue_download(c, prev);
     if (s != GKC_OK) return s;
   }
   // the slot's input buffers; growing them waits for everything in flight
@@ -1109,7 +1116,7 @@ gkc_status gkc_stream_submit(gkc_ctx *c, const gkc_params *prm, const char *read
   CK(cudaEventRecord(c->ev_up[slot], c->st_up));
   CK(cudaStreamWaitEvent(c->st, c->ev_up[slot], 0));
   // and its outputs must have been copied out before they are recomputed
-  if (t >= 2) CK(cudaStreamWaitEvent(c->st, c->ev_dl[slot], 0));
+  if (t >= 2) CK(cudaStreamWaitEvent(c->st, c->ev_dl[prev], 0));
   if (base) {
     k_rebase_offs<<<1, 1024, 0, c->st>>>(doffs, n_reads);
     LAUNCHED(c);
@@ -1130,27 +1137,33 @@ gkc_status gkc_stream_submit(gkc_ctx *c, const gkc_params *prm, const char *read
   sc.d_keys = c->bufs[slot_name(c, "out_keys")].p;
   sc.d_counts = c->bufs[slot_name(c, "counts")].p;
   sc.dl_issued = false;
-  c->calls[slot] = sc;
+  sc.waited = false;
+  c->calls[rec] = sc;
   c->next_ticket = t + 1;
   *ticket = t;
-  // the other slot's call, if its pipeline is already done: start its download now
-  const int other = slot ^ 1;
-  if (!c->calls[other].dl_issued && cudaEventQuery(c->ev_comp[other]) == cudaSuccess) {
-    s = issue_download(c, other);
-    if (s != GKC_OK) return s;
+  // the previous call (the other slot), if its pipeline is already done:
+  // start its download now
+  if (t >= 1) {
+    const int last = (int)((t + 3) & 3);
+    if (!c->calls[last].dl_issued && cudaEventQuery(c->ev_comp[slot ^ 1]) == cudaSuccess) {
+      s = issue_download(c, last);
+      if (s != GKC_OK) return s;
+    }
   }
   return GKC_OK;
 }
 
 gkc_status gkc_stream_wait(gkc_ctx *c, uint64_t ticket, uint64_t *n_distinct, uint64_t *n_kmers) {
   if (!c) return GKC_ERR_INVALID_ARG;
-  const int slot = (int)(ticket & 1);
-  if (c->calls[slot].ticket != ticket) return ctx_fail(c, GKC_ERR_NOT_FOUND, "no call in flight with this ticket");
+  const int rec = (int)(ticket & 3);
+  StreamCall &sc = c->calls[rec];
+  if (sc.ticket != ticket || sc.waited) return ctx_fail(c, GKC_ERR_NOT_FOUND, "no call in flight with this ticket");
   cudaSetDevice(c->dev);
-  gkc_status s = issue_download(c, slot);
+  gkc_status s = issue_download(c, rec);
   if (s != GKC_OK) return s;
-  CK(cudaEventSynchronize(c->ev_dl[slot]));
-  const DevTotals *h = c->h_tots[slot];
+  CK(cudaEventSynchronize(c->ev_dl[rec]));
+  sc.waited = true;
+  const DevTotals *h = &sc.tot;
   if (n_distinct) *n_distinct = h->n_distinct;
   if (n_kmers) *n_kmers = h->n_kmers;
   if (h->err & (ERR_CAPACITY | ERR_OVERSIZE_SCRATCH))
@@ -1158,7 +1171,7 @@ gkc_status gkc_stream_wait(gkc_ctx *c, uint64_t ticket, uint64_t *n_distinct, ui
   if (h->err & ERR_BIN_TOO_LARGE) return ctx_fail(c, GKC_ERR_CAPACITY, "a bin holds 2^32 or more k-mers");
   if (h->err & ERR_SPIN_TIMEOUT) return ctx_fail(c, GKC_ERR_DEVICE_TIMEOUT, "device look-back wait timed out");
   if (h->err & (ERR_BOUNDS | ERR_BAD_READ)) return ctx_fail(c, GKC_ERR_INTERNAL, "device check failed");
-  if (h->n_distinct > c->calls[slot].capacity)
+  if (h->n_distinct > sc.capacity)
     return ctx_fail(c, GKC_ERR_CAPACITY, "result larger than the output capacity (bin offsets and the first entries copied)");
   return GKC_OK;
 }

@@ -63,12 +63,30 @@ GKC_DEV uint32_t coarse_digit(K x, int key_bits, int cb) {
   return coarse_of(eq_map(key_top32<K>(x, key_bits)), cb);
 }
 
-// The sb bits of the key's map below its cb coarse bits (cb + sb <= 32).
+// Bits of a key type, its leading zeros, and the sb bits that follow the
+// first cp bits (keys of one bucket share their first cp bits, the common
+// prefix of the bucket's smallest and largest key, so these digits order the
+// bucket's keys by their first differing bits whatever the distribution).
+template <typename K> constexpr int key_type_bits() { return 8 * (int)sizeof(K); }
+GKC_DEV int key_clz(uint64_t x) { return __clzll((long long)x); }
+GKC_DEV int key_clz(u128 x) {
+  const uint64_t hi = (uint64_t)(x >> 64);
+  return hi ? __clzll((long long)hi) : 64 + __clzll((long long)(uint64_t)x);
+}
 template <typename K>
-GKC_DEV uint32_t sub_digit(K x, int key_bits, int cb, int sb) {
-  if (sb == 0) return 0u;
-  const uint32_t v = eq_map(key_top32<K>(x, key_bits));
-  return (v >> (32 - cb - sb)) & ((1u << sb) - 1u);
+GKC_DEV uint32_t prefix_digit(K x, int cp, int sb) {
+  if (sb == 0) return 0u;  // sb <= key bits - cp, so cp < key bits here
+  return (uint32_t)((K)(x << cp) >> (key_type_bits<K>() - sb));
+}
+// The sub-bucket bits of a bucket of m keys whose smallest and largest keys
+// are lo and hi: about two sub-buckets per key, at most CC_SB_MAX bits, and
+// no more than the bits below the common prefix.
+template <typename K>
+GKC_DEV void prefix_split(K lo, K hi, uint64_t m, int sb_max, int *cp, int *sb) {
+  *cp = lo == hi ? key_type_bits<K>() : key_clz((K)(lo ^ hi));
+  int b = 0;
+  while (b < sb_max && ((uint64_t)1 << b) < 2 * m) b++;
+  *sb = min(b, key_type_bits<K>() - *cp);
 }
 
 // ------------------------------------------------------------------ planning
@@ -502,6 +520,7 @@ struct CountSmem {
   uint32_t nbig, hfill, nsub;
   int flag, sp;
   uint64_t g, start, n, out_base, run, tbase;
+  K red[64];                      // block min / max
   uint32_t b;
   union {
     struct {
@@ -657,6 +676,30 @@ template <> GKC_DEV u128 shfl_up_k<u128>(u128 v, int d) {
   const uint64_t lo = __shfl_up_sync(0xffffffffu, (uint64_t)v, d);
   const uint64_t hi = __shfl_up_sync(0xffffffffu, (uint64_t)(v >> 64), d);
   return ((u128)hi << 64) | lo;
+}
+
+// Smallest and largest of the block's (lo, hi) pairs, in every thread.
+template <typename K, int NT>
+GKC_DEV void block_minmax(CountSmem<K> &S, K &lo, K &hi) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int m = 16; m > 0; m >>= 1) {
+    const K a = shfl_xor_k<K>(lo, m), b = shfl_xor_k<K>(hi, m);
+    lo = a < lo ? a : lo;
+    hi = b > hi ? b : hi;
+  }
+  if (lane == 0) {
+    S.red[w] = lo;
+    S.red[32 + w] = hi;
+  }
+  __syncthreads();
+  lo = S.red[0];
+  hi = S.red[32];
+  for (int i = 1; i < NT / 32; i++) {
+    lo = S.red[i] < lo ? S.red[i] : lo;
+    hi = S.red[32 + i] > hi ? S.red[32 + i] : hi;
+  }
+  __syncthreads();
 }
 
 GKC_DEV uint32_t warp_exclusive_scan(uint32_t c, uint32_t *total) {
@@ -1280,8 +1323,6 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
   CountSmem<K> &S = *reinterpret_cast<CountSmem<K> *>(smem_raw);
   const K *keys = reinterpret_cast<const K *>(a.keys);
   K *tmp = reinterpret_cast<K *>(a.scratch);
-  const int key_bits = 2 * a.k;
-  const int room = key_bits < 32 ? key_bits : 32;  // bits of the map
   const int tid = threadIdx.x;
   if (*a.err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
   const uint64_t n_buckets = a.bucket_base[a.nbins];
@@ -1317,8 +1358,6 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
     const uint64_t g = S.g;
     if (g >= n_buckets) break;
     const uint64_t start = S.start, n = S.n;
-    const uint32_t b = S.b;
-    const int cb = (int)a.bin_bits[b];
     // distinct keys through the table first, unless the last bucket that
     // tried it had too many (then skip it for a few buckets)
     if (n <= HT_MAX_KEYS) {
@@ -1337,14 +1376,19 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
       // ---- the whole bucket in shared memory
       const uint32_t m = (uint32_t)n;
       K xs[KPT];
+      K lo = ~(K)0, hi = 0;
 #pragma unroll
       for (int u = 0; u < KPT; u++) {
         const uint32_t i = u * NT + tid;
-        if (i < m) xs[u] = keys[start + i];
+        if (i < m) {
+          xs[u] = keys[start + i];
+          lo = xs[u] < lo ? xs[u] : lo;
+          hi = xs[u] > hi ? xs[u] : hi;
+        }
       }
-      int sb = 0;
-      while (sb < CC_SB_MAX && (1u << sb) < 2 * m) sb++;
-      sb = min(sb, room - cb);
+      block_minmax<K, NT>(S, lo, hi);
+      int cp, sb;
+      prefix_split<K>(lo, hi, m, CC_SB_MAX, &cp, &sb);
       const uint32_t nsub = 1u << sb;
       for (uint32_t jj = tid; jj < nsub; jj += NT) S.cnt[jj] = 0;
       __syncthreads();
@@ -1355,7 +1399,7 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
       for (int u = 0; u < KPT; u++) {
         const uint32_t i = u * NT + tid;
         if (i < m) {
-          const uint32_t r = atomicAdd(&S.cnt[sub_digit<K>(xs[u], key_bits, cb, sb)], 1u);
+          const uint32_t r = atomicAdd(&S.cnt[prefix_digit<K>(xs[u], cp, sb)], 1u);
           rk[u / 2] |= r << (16 * (u & 1));
         }
       }
@@ -1365,7 +1409,7 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
       for (int u = 0; u < KPT; u++) {
         const uint32_t i = u * NT + tid;
         if (i < m)
-          S.u.A[S.cnt[sub_digit<K>(xs[u], key_bits, cb, sb)] + ((rk[u / 2] >> (16 * (u & 1))) & 0xFFFFu)] = xs[u];
+          S.u.A[S.cnt[prefix_digit<K>(xs[u], cp, sb)] + ((rk[u / 2] >> (16 * (u & 1))) & 0xFFFFu)] = xs[u];
       }
       __syncthreads();
       const uint32_t D = slice_runs<K, NT>(S, m, 0, nsub, 0);
@@ -1380,7 +1424,15 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
 
     // ---- oversized bucket: placed by sub-bucket in the scratch area, then
     // counted in slices of at most CAP keys in key order
-    const int sb = max(0, min(CC_SB_MAX, room - cb));
+    K lo = ~(K)0, hi = 0;
+    for (uint64_t i = tid; i < n; i += NT) {
+      const K x = keys[start + i];
+      lo = x < lo ? x : lo;
+      hi = x > hi ? x : hi;
+    }
+    block_minmax<K, NT>(S, lo, hi);
+    int cp, sb;
+    prefix_split<K>(lo, hi, n, CC_SB_MAX, &cp, &sb);
     const uint32_t nsub = 1u << sb;
     if (tid == 0) {
       S.flag = 0;
@@ -1399,7 +1451,7 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
       continue;
     }
     K *place = tmp + S.tbase;
-    for (uint64_t i = tid; i < n; i += NT) atomicAdd(&S.cnt[sub_digit<K>(keys[start + i], key_bits, cb, sb)], 1u);
+    for (uint64_t i = tid; i < n; i += NT) atomicAdd(&S.cnt[prefix_digit<K>(keys[start + i], cp, sb)], 1u);
     __syncthreads();
     scan_sub<K, NT>(S, nsub);
     static_assert(sizeof(S.C) / 4 >= CC_NSUB_MAX, "cursors fit in C");
@@ -1408,7 +1460,7 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
     __syncthreads();
     for (uint64_t i = tid; i < n; i += NT) {
       const K x = keys[start + i];
-      place[atomicAdd(&cur[sub_digit<K>(x, key_bits, cb, sb)], 1u)] = x;
+      place[atomicAdd(&cur[prefix_digit<K>(x, cp, sb)], 1u)] = x;
     }
     __threadfence_block();
     __syncthreads();
@@ -1443,6 +1495,10 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
         }
         __syncthreads();
         if (tid == 0) S.run += D;
+        __syncthreads();
+      } else if (hash_count<NT>(S, a, place + s0, ns, S.out_base + S.run)) {
+        // one sub-bucket larger than a slice with few distinct keys
+        if (tid == 0) S.run += S.hfill;
         __syncthreads();
       } else {
         heavy_slice<K, NT>(S, a, place + s0, ns);

@@ -56,7 +56,9 @@ struct StreamCall {
   uint64_t *h_bin_off = nullptr, *h_keys = nullptr;
   uint32_t *h_counts = nullptr;
   const void *d_bin_off = nullptr, *d_keys = nullptr, *d_counts = nullptr;
-  bool dl_issued = true;  // the download has been enqueued (ev_dl recorded)
+  bool dl_issued = true;  // the download has been enqueued (ev_dl of the record recorded)
+  bool waited = true;     // the record is free for a new call
+  DevTotals tot{};        // the call's totals, copied when its download is enqueued
 };
 
 struct gkc_ctx {
@@ -104,8 +106,12 @@ struct gkc_ctx {
   SlotGraph graphs[2];
   // streaming host form: upload and download streams, events per slot
   cudaStream_t st_up = nullptr, st_dl = nullptr;
-  cudaEvent_t ev_up[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr}, ev_dl[2] = {nullptr, nullptr};
-  StreamCall calls[2];
+  // streaming: inputs and outputs in two slots (ticket & 1), call records
+  // with their download events in four (ticket & 3): up to four calls may
+  // await their wait
+  cudaEvent_t ev_up[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr};
+  cudaEvent_t ev_dl[4] = {nullptr, nullptr, nullptr, nullptr};
+  StreamCall calls[4];
   uint64_t next_ticket = 0;
   // host scratch
   std::vector<uint64_t> offs_tmp, desc_tmp;

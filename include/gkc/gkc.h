@@ -342,6 +342,13 @@ gkc_status gkc_pipeline_host(gkc_ctx *ctx, const gkc_params *prm, gkc_mode mode,
  *      context's device views do not describe them.  (No reference
  *      counterpart: the reference uploads, computes and downloads each batch
  *      in turn, gkc_cuda.cu:414-498.) ---- */
+/* The download of call t is three DMA copies, enqueued once its pipeline is
+ * done: by gkc_stream_wait(t), or by the next gkc_stream_submit when call t
+ * has finished by then.  Up to four calls may await their wait (a fifth
+ * submit returns GKC_ERR_INVALID_ARG before doing anything); call t
+ * reuses call t-2's device buffers, so submitting t before waiting for t-2
+ * (with a third set of host outputs) lets t's upload run during t-2's
+ * download. */
 gkc_status gkc_stream_submit(gkc_ctx *ctx, const gkc_params *prm, const char *reads, const uint64_t *offs,
                              uint64_t n_reads, uint64_t *bin_off, uint64_t *keys, uint32_t *counts,
                              uint64_t capacity, uint64_t *ticket);

@@ -69,6 +69,38 @@ def test_overlapping_calls_match_the_oracle(torch):
             assert nk == int(np.maximum(np.diff(batches[i][1].astype(np.int64)) - k + 1, 0).sum())
 
 
+def test_submitting_ahead_of_the_waits(torch):
+    """Call i is submitted before call i - 2 is waited for (three host output
+    sets), so uploads overlap downloads; every call still matches the oracle,
+    and a fifth call without a wait is refused."""
+    k, p, nb = 31, 11, 32
+    batches = [synth.iid_reads(40 + s, 500 + 50 * s, 150, 0.002) for s in range(6)]
+    with G.Context(0) as ctx:
+        prm = G.params(k, p, nb)
+        ins = [(pinned(torch, r), pinned(torch, o)) for r, o in batches]
+        cap = max(int(o[-1]) for _, o in batches)
+        outs = [outputs(torch, nb, cap) for _ in range(3)]
+        tickets = []
+        for i, (r, o) in enumerate(ins):
+            tickets.append(ctx.stream_submit(r, o, len(batches[i][1]) - 1, prm, *outs[i % 3], cap))
+            if i >= 2:
+                nd, _ = ctx.stream_wait(tickets[i - 2])
+                check(outs[(i - 2) % 3], expect(*batches[i - 2], k, p, nb), nd)
+        # calls 4 and 5 still await their wait: two more are allowed, a third is not
+        r, o = ins[0]
+        fourth = outputs(torch, nb, cap)
+        extra = [ctx.stream_submit(r, o, len(batches[0][1]) - 1, prm, *outs[0], cap),
+                 ctx.stream_submit(r, o, len(batches[0][1]) - 1, prm, *fourth, cap)]
+        with pytest.raises(G.GkcError):
+            ctx.stream_submit(r, o, len(batches[0][1]) - 1, prm, *fourth, cap)
+        for i in (4, 5):
+            nd, _ = ctx.stream_wait(tickets[i])
+            check(outs[i % 3], expect(*batches[i], k, p, nb), nd)
+        for t, out in zip(extra, (outs[0], fourth)):
+            nd, _ = ctx.stream_wait(t)
+            check(out, expect(*batches[0], k, p, nb), nd)
+
+
 def test_reads_cut_from_a_larger_csr(torch):
     k, p, nb = 25, 9, 16
     reads, offs = synth.iid_reads(21, 900, 120, 0.0)
