@@ -735,6 +735,8 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   stage_mark(c, 5);
   // persistent, buckets taken by ticket
   const int ctas = std::max(1, std::min(occ, c->tune.count_ctas ? (int)c->tune.count_ctas : 2));
+  WS(sstarts, uint32_t, "slice_starts", (uint64_t)c->n_sms * ctas * 4097);
+  sa.slice_starts = sstarts;
   k_bucket_count<K><<<c->n_sms * ctas, kBucketCountThreads, smem, c->st>>>(sa);
   LAUNCHED(c);
   stage_mark(c, 6);

@@ -1199,6 +1199,7 @@ GKC_DEV int block_merge_sort(uint64_t *k0, CT *c0, uint64_t *k1, CT *c1, uint32_
 constexpr uint32_t HT_SLOTS = 4096;
 constexpr uint32_t HT_MAX_DISTINCT = 3072;  // 3/4 full: beyond it the bucket takes the sub-bucket path
 constexpr uint64_t HT_MAX_KEYS = 65535;     // counts of the sorted pairs are 16-bit
+constexpr uint32_t HT_MAX_PROBE = 64;       // a longer probe chain also abandons the table
 constexpr uint64_t HT_EMPTY = ~0ull;        // never a canonical key: the reverse complement of all-T is all-A
 
 GKC_DEV uint32_t ht_slot(uint64_t x) { return (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> 52); }
@@ -1249,9 +1250,13 @@ __device__ __noinline__ bool hash_count(CountSmem<uint64_t> &S, const SortCountA
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const uint64_t x = xs[u];
-      if (i0 + (uint64_t)u * NT >= n) break;
+      if (i0 + (uint64_t)u * NT >= n || *(volatile int *)&S.flag) break;
       uint32_t h = ht_slot(x);
-      for (uint32_t probe = 0; probe < HT_SLOTS; probe++) {
+      for (uint32_t probe = 0;; probe++) {
+        if (probe == HT_MAX_PROBE) {  // a long chain: the table is too full, give up
+          S.flag = 1;
+          break;
+        }
         uint64_t cur = T[h];
         if (cur == HT_EMPTY) {
           cur = atomicCAS((unsigned long long *)(S.u.A + HT_SLOTS + h), (unsigned long long)HT_EMPTY,
@@ -1316,6 +1321,54 @@ __device__ __noinline__ bool hash_count(CountSmem<uint64_t> &S, const SortCountA
   return true;
 }
 
+// Counts the m <= CAP keys src[0, m) in shared memory and stages their runs
+// at out_at; returns their number.  The keys are counting-sorted by the
+// sub-bucket digit that follows the common prefix of their smallest and
+// largest key, then each sub-bucket is reduced to runs (slice_runs).  Not
+// inlined: it is called for whole buckets and for the slices of large ones.
+template <typename K, int NT, int KPT>
+__device__ __noinline__ uint32_t smem_count(CountSmem<K> &S, const SortCountArgs &a, const K *src, uint32_t m,
+                                            uint64_t out_at) {
+  const int tid = threadIdx.x;
+  K xs[KPT];
+  K lo = ~(K)0, hi = 0;
+#pragma unroll
+  for (int u = 0; u < KPT; u++) {
+    const uint32_t i = u * NT + tid;
+    if (i < m) {
+      xs[u] = src[i];
+      lo = xs[u] < lo ? xs[u] : lo;
+      hi = xs[u] > hi ? xs[u] : hi;
+    }
+  }
+  block_minmax<K, NT>(S, lo, hi);
+  int cp, sb;
+  prefix_split<K>(lo, hi, m, CC_SB_MAX, &cp, &sb);
+  const uint32_t nsub = 1u << sb;
+  for (uint32_t jj = tid; jj < nsub; jj += NT) S.cnt[jj] = 0;
+  __syncthreads();
+  uint32_t rk[(KPT + 1) / 2];
+#pragma unroll
+  for (int u = 0; u < (KPT + 1) / 2; u++) rk[u] = 0;
+#pragma unroll
+  for (int u = 0; u < KPT; u++) {
+    const uint32_t i = u * NT + tid;
+    if (i < m) rk[u / 2] |= atomicAdd(&S.cnt[prefix_digit<K>(xs[u], cp, sb)], 1u) << (16 * (u & 1));
+  }
+  __syncthreads();
+  scan_sub<K, NT>(S, nsub);
+#pragma unroll
+  for (int u = 0; u < KPT; u++) {
+    const uint32_t i = u * NT + tid;
+    if (i < m) S.u.A[S.cnt[prefix_digit<K>(xs[u], cp, sb)] + ((rk[u / 2] >> (16 * (u & 1))) & 0xFFFFu)] = xs[u];
+  }
+  __syncthreads();
+  const uint32_t D = slice_runs<K, NT>(S, m, 0, nsub, 0);
+  write_runs<K, NT>(S, a, D, out_at);
+  __syncthreads();
+  return D;
+}
+
 template <typename K>
 __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCountArgs a) {
   constexpr int NT = CountShape<K>::NT, CAP = CountShape<K>::CAP, KPT = CAP / NT;
@@ -1373,52 +1426,11 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
       }
     }
     if (n <= (uint64_t)CAP) {
-      // ---- the whole bucket in shared memory
-      const uint32_t m = (uint32_t)n;
-      K xs[KPT];
-      K lo = ~(K)0, hi = 0;
-#pragma unroll
-      for (int u = 0; u < KPT; u++) {
-        const uint32_t i = u * NT + tid;
-        if (i < m) {
-          xs[u] = keys[start + i];
-          lo = xs[u] < lo ? xs[u] : lo;
-          hi = xs[u] > hi ? xs[u] : hi;
-        }
-      }
-      block_minmax<K, NT>(S, lo, hi);
-      int cp, sb;
-      prefix_split<K>(lo, hi, m, CC_SB_MAX, &cp, &sb);
-      const uint32_t nsub = 1u << sb;
-      for (uint32_t jj = tid; jj < nsub; jj += NT) S.cnt[jj] = 0;
-      __syncthreads();
-      uint32_t rk[(KPT + 1) / 2];
-#pragma unroll
-      for (int u = 0; u < (KPT + 1) / 2; u++) rk[u] = 0;
-#pragma unroll
-      for (int u = 0; u < KPT; u++) {
-        const uint32_t i = u * NT + tid;
-        if (i < m) {
-          const uint32_t r = atomicAdd(&S.cnt[prefix_digit<K>(xs[u], cp, sb)], 1u);
-          rk[u / 2] |= r << (16 * (u & 1));
-        }
-      }
-      __syncthreads();
-      scan_sub<K, NT>(S, nsub);
-#pragma unroll
-      for (int u = 0; u < KPT; u++) {
-        const uint32_t i = u * NT + tid;
-        if (i < m)
-          S.u.A[S.cnt[prefix_digit<K>(xs[u], cp, sb)] + ((rk[u / 2] >> (16 * (u & 1))) & 0xFFFFu)] = xs[u];
-      }
-      __syncthreads();
-      const uint32_t D = slice_runs<K, NT>(S, m, 0, nsub, 0);
-      // the runs go to the staging arrays at the bucket's own key range
-      // (its keys are all in registers or shared memory by now); a later
-      // pass moves them to their final place
+      // ---- the whole bucket in shared memory; the runs go to the staging
+      // arrays at the bucket's own key range (its keys are all on chip by
+      // then), and a later pass moves them to their final place
+      const uint32_t D = smem_count<K, NT, KPT>(S, a, keys + start, (uint32_t)n, start);
       if (tid == 0) a.bucket_d[g] = D;
-      write_runs<K, NT>(S, a, D, start);
-      __syncthreads();
       continue;
     }
 
@@ -1462,6 +1474,10 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
       const K x = keys[start + i];
       place[atomicAdd(&cur[prefix_digit<K>(x, cp, sb)], 1u)] = x;
     }
+    // the sub-bucket starts go to this CTA's global area: the slices are
+    // counted with the shared-memory counters
+    uint32_t *gst = a.slice_starts + (uint64_t)blockIdx.x * (CC_NSUB_MAX + 1);
+    for (uint32_t jj = tid; jj < nsub; jj += NT) gst[jj] = S.cnt[jj];
     __threadfence_block();
     __syncthreads();
     if (tid == 0) {
@@ -1472,27 +1488,27 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
     uint32_t jlo = 0;
     while (jlo < nsub) {
       // next slice: sub-buckets [jlo, jhi), at most CAP keys, or one heavy sub-bucket
-      const uint32_t s0 = S.cnt[jlo];
+      const uint32_t s0 = gst[jlo];
       uint32_t lo = jlo + 1, hi = nsub;
       while (lo < hi) {
         const uint32_t mid = (lo + hi + 1) >> 1;
-        const uint64_t e = mid < nsub ? S.cnt[mid] : n;
+        const uint64_t e = mid < nsub ? gst[mid] : n;
         if (e - s0 <= (uint64_t)CAP) lo = mid; else hi = mid - 1;
       }
       const uint32_t jhi = lo;
-      const uint64_t se = jhi < nsub ? S.cnt[jhi] : n;
+      const uint64_t se = jhi < nsub ? gst[jhi] : n;
       const uint64_t ns = se - s0;
       if (ns <= (uint64_t)CAP) {
         uint32_t D;
-        if (hash_count<NT>(S, a, place + s0, ns, S.out_base + S.run)) {
-          D = S.hfill;
+        bool hashed = false;
+        if (hash_skip == 0) {
+          hashed = hash_count<NT>(S, a, place + s0, ns, S.out_base + S.run);
+          if (!hashed) hash_skip = 8;
         } else {
-          const uint32_t m = (uint32_t)ns;
-          for (uint32_t i = tid; i < m; i += NT) S.u.A[i] = place[s0 + i];
-          __syncthreads();
-          D = slice_runs<K, NT>(S, m, jlo, jhi - jlo, s0);
-          write_runs<K, NT>(S, a, D, S.out_base + S.run);
+          hash_skip--;
         }
+        if (hashed) D = S.hfill;
+        else D = smem_count<K, NT, KPT>(S, a, place + s0, (uint32_t)ns, S.out_base + S.run);
         __syncthreads();
         if (tid == 0) S.run += D;
         __syncthreads();

@@ -113,6 +113,7 @@ struct SortCountArgs {
   void *scratch;                  // oversized buckets, placed by sub-bucket
   uint64_t scratch_keys;
   unsigned long long *scratch_cursor;  // zeroed
+  uint32_t *slice_starts;         // per CTA: sub-bucket starts of its current large bucket (4097 each)
   void *stage_keys;               // runs of bucket g at [bucket_start[g], + its distinct count)
   uint32_t *stage_counts;
   uint64_t stage_cap;
