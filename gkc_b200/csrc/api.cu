@@ -388,6 +388,7 @@ uint64_t gkc_job_hbm_estimate(const gkc_params *prm, uint64_t n_bases, uint64_t 
   e += w * std::max<uint64_t>(kc / 16, 1 << 16);                         // oversized-bucket scratch
   e += ((uint64_t)prm->nbins << max_bits) * (8 * 5 + 4 * 2);             // bucket starts, sizes, distinct counts,
                                                                          // offsets, scan; bins, large-bucket list
+  e += 8ull << 20;                                                       // count kernel's per-CTA slice starts
   return e + (64ull << 20);
 }
 

@@ -23,8 +23,9 @@
 //                         hash table and the distinct (key, count) pairs
 //                         sorted by a bitonic network; a bucket with too many
 //                         distinct keys is counting-sorted by sub-bucket
-//                         instead, each sub-bucket reduced by its thread or a
-//                         warp.  The runs are staged at the bucket's own key
+//                         instead (the digit that follows the common prefix
+//                         of its smallest and largest key), each sub-bucket
+//                         reduced by its thread or a warp.  The runs are staged at the bucket's own key
 //                         range and its distinct count recorded;
 //                         k_compact_runs then moves them to the scan of the
 //                         counts.  A bucket larger than shared memory is
