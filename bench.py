@@ -729,7 +729,7 @@ def run_ours(args, wl):
         # its own workspaces: the count pipeline's 16-byte key arrays are given back first
         assert G.lib().gkc_ctx_release_workspace(ctx.h) == 0
         result["subsample_positions"] = time_subsample(ctx, G, torch, stream, reads, offs, n_reads, n_bases, wl)
-        step()  # the batched result back in the context
+        assert G.lib().gkc_ctx_release_workspace(ctx.h) == 0
 
     # the CPU baseline's reads: the workload's first reads, copied from the
     # device (at most 10 M reads, enough for about 10 s of reference CPU work)

@@ -385,7 +385,6 @@ uint64_t gkc_job_hbm_estimate(const gkc_params *prm, uint64_t n_bases, uint64_t 
   const uint64_t chunks = kc / 32768 + prm->nbins + 1;  // the smallest chunk the tuner picks
   e += 4 * (chunks << max_bits) + 8 * chunks;                            // chunk matrix, first superkmers
   e += w * kc * 2 + 4 * kc * 2;                                          // keys, output keys, staged and output counts
-  e += w * std::max<uint64_t>(kc / 16, 1 << 16);                         // oversized-bucket scratch
   e += ((uint64_t)prm->nbins << max_bits) * (8 * 5 + 4 * 2);             // bucket starts, sizes, distinct counts,
                                                                          // offsets, scan; bins, large-bucket list
   e += 8ull << 20;                                                       // count kernel's per-CTA slice starts
@@ -605,7 +604,7 @@ gkc_status gkc_partition_device(gkc_ctx *c, const gkc_params *prm, const char *d
 
 template <typename K>
 static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint64_t keys_cap,
-                                        uint64_t scratch_keys) {
+                                        uint64_t) {
   const uint32_t nbins = (uint32_t)prm->nbins;
   uint32_t max_bits = kCoarseMaxBits;
   while (max_bits > 0 && ((uint64_t)nbins << max_bits) > (1ull << 20)) max_bits--;
@@ -683,7 +682,7 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   LAUNCHED(c);
   WS(bbin, uint32_t, "bucket_bin", max_buckets + 1);
   WS(big_list, uint32_t, "big_list", max_buckets + 1);
-  // [0] bucket ticket, [1] scratch cursor, [2] large buckets listed, [3] their ticket
+  // [0] bucket ticket, [1] unused, [2] large buckets listed, [3] their ticket
   WS(ticket, unsigned long long, "count_ticket", 4);
   CK(cudaMemsetAsync(ticket, 0, 32, c->st));
   ea.big_list = big_list;
@@ -699,13 +698,12 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
 
   // counting: buckets independently, each bucket's runs staged over its own
   // keys (counts beside them), then moved to the scan of the distinct counts;
-  // oversized buckets go through the scratch area
+  // oversized buckets are placed at their own key range of the result's key
+  // array (free between the scatter and the compaction)
   WS(stage_counts, uint32_t, "stage_counts", keys_cap);
   WS(bucket_d, unsigned long long, "bucket_d", max_buckets + 1);
   WS(bucket_out, uint64_t, "bucket_out", max_buckets + 2);
   WS(dtmp, uint64_t, "scan_tmp3", scan_u64_tmp_words(max_buckets + 1) + 8);
-  scratch_keys = std::max<uint64_t>(scratch_keys, 1 << 16);
-  WS(scratch, K, "sort_scratch", scratch_keys);
   SortCountArgs sa;
   memset(&sa, 0, sizeof(sa));
   sa.nbins = nbins;
@@ -716,9 +714,7 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   sa.bucket_size = bsize;
   sa.bucket_bin = bbin;
   sa.keys = keys;
-  sa.scratch = scratch;
-  sa.scratch_keys = scratch_keys;
-  sa.scratch_cursor = ticket + 1;
+  sa.scratch = out_keys;
   sa.stage_keys = keys;
   sa.stage_counts = stage_counts;
   sa.stage_cap = keys_cap;
@@ -753,12 +749,9 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   return GKC_OK;
 }
 
-// Oversized buckets are placed through a scratch area; it starts at 1/16 of
-// the keys and grows to the full key count if the oversized buckets need more.
 static gkc_status enqueue_count(gkc_ctx *c, const gkc_params *prm, uint64_t keys_cap) {
-  uint64_t scratch = c->scratch_full ? keys_cap : keys_cap / 16;
-  if (prm->k <= 32) return enqueue_count_batched<uint64_t>(c, prm, keys_cap, scratch);
-  return enqueue_count_batched<u128>(c, prm, keys_cap, scratch);
+  if (prm->k <= 32) return enqueue_count_batched<uint64_t>(c, prm, keys_cap, 0);
+  return enqueue_count_batched<u128>(c, prm, keys_cap, 0);
 }
 
 static void fill_count_view(gkc_ctx *c, const gkc_params *prm) {
@@ -781,19 +774,12 @@ gkc_status count_device_impl(gkc_ctx *c, const gkc_params *prm, gkc_mode mode) {
   if (mode == GKC_MODE_PLAIN) return count_plain_impl(c, prm);
   uint64_t n_kmers = c->pv.n_kmers;
   uint64_t keys_cap = n_kmers + 16;
-  gkc_status s = GKC_OK;
-  for (int attempt = 0; attempt < 2; attempt++) {
-    CK(cudaMemsetAsync(c->bufs["err"].p, 0, 16, c->st));
-    s = enqueue_count(c, prm, keys_cap);
-    if (s != GKC_OK) return s;
-    s = read_totals(c, true, (uint32_t)prm->nbins);
-    if (s != GKC_OK) return s;
-    CK(cudaStreamSynchronize(c->st));
-    if (!(c->h_tot->err & ERR_OVERSIZE_SCRATCH)) break;
-    c->scratch_full = true;
-  }
-  if (c->h_tot->err & ERR_OVERSIZE_SCRATCH)
-    return ctx_fail(c, GKC_ERR_CAPACITY, "oversized bucket beyond sort scratch");
+  CK(cudaMemsetAsync(c->bufs["err"].p, 0, 16, c->st));
+  gkc_status s = enqueue_count(c, prm, keys_cap);
+  if (s != GKC_OK) return s;
+  s = read_totals(c, true, (uint32_t)prm->nbins);
+  if (s != GKC_OK) return s;
+  CK(cudaStreamSynchronize(c->st));
   if (c->h_tot->err & ERR_CAPACITY) return ctx_fail(c, GKC_ERR_CAPACITY, "key capacity");
   if (c->h_tot->err & ERR_BOUNDS) return check_device_err(c);
   s = check_device_err(c);
@@ -905,7 +891,6 @@ static gkc_status pipeline_batched(gkc_ctx *c, const gkc_params *prm, const char
     if (!(c->h_tot->err & (ERR_CAPACITY | ERR_OVERSIZE_SCRATCH))) break;
     // grow to the sizes the device reported and retry
     graphs_invalidate(c);
-    if (c->h_tot->err & ERR_OVERSIZE_SCRATCH) c->scratch_full = true;
     cap_skm = std::max<uint64_t>(cap_skm, c->h_tot->n_skm + 16);
     cap_bytes = std::max<uint64_t>(cap_bytes, c->h_tot->n_packed + 64);
     keys_cap = std::max<uint64_t>(keys_cap, c->h_tot->n_kmers + 16);

@@ -1381,6 +1381,7 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
   if (*a.err & (ERR_CAPACITY | ERR_BAD_READ | ERR_BIN_TOO_LARGE)) return;
   const uint64_t n_buckets = a.bucket_base[a.nbins];
   int hash_skip = 0;                // the same in every thread of the block
+  int slice_skip = 0;               // the same, for the slices of large buckets
   uint64_t t_next = 0, t_end = 0;   // thread 0: the rest of its batch of tickets
   bool big_phase = true;            // thread 0: the large buckets first, so none is left for the end
   while (true) {
@@ -1447,23 +1448,11 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
     int cp, sb;
     prefix_split<K>(lo, hi, n, CC_SB_MAX, &cp, &sb);
     const uint32_t nsub = 1u << sb;
-    if (tid == 0) {
-      S.flag = 0;
-      const unsigned long long at = atomicAdd(a.scratch_cursor, (unsigned long long)n);
-      if (at + n > a.scratch_keys) {
-        atomicOr(a.err, ERR_OVERSIZE_SCRATCH);
-        S.flag = 1;
-      }
-      S.tbase = at;
-    }
     for (uint32_t jj = tid; jj < nsub; jj += NT) S.cnt[jj] = 0;
     __syncthreads();
-    if (S.flag) {  // no room: an empty result (the host re-runs with a larger area)
-      if (tid == 0) a.bucket_d[g] = 0;
-      __syncthreads();
-      continue;
-    }
-    K *place = tmp + S.tbase;
+    // the bucket's own key range of the scratch array (the result's key
+    // array, written only after this kernel)
+    K *place = tmp + start;
     for (uint64_t i = tid; i < n; i += NT) atomicAdd(&S.cnt[prefix_digit<K>(keys[start + i], cp, sb)], 1u);
     __syncthreads();
     scan_sub<K, NT>(S, nsub);
@@ -1502,11 +1491,11 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
       if (ns <= (uint64_t)CAP) {
         uint32_t D;
         bool hashed = false;
-        if (hash_skip == 0) {
+        if (slice_skip == 0) {
           hashed = hash_count<NT>(S, a, place + s0, ns, S.out_base + S.run);
-          if (!hashed) hash_skip = 8;
+          if (!hashed) slice_skip = 8;
         } else {
-          hash_skip--;
+          slice_skip--;
         }
         if (hashed) D = S.hfill;
         else D = smem_count<K, NT, KPT>(S, a, place + s0, (uint32_t)ns, S.out_base + S.run);

@@ -100,7 +100,6 @@ struct gkc_ctx {
   int ck = 0;
   gkc_count_view cv{};
   uint64_t count_keys_cap = 0;
-  bool scratch_full = false;  // oversized buckets needed a full-size sort scratch
   bool one_shot = false;      // inputs are not run again: no graph capture
   // graphs of the batched pipeline, one per slot
   SlotGraph graphs[2];

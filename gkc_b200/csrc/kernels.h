@@ -110,9 +110,7 @@ struct SortCountArgs {
   const uint64_t *bucket_size;
   const uint32_t *bucket_bin;     // bin of each bucket
   const void *keys;               // bucketed keys
-  void *scratch;                  // oversized buckets, placed by sub-bucket
-  uint64_t scratch_keys;
-  unsigned long long *scratch_cursor;  // zeroed
+  void *scratch;                  // oversized buckets, placed by sub-bucket at their own key range
   uint32_t *slice_starts;         // per CTA: sub-bucket starts of its current large bucket (4097 each)
   void *stage_keys;               // runs of bucket g at [bucket_start[g], + its distinct count)
   uint32_t *stage_counts;
