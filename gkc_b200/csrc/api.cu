@@ -375,7 +375,7 @@ uint64_t gkc_job_hbm_estimate(const gkc_params *prm, uint64_t n_bases, uint64_t 
   uint64_t e = (B + 64) + 8 * (R + 1);                                  // reads, offsets
   if (prm->hpc) e += 8 * (R + 1) + 8 * (R + 2) + (B + 64) + 4 * (B + 16);  // HPC copies
   e += (B + 1) / 8 + 16;                                                 // read starts
-  e += cap_skm * (8 + 4 + 8 + 4) + cap_bytes;                            // superkmers
+  e += cap_skm * (8 + 4 + 8 + 4) + 2 * cap_bytes;                        // superkmers, tile and bin order
   e += cap_skm * 16;                                                     // k-mer offsets
   if ((uint32_t)prm->nbins <= (uint32_t)kBinPlaceMaxBins)                // bin placement matrices
     e += 17 * ((cap_skm + kBinChunk - 1) / kBinChunk) * (uint64_t)prm->nbins;
@@ -503,6 +503,22 @@ static gkc_status enqueue_partition(gkc_ctx *c, const gkc_params *prm, const cha
                                                    bmm, nullptr, nullptr, err);
     LAUNCHED(c);
   }
+  // packed bases into bin order (byte offsets from a scan of ceil(len / 4)
+  // over the bin-ordered superkmers; the count stage's k-mer-offset buffers
+  // serve, they are rewritten later)
+  {
+    WS(pnb, unsigned long long, "skm_nk", cap_skm + 1);
+    WS(poff, uint64_t, "skm_koff", cap_skm + 2);
+    WS(ptmp, uint64_t, "scan_tmp2", scan_u64_tmp_words(cap_skm + 1) + 8);
+    WS(pbin, uint8_t, "packed_bin", cap_bytes);
+    k_skm_nbytes<<<c->n_sms * 8, 256, 0, c->st>>>(bdesc, tot, pnb);
+    LAUNCHED(c);
+    scan_u64_dev(pnb, poff, cap_skm, (const uint64_t *)tot, ptmp, c->st);
+    c->launches += 4;
+    k_pack_bin_order<<<c->n_sms * 8, 256, 0, c->st>>>(bdesc, tot, poff, packed, pbin, cap_bytes, err);
+    LAUNCHED(c);
+    c->part_packed = pbin;
+  }
 
   c->part_cap_skm = cap_skm;
   c->part_cap_bytes = cap_bytes;
@@ -524,7 +540,7 @@ static gkc_status fill_partition_view(gkc_ctx *c, const gkc_params *prm, uint64_
   v.bin_kmer_off = (const uint64_t *)c->bufs["bin_kstart"].p;
   v.skm_desc = (const uint64_t *)c->bufs["skm_desc_bin"].p;
   v.skm_minimizer = (const uint32_t *)c->bufs["skm_mm_bin"].p;
-  v.packed = (const uint8_t *)c->bufs["packed"].p;
+  v.packed = c->part_packed;
   v.hpc_reads = c->part_hpc_reads;
   v.hpc_offs = c->part_hpc_offs;
   v.hpc_orig_pos = c->part_hpc_orig;
@@ -660,7 +676,7 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   memset(&ea, 0, sizeof(ea));
   ea.desc = desc;
   ea.koff = koff;
-  ea.packed = (const uint8_t *)c->bufs["packed"].p;
+  ea.packed = c->part_packed;
   ea.nbins = nbins;
   ea.bin_start = bin_start;
   ea.bin_kstart = bin_kstart;
@@ -1270,7 +1286,7 @@ gkc_status gkc_count_superkmers_host(gkc_ctx *c, int k, const uint32_t *skm_len,
     if (skm_len[i] >= (uint32_t)k) nk += skm_len[i] - k + 1;
   }
   WS(dd, uint64_t, "skm_desc_bin", n_skm + 1);
-  WS(dp, uint8_t, "packed", off + 16);
+  WS(dp, uint8_t, "packed_bin", off + 16);
   WS(dmm, uint32_t, "skm_mm_bin", n_skm + 1);
   WS(bs, uint64_t, "bin_start", 2);
   WS(bk, uint64_t, "bin_kstart", 2);
@@ -1278,6 +1294,7 @@ gkc_status gkc_count_superkmers_host(gkc_ctx *c, int k, const uint32_t *skm_len,
   WS(err, uint32_t, "err", 4);
   if (n_skm) CK(cudaMemcpyAsync(dd, desc.data(), n_skm * 8, cudaMemcpyHostToDevice, c->st));
   if (off) CK(cudaMemcpyAsync(dp, packed, off, cudaMemcpyHostToDevice, c->st));
+  c->part_packed = dp;
   uint64_t hb[4] = {0, n_skm, 0, nk};
   CK(cudaMemcpyAsync(bs, hb, 16, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(bk, hb + 2, 16, cudaMemcpyHostToDevice, c->st));

@@ -85,6 +85,7 @@ struct gkc_ctx {
   bool have_part = false;
   gkc_partition_view pv{};
   uint64_t part_cap_skm = 0, part_cap_bytes = 0;
+  const uint8_t *part_packed = nullptr;  // packed bases the partition's descriptors point into
   const uint64_t *part_nbytes_dev = nullptr;
   const char *part_hpc_reads = nullptr;
   const uint64_t *part_hpc_offs = nullptr;

@@ -192,7 +192,7 @@ gkc_status gkc_partition_import(gkc_ctx *c, const gkc_params *prm, uint32_t n_sr
   // descriptors keep the byte offset in 40 bits, rebased over all runs
   if (nbytes >> 40) return ctx_fail(c, GKC_ERR_INVALID_ARG, "received bytes exceed 2^40");
   WS(dd, uint64_t, "skm_desc_bin", n + 1);
-  WS(dp, uint8_t, "packed", nbytes + 16);
+  WS(dp, uint8_t, "packed_bin", nbytes + 16);
   WS(dbs, uint64_t, "bin_start", nbl + 1);
   WS(dbk, uint64_t, "bin_kstart", nbl + 1);
   WS(cur, unsigned long long, "cursors", 4);
@@ -231,6 +231,7 @@ gkc_status gkc_partition_import(gkc_ctx *c, const gkc_params *prm, uint32_t n_sr
   v.skm_desc = dd;
   v.skm_minimizer = nullptr;  // minimizers do not travel
   v.packed = dp;
+  c->part_packed = dp;
   c->part_nbytes_dev = nullptr;
   c->part_hpc_reads = nullptr;
   c->part_hpc_offs = nullptr;

@@ -607,6 +607,34 @@ size_t bin_place_smem_bytes(uint32_t nbins) {
   return (size_t)kBinRound * 12 + (size_t)nbins * 16;
 }
 
+// Packed bytes of every bin-ordered superkmer (ceil(len / 4)).
+__global__ void k_skm_nbytes(const uint64_t *desc, const unsigned long long *n_skm_ptr, unsigned long long *nb) {
+  const uint64_t n = *n_skm_ptr;
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < n; s += (uint64_t)gridDim.x * blockDim.x)
+    nb[s] = ((desc[s] & 0xFFFFFFull) + 3) >> 2;
+}
+
+// Moves the packed bases into bin order: superkmer s (bin order) goes to
+// byte boff[s] of dst, its descriptor rewritten to point there; the total
+// becomes the partition's packed size.  The bases of a bin are then
+// contiguous, so the expansion reads them in order.
+__global__ void k_pack_bin_order(uint64_t *desc, unsigned long long *cursors, const uint64_t *boff,
+                                 const uint8_t *src, uint8_t *dst, uint64_t cap_bytes, uint32_t *err) {
+  if (*err & (ERR_CAPACITY | ERR_BAD_READ)) return;
+  const uint64_t n = cursors[0];
+  const uint64_t t0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x, nt = (uint64_t)gridDim.x * blockDim.x;
+  if (t0 == 0) cursors[1] = boff[n];
+  for (uint64_t s = t0; s < n; s += nt) {
+    const uint64_t d = desc[s], len = d & 0xFFFFFFull, from = d >> 24, to = boff[s], nb = (len + 3) >> 2;
+    if (to + nb > cap_bytes) {
+      atomicOr(err, ERR_CAPACITY);
+      continue;
+    }
+    for (uint64_t i = 0; i < nb; i++) dst[to + i] = __ldg(src + from + i);
+    desc[s] = (to << 24) | len;
+  }
+}
+
 // Exclusive scans of the per-bin counters (one thread; nbins is small).
 __global__ void k_bin_prefix(const unsigned long long *bin_nskm, const unsigned long long *bin_nkmers,
                              uint32_t nbins, uint64_t *bin_start, uint64_t *bin_kstart) {

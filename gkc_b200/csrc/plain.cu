@@ -321,6 +321,7 @@ gkc_status partition_plain_impl(gkc_ctx *c, const gkc_params *prm, const char *d
   v.skm_desc = bdesc;
   v.skm_minimizer = bmm;
   v.packed = packed;
+  c->part_packed = packed;
   v.hpc_reads = c->part_hpc_reads;
   v.hpc_offs = c->part_hpc_offs;
   v.hpc_orig_pos = c->part_hpc_orig;
