@@ -32,7 +32,7 @@ constexpr int PT_NW = PT_T + PT_H;               // windows with break flags
 constexpr int PT_WORDS = PT_NLOC / 32;
 constexpr int PT_PER_THREAD = PT_NW / PT_NT;     // 9 contiguous windows per thread
 constexpr int PT_PT = 9;                         // positions per rolling p-mer task
-constexpr int PT_STG = 8192;                     // packed bytes of a tile staged in shared memory
+constexpr int PT_STG = 6144;                     // packed bytes of a tile staged in shared memory
 static_assert(PT_NW % PT_NT == 0, "windows per thread");
 static_assert(PT_NLOC % 64 == 0, "tile alignment");
 
@@ -124,7 +124,7 @@ GKC_DEV uint32_t span_or(uint32_t x0, uint32_t x1, uint32_t x2, int n) {
   return (uint32_t)lo;
 }
 
-__global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
+__global__ void __launch_bounds__(PT_NT, 3) k_partition(PartArgs a) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   PartSmem &S = *reinterpret_cast<PartSmem *>(smem_raw);
   const int tid = threadIdx.x;
@@ -311,7 +311,6 @@ __global__ void __launch_bounds__(PT_NT, 2) k_partition(PartArgs a) {
     if (n_skm > 0 && tid == 0) {
       uint32_t jlast = S.skm[n_skm - 1];
       if (jlast + 1 >= n_brk) {
-        int l = S.brk[jlast];
         uint32_t mv = S.b.smm[n_skm - 1];
         uint64_t w = (uint64_t)(G0 + PT_PRE + PT_NW);
         // walk windows beyond the halo with the exact rule until a break
@@ -617,21 +616,38 @@ __global__ void k_skm_nbytes(const uint64_t *desc, const unsigned long long *n_s
 // Moves the packed bases into bin order: superkmer s (bin order) goes to
 // byte boff[s] of dst, its descriptor rewritten to point there; the total
 // becomes the partition's packed size.  The bases of a bin are then
-// contiguous, so the expansion reads them in order.
+// contiguous, so the expansion reads them in order.  A warp takes 32
+// consecutive superkmers, whose destination bytes are contiguous: each lane
+// writes every 32nd of them (coalesced), its source superkmer found by a
+// search over the 32 destination offsets held one per lane.
 __global__ void k_pack_bin_order(uint64_t *desc, unsigned long long *cursors, const uint64_t *boff,
                                  const uint8_t *src, uint8_t *dst, uint64_t cap_bytes, uint32_t *err) {
   if (*err & (ERR_CAPACITY | ERR_BAD_READ)) return;
   const uint64_t n = cursors[0];
-  const uint64_t t0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x, nt = (uint64_t)gridDim.x * blockDim.x;
-  if (t0 == 0) cursors[1] = boff[n];
-  for (uint64_t s = t0; s < n; s += nt) {
-    const uint64_t d = desc[s], len = d & 0xFFFFFFull, from = d >> 24, to = boff[s], nb = (len + 3) >> 2;
-    if (to + nb > cap_bytes) {
-      atomicOr(err, ERR_CAPACITY);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t w0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  if (w0 == 0 && lane == 0) cursors[1] = boff[n];
+  for (uint64_t g0 = w0 * 32; g0 < n; g0 += nw * 32) {
+    const uint64_t s = g0 + lane;
+    const bool valid = s < n;
+    const uint64_t end = boff[min(g0 + 32, n)];
+    const uint64_t d = valid ? desc[s] : 0, len = d & 0xFFFFFFull, from = d >> 24;
+    const uint64_t to = valid ? boff[s] : end;  // lanes past n start at the end: no byte is theirs
+    if (end > cap_bytes) {
+      if (lane == 0) atomicOr(err, ERR_CAPACITY);
       continue;
     }
-    for (uint64_t i = 0; i < nb; i++) dst[to + i] = __ldg(src + from + i);
-    desc[s] = (to << 24) | len;
+    const uint64_t to0 = __shfl_sync(0xffffffffu, to, 0);
+    for (uint64_t p = to0 + lane; __any_sync(0xffffffffu, p < end); p += 32) {
+      uint32_t j = 0;  // the last lane whose superkmer starts at or before p
+#pragma unroll
+      for (uint32_t st = 16; st > 0; st >>= 1)
+        if (__shfl_sync(0xffffffffu, to, j + st) <= p) j += st;
+      const uint64_t tj = __shfl_sync(0xffffffffu, to, j), fj = __shfl_sync(0xffffffffu, from, j);
+      if (p < end) dst[p] = __ldg(src + fj + (p - tj));
+    }
+    if (valid) desc[s] = (to << 24) | len;
   }
 }
 
