@@ -375,7 +375,7 @@ uint64_t gkc_job_hbm_estimate(const gkc_params *prm, uint64_t n_bases, uint64_t 
   uint64_t e = (B + 64) + 8 * (R + 1);                                  // reads, offsets
   if (prm->hpc) e += 8 * (R + 1) + 8 * (R + 2) + (B + 64) + 4 * (B + 16);  // HPC copies
   e += (B + 1) / 8 + 16;                                                 // read starts
-  e += cap_skm * (8 + 4 + 8 + 4) + 2 * cap_bytes;                        // superkmers, tile and bin order
+  e += cap_skm * (8 + 4 + 8 + 4) + cap_bytes;                            // superkmers
   e += cap_skm * 16;                                                     // k-mer offsets
   if ((uint32_t)prm->nbins <= (uint32_t)kBinPlaceMaxBins)                // bin placement matrices
     e += 17 * ((cap_skm + kBinChunk - 1) / kBinChunk) * (uint64_t)prm->nbins;
@@ -503,22 +503,7 @@ static gkc_status enqueue_partition(gkc_ctx *c, const gkc_params *prm, const cha
                                                    bmm, nullptr, nullptr, err);
     LAUNCHED(c);
   }
-  // packed bases into bin order (byte offsets from a scan of ceil(len / 4)
-  // over the bin-ordered superkmers; the count stage's k-mer-offset buffers
-  // serve, they are rewritten later)
-  {
-    WS(pnb, unsigned long long, "skm_nk", cap_skm + 1);
-    WS(poff, uint64_t, "skm_koff", cap_skm + 2);
-    WS(ptmp, uint64_t, "scan_tmp2", scan_u64_tmp_words(cap_skm + 1) + 8);
-    WS(pbin, uint8_t, "packed_bin", cap_bytes);
-    k_skm_nbytes<<<c->n_sms * 8, 256, 0, c->st>>>(bdesc, tot, pnb);
-    LAUNCHED(c);
-    scan_u64_dev(pnb, poff, cap_skm, (const uint64_t *)tot, ptmp, c->st);
-    c->launches += 4;
-    k_pack_bin_order<<<c->n_sms * 8, 256, 0, c->st>>>(bdesc, tot, poff, packed, pbin, cap_bytes, err);
-    LAUNCHED(c);
-    c->part_packed = pbin;
-  }
+  c->part_packed = packed;  // descriptors point into the tile-order bases
 
   c->part_cap_skm = cap_skm;
   c->part_cap_bytes = cap_bytes;

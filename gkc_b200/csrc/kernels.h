@@ -44,9 +44,6 @@ __global__ void k_bin_scatter(const unsigned long long *n_skm_ptr, const uint64_
                               const uint32_t *mm, uint32_t nbins, const uint64_t *bin_start,
                               unsigned long long *bin_fill, uint64_t *out_desc, uint32_t *out_mm,
                               const uint64_t *gpos, uint64_t *out_gpos, const uint32_t *err);
-__global__ void k_skm_nbytes(const uint64_t *desc, const unsigned long long *n_skm_ptr, unsigned long long *nb);
-__global__ void k_pack_bin_order(uint64_t *desc, unsigned long long *cursors, const uint64_t *boff,
-                                 const uint8_t *src, uint8_t *dst, uint64_t cap_bytes, uint32_t *err);
 __global__ void k_bin_prefix(const unsigned long long *bin_nskm,
                              const unsigned long long *bin_nkmers, uint32_t nbins,
                              uint64_t *bin_start, uint64_t *bin_kstart);

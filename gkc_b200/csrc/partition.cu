@@ -606,51 +606,6 @@ size_t bin_place_smem_bytes(uint32_t nbins) {
   return (size_t)kBinRound * 12 + (size_t)nbins * 16;
 }
 
-// Packed bytes of every bin-ordered superkmer (ceil(len / 4)).
-__global__ void k_skm_nbytes(const uint64_t *desc, const unsigned long long *n_skm_ptr, unsigned long long *nb) {
-  const uint64_t n = *n_skm_ptr;
-  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < n; s += (uint64_t)gridDim.x * blockDim.x)
-    nb[s] = ((desc[s] & 0xFFFFFFull) + 3) >> 2;
-}
-
-// Moves the packed bases into bin order: superkmer s (bin order) goes to
-// byte boff[s] of dst, its descriptor rewritten to point there; the total
-// becomes the partition's packed size.  The bases of a bin are then
-// contiguous, so the expansion reads them in order.  A warp takes 32
-// consecutive superkmers, whose destination bytes are contiguous: each lane
-// writes every 32nd of them (coalesced), its source superkmer found by a
-// search over the 32 destination offsets held one per lane.
-__global__ void k_pack_bin_order(uint64_t *desc, unsigned long long *cursors, const uint64_t *boff,
-                                 const uint8_t *src, uint8_t *dst, uint64_t cap_bytes, uint32_t *err) {
-  if (*err & (ERR_CAPACITY | ERR_BAD_READ)) return;
-  const uint64_t n = cursors[0];
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint64_t w0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  if (w0 == 0 && lane == 0) cursors[1] = boff[n];
-  for (uint64_t g0 = w0 * 32; g0 < n; g0 += nw * 32) {
-    const uint64_t s = g0 + lane;
-    const bool valid = s < n;
-    const uint64_t end = boff[min(g0 + 32, n)];
-    const uint64_t d = valid ? desc[s] : 0, len = d & 0xFFFFFFull, from = d >> 24;
-    const uint64_t to = valid ? boff[s] : end;  // lanes past n start at the end: no byte is theirs
-    if (end > cap_bytes) {
-      if (lane == 0) atomicOr(err, ERR_CAPACITY);
-      continue;
-    }
-    const uint64_t to0 = __shfl_sync(0xffffffffu, to, 0);
-    for (uint64_t p = to0 + lane; __any_sync(0xffffffffu, p < end); p += 32) {
-      uint32_t j = 0;  // the last lane whose superkmer starts at or before p
-#pragma unroll
-      for (uint32_t st = 16; st > 0; st >>= 1)
-        if (__shfl_sync(0xffffffffu, to, j + st) <= p) j += st;
-      const uint64_t tj = __shfl_sync(0xffffffffu, to, j), fj = __shfl_sync(0xffffffffu, from, j);
-      if (p < end) dst[p] = __ldg(src + fj + (p - tj));
-    }
-    if (valid) desc[s] = (to << 24) | len;
-  }
-}
-
 // Exclusive scans of the per-bin counters (one thread; nbins is small).
 __global__ void k_bin_prefix(const unsigned long long *bin_nskm, const unsigned long long *bin_nkmers,
                              uint32_t nbins, uint64_t *bin_start, uint64_t *bin_kstart) {
