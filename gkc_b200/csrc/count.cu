@@ -90,6 +90,9 @@ GKC_DEV void prefix_split(K lo, K hi, uint64_t m, int sb_max, int *cp, int *sb) 
   *sb = min(b, key_type_bits<K>() - *cp);
 }
 
+// Pulls the 128-byte line holding p into L2 (no register waits for it).
+GKC_DEV void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // ------------------------------------------------------------------ planning
 
 __global__ void k_count_plan(CountPlan pl) {
@@ -422,6 +425,11 @@ __global__ void __launch_bounds__(SC_THREADS, 1) k_bucket_scatter(ExpandArgs a) 
     }
     for (uint64_t t0 = q0; t0 < q1; t0 += SC_TILE) {
       const uint32_t tn = (uint32_t)min((uint64_t)SC_TILE, q1 - t0);
+      // the chunk's next tile into L2 while this one is sorted and written
+      constexpr int KPL = 128 / (int)sizeof(K);  // keys per line
+      for (uint64_t i = t0 + SC_TILE + (uint64_t)tid * KPL; i < q1 && i < t0 + 2 * (uint64_t)SC_TILE;
+           i += (uint64_t)SC_THREADS * KPL)
+        prefetch_l2(flat + i);
       for (uint32_t d = tid; d < nd; d += SC_THREADS) toff[d] = 0;
       __syncthreads();
       K xs[KPT];
@@ -521,6 +529,7 @@ struct CountSmem {
   uint32_t nbig, hfill, nsub;
   int flag, sp;
   uint64_t g, start, n, out_base, run, tbase;
+  uint64_t pf_start, pf_n;        // the next bucket's keys, prefetched into L2
   K red[64];                      // block min / max
   uint32_t b;
   union {
@@ -1408,11 +1417,25 @@ __global__ void __launch_bounds__(CountShape<K>::NT, 2) k_bucket_count(SortCount
         S.start = a.bucket_start[gg];
         S.n = a.bucket_size[gg];
       }
+      // the next bucket of the batch, if it is a regular one
+      S.pf_n = 0;
+      if (!big_phase && t_next < t_end && t_next < n_buckets) {
+        const uint64_t nn = a.bucket_size[t_next];
+        if (nn < a.big_min) {
+          S.pf_start = a.bucket_start[t_next];
+          S.pf_n = nn;
+        }
+      }
     }
     __syncthreads();
     const uint64_t g = S.g;
     if (g >= n_buckets) break;
     const uint64_t start = S.start, n = S.n;
+    {
+      constexpr int KPL = 128 / (int)sizeof(K);
+      const uint64_t ps = S.pf_start, pe = ps + S.pf_n;
+      for (uint64_t i = ps + (uint64_t)tid * KPL; i < pe; i += (uint64_t)NT * KPL) prefetch_l2(keys + i);
+    }
     // distinct keys through the table first, unless the last bucket that
     // tried it had too many (then skip it for a few buckets)
     if (n <= HT_MAX_KEYS) {
