@@ -694,7 +694,7 @@ static gkc_status enqueue_count_batched(gkc_ctx *c, const gkc_params *prm, uint6
   stage_mark(c, 4);
   const size_t sct_smem = bucket_scatter_smem_bytes<K>();
   if ((int)sct_smem > c->max_smem_optin) return ctx_fail(c, GKC_ERR_INTERNAL, "scatter tile exceeds shared memory");
-  k_bucket_scatter<K><<<c->n_sms * 2, kBucketScatterThreads, sct_smem, c->st>>>(ea);
+  k_bucket_scatter<K><<<c->n_sms, kBucketScatterThreads, sct_smem, c->st>>>(ea);
   LAUNCHED(c);
 
   // counting: buckets independently, each bucket's runs staged over its own

@@ -382,11 +382,10 @@ __global__ void __launch_bounds__(BS_NT) k_bucket_scan(ExpandArgs a, uint64_t *b
 
 // -------------------------------------------------------------- 3. scatter
 
-constexpr int SC_THREADS = 512;
-// keys per scatter tile: the tile and three digit tables fill half the
-// shared memory of an SM, so two CTAs share one (one's loads overlap the
-// other's sorting)
-template <typename K> constexpr int sc_tile() { return sizeof(K) == 8 ? 8192 : 4096; }
+constexpr int SC_THREADS = 1024;
+// keys per scatter tile: the tile, its digits and three digit tables fill
+// most of the shared memory of one CTA per SM
+template <typename K> constexpr int sc_tile() { return sizeof(K) == 8 ? 16384 : 8192; }
 
 // Moves every key of `flat` to its bucket.  Each CTA takes whole chunks, a
 // tile of SC_TILE keys at a time: the tile is counting-sorted by digit in
@@ -395,12 +394,13 @@ template <typename K> constexpr int sc_tile() { return sizeof(K) == 8 ? 8192 : 4
 // contiguous run at the chunk's write offset for the digit (from the scan)
 // plus the digit's keys of the chunk's earlier tiles.
 template <typename K>
-__global__ void __launch_bounds__(SC_THREADS, 2) k_bucket_scatter(ExpandArgs a) {
+__global__ void __launch_bounds__(SC_THREADS, 1) k_bucket_scatter(ExpandArgs a) {
   constexpr int SC_TILE = sc_tile<K>(), KPT = SC_TILE / SC_THREADS;
   constexpr int ND = 1 << kCoarseMaxBits;
   extern __shared__ __align__(16) uint8_t sc_smem[];
   K *S = reinterpret_cast<K *>(sc_smem);                      // the tile, by digit
-  uint32_t *gbase = reinterpret_cast<uint32_t *>(S + SC_TILE);  // chunk's write offsets
+  uint16_t *Sd = reinterpret_cast<uint16_t *>(S + SC_TILE);   // digits of S
+  uint32_t *gbase = reinterpret_cast<uint32_t *>(Sd + SC_TILE);  // chunk's write offsets
   uint32_t *done = gbase + ND;                                // digit's keys of the chunk's earlier tiles
   uint32_t *toff = done + ND;                                 // tile counts, then tile offsets (ND + 1)
   uint32_t *tmp = toff + ND + 1;                              // block scan
@@ -463,12 +463,14 @@ __global__ void __launch_bounds__(SC_THREADS, 2) k_bucket_scatter(ExpandArgs a) 
         const uint32_t i = u * SC_THREADS + tid;
         if (i < tn) {
           const uint32_t d = coarse_digit<K>(xs[u], key_bits, cb);
-          S[toff[d] + ((rk[u / 2] >> (16 * (u & 1))) & 0xFFFFu)] = xs[u];
+          const uint32_t at = toff[d] + ((rk[u / 2] >> (16 * (u & 1))) & 0xFFFFu);
+          S[at] = xs[u];
+          Sd[at] = (uint16_t)d;
         }
       }
       __syncthreads();
       for (uint32_t i = tid; i < tn; i += SC_THREADS) {
-        const uint32_t d = coarse_digit<K>(S[i], key_bits, cb);
+        const uint32_t d = Sd[i];
         const uint64_t slot = kbase + gbase[d] + done[d] + (i - toff[d]);
         if (slot < a.keys_cap) keys[slot] = S[i];
         else atomicOr(a.err, ERR_CAPACITY);
@@ -483,7 +485,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2) k_bucket_scatter(ExpandArgs a) 
 template <typename K> size_t bucket_scatter_smem_bytes() {
   constexpr int ND = 1 << kCoarseMaxBits;
   static_assert(sc_tile<K>() <= 65536 && sc_tile<K>() % SC_THREADS == 0, "16-bit ranks, whole rounds");
-  return (size_t)sc_tile<K>() * sizeof(K) + 4 * (3 * ND + 1 + 64);
+  return (size_t)sc_tile<K>() * (sizeof(K) + 2) + 4 * (3 * ND + 1 + 64);
 }
 template size_t bucket_scatter_smem_bytes<uint64_t>();
 template size_t bucket_scatter_smem_bytes<u128>();

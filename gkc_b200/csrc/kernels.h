@@ -96,7 +96,7 @@ __global__ void k_bucket_scan(ExpandArgs a, uint64_t *bucket_start, uint64_t *bu
 template <typename K> __global__ void k_bucket_scatter(ExpandArgs a);
 constexpr int kBucketScanThreads = 1024;
 constexpr int kBucketHistThreads = 256;
-constexpr int kBucketScatterThreads = 512;
+constexpr int kBucketScatterThreads = 1024;
 template <typename K> size_t bucket_scatter_smem_bytes();
 __global__ void k_skm_nk(const uint64_t *desc, const unsigned long long *n_skm_dev, int k,
                          unsigned long long *nk);
