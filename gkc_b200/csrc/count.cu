@@ -1210,7 +1210,6 @@ constexpr uint32_t HT_SLOTS = 4096;
 constexpr uint32_t HT_MAX_DISTINCT = 3072;  // 3/4 full: beyond it the bucket takes the sub-bucket path
 constexpr uint64_t HT_MAX_KEYS = 65535;     // counts of the sorted pairs are 16-bit
 constexpr uint32_t HT_MAX_PROBE = 64;       // a longer probe chain also abandons the table
-constexpr uint32_t HT_SUB_MAX = 32;         // distinct keys per digit sub-bucket sorted by insertion
 constexpr uint64_t HT_EMPTY = ~0ull;        // never a canonical key: the reverse complement of all-T is all-A
 
 GKC_DEV uint32_t ht_slot(uint64_t x) { return (uint32_t)((x * 0x9E3779B97F4A7C15ull) >> 52); }
@@ -1225,8 +1224,8 @@ GKC_DEV bool hash_count(CountSmem<K> &, const SortCountArgs &, const K *, uint64
 // arrays at `out_at`; their number is left in S.hfill.  Returns false, with
 // nothing written, when there are more than HT_MAX_DISTINCT distinct keys
 // (the caller then takes another path).  Uses the key area, the run-count
-// area, the per-sub-bucket array and the sub-bucket counters.  Not inlined:
-// its registers are then not added to the count kernel's.
+// area and the per-sub-bucket array only (S.cnt is left as it is).  Not
+// inlined: its registers are then not added to the count kernel's.
 template <int NT>
 __device__ __noinline__ bool hash_count(CountSmem<uint64_t> &S, const SortCountArgs &a, const uint64_t *src,
                                         uint64_t n, uint64_t out_at) {
@@ -1313,72 +1312,12 @@ __device__ __noinline__ bool hash_count(CountSmem<uint64_t> &S, const SortCountA
     BC[i] = 0;
   }
   __syncthreads();
-  // the table is free now: its two areas are the sort's second buffer.
-  // First by the digit that follows the distinct keys' common prefix (a
-  // counting sort, then each sub-bucket's few keys by insertion); when a
-  // sub-bucket gets more than HT_SUB_MAX keys, by the merge sort instead.
+  // the table is free now: its two areas are the sort's second buffer
   uint64_t *B1 = S.u.A + HT_SLOTS;
   uint16_t *BC1 = S.C;
-  const uint64_t *RK;
-  const uint16_t *RC;
-  uint64_t lo = ~0ull, hi = 0;
-  for (uint32_t i = tid; i < D; i += NT) {
-    lo = B[i] < lo ? B[i] : lo;
-    hi = B[i] > hi ? B[i] : hi;
-  }
-  block_minmax<uint64_t, NT>(S, lo, hi);
-  int cp, sb;
-  prefix_split<uint64_t>(lo, hi, D, CC_SB_MAX, &cp, &sb);
-  const uint32_t nsub = 1u << sb;
-  for (uint32_t jj = tid; jj < nsub; jj += NT) S.cnt[jj] = 0;
-  if (tid == 0) S.flag = 0;
-  __syncthreads();
-  constexpr int RPT = (HT_MAX_DISTINCT + NT - 1) / NT;
-  uint32_t rk[RPT];
-#pragma unroll
-  for (int u = 0; u < RPT; u++) {
-    const uint32_t i = u * NT + tid;
-    if (i < D) rk[u] = atomicAdd(&S.cnt[prefix_digit<uint64_t>(B[i], cp, sb)], 1u);
-  }
-  __syncthreads();
-  scan_sub<uint64_t, NT>(S, nsub);
-#pragma unroll
-  for (int u = 0; u < RPT; u++) {
-    const uint32_t i = u * NT + tid;
-    if (i < D) {
-      const uint32_t at = S.cnt[prefix_digit<uint64_t>(B[i], cp, sb)] + rk[u];
-      B1[at] = B[i];
-      BC1[at] = BC[i];
-    }
-  }
-  const uint32_t j0 = (uint32_t)(((uint64_t)tid * nsub) / NT), j1 = (uint32_t)(((uint64_t)(tid + 1) * nsub) / NT);
-  for (uint32_t jj = j0; jj < j1; jj++)
-    if ((jj + 1 < nsub ? S.cnt[jj + 1] : D) - S.cnt[jj] > HT_SUB_MAX) S.flag = 1;
-  __syncthreads();
-  if (!S.flag) {
-    for (uint32_t jj = j0; jj < j1; jj++) {
-      const uint32_t b0 = S.cnt[jj], b1 = jj + 1 < nsub ? S.cnt[jj + 1] : D;
-      for (uint32_t p = b0 + 1; p < b1; p++) {
-        const uint64_t x = B1[p];
-        const uint16_t c = BC1[p];
-        uint32_t q = p;
-        while (q > b0 && x < B1[q - 1]) {
-          B1[q] = B1[q - 1];
-          BC1[q] = BC1[q - 1];
-          q--;
-        }
-        B1[q] = x;
-        BC1[q] = c;
-      }
-    }
-    __syncthreads();
-    RK = B1;
-    RC = BC1;
-  } else {  // B still holds the compacted pairs, padded to P
-    const int res = block_merge_sort<NT, uint16_t>(B, BC, B1, BC1, P);
-    RK = res ? B1 : B;
-    RC = res ? BC1 : BC;
-  }
+  const int res = block_merge_sort<NT, uint16_t>(B, BC, B1, BC1, P);
+  const uint64_t *RK = res ? B1 : B;
+  const uint16_t *RC = res ? BC1 : BC;
   uint64_t *out = reinterpret_cast<uint64_t *>(a.stage_keys);
   for (uint32_t i = tid; i < D; i += NT) {
     if (out_at + i < a.stage_cap) {
