@@ -53,6 +53,13 @@ WORKLOADS = {
                     min_len=1000, max_len=50000, k=25, p=15, nbins=256, hpc=1),
 }
 METRIC = "canonical k-mers counted/s"
+_T0 = time.perf_counter()
+
+
+def progress(what):
+    """One line per bench leg on stderr (the JSON line stays alone on stdout)."""
+    sys.stderr.write(f"[bench {time.perf_counter() - _T0:7.1f} s] {what}\n")
+    sys.stderr.flush()
 SEED = 2026
 
 
@@ -73,6 +80,10 @@ def parse():
     ap.add_argument("--serve", action="store_true",
                     help="only the serving mix (config 5): 1000 jobs at 50/80/95%% load")
     ap.add_argument("--serve-jobs", type=int, default=None)
+    ap.add_argument("--serve-loads", default="0.5,0.8,0.95",
+                    help="loads of the serving mix, as fractions of the measured capacity")
+    ap.add_argument("--serve-timeout", type=float, default=300.0,
+                    help="seconds the default run gives its serving mix (a child process) before ending it")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default count-stage shapes instead of tuning them on a sample first")
@@ -393,7 +404,7 @@ def host_read_pool(G, seed, n_bases):
 
 
 def serve_mix(G, device, n_jobs, loads, seed, max_running=4, lo=1e5, hi=1e9, calib_jobs=40, host_frac=0.25,
-              host_pool_bases=200_000_000):
+              host_pool_bases=200_000_000, grace_s=60.0):
     """The serving mix: jobs of log-uniform size in [lo, hi] bases, each from
     the config-2 (short reads of a genome, 30x) or config-3 (long reads, 20x,
     HPC) generator at random, k in {25, 31}, Poisson arrivals at each load
@@ -402,7 +413,11 @@ def serve_mix(G, device, n_jobs, loads, seed, max_running=4, lo=1e5, hi=1e9, cal
     of the config-2 jobs hands the server reads in host memory (taken from a
     pool made on the host, at most host_pool_bases bases), so their latency
     includes the upload; the others' reads are generated on the device when
-    the job starts, inside its latency."""
+    the job starts, inside its latency.  A job still unfinished grace_s
+    seconds after the last submission is reported in "unfinished" (id, size,
+    generator, k, state) instead of being waited for; out["stuck"] is then
+    true and the server cannot be shut down cleanly (its worker still holds
+    the job), so the caller ends the process."""
     import threading
     rng = np.random.default_rng(seed)
     pool_reads, pool_offs = host_read_pool(G, seed + 17, host_pool_bases)
@@ -426,13 +441,16 @@ def serve_mix(G, device, n_jobs, loads, seed, max_running=4, lo=1e5, hi=1e9, cal
            "sizes_bases": [lo, hi], "k": [25, 31], "slots": max_running,
            "host_read_jobs": f"{host_frac:.0%} of the config-2 jobs, reads in host memory "
                              f"(at most {host_pool_bases:.0e} bases), upload inside the latency"}
-    with G.Server(device, max_running=max_running) as srv:
+    out["stuck"] = False
+    srv = G.Server(device, max_running=max_running)
+    try:
         def collect(ids, infos):
             for j in ids:
                 infos.append(srv.wait(j))
                 srv.release(j)
 
         cal = draw(calib_jobs)
+        progress(f"serving: capacity from a burst of {calib_jobs} jobs")
         t0 = time.perf_counter()
         ids = [submit(srv, sz, g, k, seed * 7919 + i) for i, (sz, g, k) in enumerate(cal)]
         infos = []
@@ -443,12 +461,14 @@ def serve_mix(G, device, n_jobs, loads, seed, max_running=4, lo=1e5, hi=1e9, cal
         out["loads"] = {}
         for li, load in enumerate(loads):
             jobs = draw(n_jobs)
+            progress(f"serving: {n_jobs} jobs at {load:.0%} load")
             mean_bases = float(np.mean([sz for sz, _, _ in jobs]))
             rate = load * cap / mean_bases
             gaps = rng.exponential(1.0 / rate, n_jobs)
-            ids, infos = [], []
+            ids, infos, unfinished = [], [], []
             lock = threading.Lock()
             done = threading.Event()
+            t_last = [None]  # host clock of the last submission
 
             def collector():
                 k = 0
@@ -460,11 +480,21 @@ def serve_mix(G, device, n_jobs, loads, seed, max_running=4, lo=1e5, hi=1e9, cal
                             return
                         time.sleep(0.001)
                         continue
-                    infos.append(srv.wait(j))
-                    srv.release(j)
+                    while True:
+                        info = srv.wait(j, 1.0)
+                        if info.state in (2, 3, 4):  # done, failed, cancelled
+                            infos.append(info)
+                            srv.release(j)
+                            break
+                        if t_last[0] is not None and time.perf_counter() - t_last[0] > grace_s:
+                            sz, g, kk = jobs[j - first_id]
+                            unfinished.append({"job": j, "bases": int(sz), "generator": int(g), "k": int(kk),
+                                               "state": "running" if info.state == 1 else "queued"})
+                            break
                     k += 1
 
             th = threading.Thread(target=collector)
+            first_id = None
             th.start()
             start, t = time.perf_counter(), 0.0
             for i, ((sz, g, k), gap) in enumerate(zip(jobs, gaps)):
@@ -473,22 +503,54 @@ def serve_mix(G, device, n_jobs, loads, seed, max_running=4, lo=1e5, hi=1e9, cal
                 if dt > 0:
                     time.sleep(dt)
                 jid = submit(srv, sz, g, k, seed * 100003 + li * 10007 + i)
+                if first_id is None:
+                    first_id = jid
                 with lock:
                     ids.append(jid)
+            t_last[0] = time.perf_counter()
             done.set()
             th.join()
             ok = [i for i in infos if i.state == 2]
+            n_jobs_done = len(infos)
             lat = np.array([i.end_s - i.submit_s for i in ok])
             span = max(i.end_s for i in ok) - min(i.submit_s for i in ok)
             out["loads"][f"{load:.2f}"] = {
-                "jobs": n_jobs, "failed": n_jobs - len(ok),
+                "jobs": n_jobs, "failed": n_jobs_done - len(ok), "unfinished_count": len(unfinished),
                 "failed_status": sorted({int(i.status) for i in infos if i.state != 2}),
                 "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
                 "mean_latency_s": float(lat.mean()),
                 "kmers_per_s": sum(int(i.n_kmers) for i in ok) / span,
                 "bases_per_s": sum(int(i.n_bases) for i in ok) / span,
                 "offered_bases_per_s": load * cap, "span_s": span}
+            if unfinished:
+                out["loads"][f"{load:.2f}"]["unfinished"] = unfinished
+                out["stuck"] = True
+                break
+    finally:
+        if not out["stuck"]:
+            srv.close()
     return out
+
+
+def serve_child(args):
+    """The default run's serving mix (200 jobs at 80% load) in a child
+    process with a time limit, so that the throughput line is printed
+    whatever the mix does; returns its "serving" object, or an error."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--serve", "--serve-jobs", str(args.serve_jobs or 200),
+           "--serve-loads", "0.8", "--seed", str(args.seed)]
+    try:
+        r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True,
+                           timeout=args.serve_timeout, start_new_session=True)
+    except subprocess.TimeoutExpired as e:
+        tail = (e.stderr or "")[-400:] if isinstance(e.stderr, str) else ""
+        return {"error": f"the serving mix did not finish within {args.serve_timeout:.0f} s", "stderr_tail": tail}
+    line = next((ln for ln in reversed(r.stdout.splitlines()) if ln.startswith("{")), None)
+    if line is None:
+        return {"error": f"the serving mix exited {r.returncode} without a result", "stderr_tail": r.stderr[-400:]}
+    res = json.loads(line).get("serving", {})
+    if r.returncode != 0:
+        res["exit_code"] = r.returncode
+    return res
 
 
 def run_serve(args):
@@ -499,15 +561,26 @@ def run_serve(args):
         return
     torch.cuda.set_device(local)
     n = args.serve_jobs or 1000
-    res = serve_mix(G, local, n, (0.5, 0.8, 0.95), args.seed)
-    l80 = res["loads"]["0.80"]
+    loads = tuple(float(x) for x in args.serve_loads.split(","))
+    res = serve_mix(G, local, n, loads, args.seed)
+    key = "0.80" if "0.80" in res["loads"] else sorted(res["loads"])[-1] if res["loads"] else None
+    if key is None:
+        print(json.dumps({"metric": "served canonical k-mers counted/s", "value": None, "serving": res}))
+        sys.stdout.flush()
+        os._exit(1)
+    l80 = res["loads"][key]
     print(json.dumps({
         "metric": "served canonical k-mers counted/s at 80% load (p50/p99 job latency in serving)",
         "value": l80["kmers_per_s"], "unit": "kmers/s", "n_gpus": 1, "steps": n, "warmup": 40,
         "ms_per_step": 1000 * l80["mean_latency_s"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": f"config5-serving-mix-{n}-jobs", "loads": [0.5, 0.8, 0.95]},
+        "config": {"workload": f"config5-serving-mix-{n}-jobs", "loads": list(loads)},
         "serving": res}))
+    sys.stdout.flush()
+    if res["stuck"]:
+        # a worker still holds an unfinished job: the server cannot be joined
+        sys.stderr.write("serving: unfinished jobs; ending the process without shutting the server down\n")
+        os._exit(3)
 
 
 def wl_name(args):
@@ -570,6 +643,7 @@ def run_ours(args, wl):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
+    progress("workload")
     reads, offs, n_reads, n_bases, genome = make_workload_device(wl, args.seed, rank, torch, G)
     torch.cuda.synchronize()
     prm = G.params(wl["k"], wl["p"], wl["nbins"], wl["hpc"])
@@ -582,6 +656,7 @@ def run_ours(args, wl):
     # sample of the reads (outside the timed region)
     tune = None
     if not args.no_tune:
+        progress("tuning the count stage on a sample")
         rep = ctx.autotune_device(reads, n_bases, offs, n_reads, prm, force=True)
         tune = {"chosen": rep.chosen.as_dict(), "defaults": rep.defaults.as_dict(),
                 "sample_bases": int(rep.sample_bases), "candidates": int(rep.candidates),
@@ -591,9 +666,11 @@ def run_ours(args, wl):
     def step():
         return ctx.pipeline_device(reads, n_bases, offs, n_reads, prm, G.MODE_BATCHED)
 
+    progress("warm-up")
     for _ in range(max(args.warmup, 3)):
         pv, cv = step()
     torch.cuda.synchronize()
+    progress("timed steps")
 
     def barrier():
         if dist:
@@ -676,6 +753,7 @@ def run_ours(args, wl):
     # plain per-stage form on the same input, its whole output compared with
     # the batched one on the device (bin offsets, every key and count)
     if not args.no_plain and rank == 0:
+        progress("plain per-stage form")
         kw = 1 if wl["k"] <= 32 else 2
         nd_b = int(cv.n_distinct)
         # the plain form allocates its own buffers: with 16-byte keys the
@@ -745,6 +823,7 @@ def run_ours(args, wl):
     # and the one before's download overlap; beside it the one-call form
     # (gkc_pipeline_host + gkc_count_copy_out), each step in turn.
     if not args.no_e2e:
+        progress("end to end from host memory")
         h_reads = torch.empty(n_bases, dtype=torch.uint8, pin_memory=True)
         h_offs = torch.empty(n_reads + 1, dtype=torch.int64, pin_memory=True)
         h_reads.copy_(reads[:n_bases])
@@ -794,6 +873,7 @@ def run_ours(args, wl):
                              "api": "gkc_stream_submit + gkc_stream_wait (pinned host buffers; calls overlap)",
                              "clock": "host clock between device synchronisations"}
         # the one-call form, each step in turn
+        progress("end to end, one call at a time")
         h_binoff, h_keys, h_counts = outs[0]
 
         def e2e_step():
@@ -828,6 +908,7 @@ def run_ours(args, wl):
     if not args.no_cpu and rank == 0 and world == 1:
         import oracle_ffi as F
         if F.ref_available():
+            progress("reference CPU path on a sample")
             threads = os.cpu_count() or 1
             n_cal = min(sample_reads(args, wl), cpu_sample[1].size - 1)
             cal_o = cpu_sample[1][:n_cal + 1]
@@ -845,6 +926,7 @@ def run_ours(args, wl):
                 result["parity"] = {"reads": len(so) - 1, "match": None,
                                     "note": "the reference's keys are 64-bit: no comparison at k > 32"}
             else:
+                progress("parity against the reference on that sample")
                 result["parity"] = reference_parity(ctx, G, prm, sr, so, wl, threads)
         else:
             result["cpu_baseline"] = {"value": None, "unit": "kmers/s", "cores": 0, "kind": "reference",
@@ -854,10 +936,8 @@ def run_ours(args, wl):
     if not args.no_serve and rank == 0 and world == 1:
         del ctx
         torch.cuda.empty_cache()
-        try:
-            result["serving"] = serve_mix(G, local, args.serve_jobs or 200, (0.8,), args.seed)
-        except Exception as e:  # reported, not fatal to the throughput line
-            result["serving"] = {"error": str(e)}
+        progress("serving mix")
+        result["serving"] = serve_child(args)
     if rank == 0:
         print(json.dumps(result))
     if dist:

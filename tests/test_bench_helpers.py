@@ -1,7 +1,9 @@
 """Host-side helpers of bench.py: the CPU-baseline sample sizing, the
-whole-job rate and the algorithmic byte model of the roofline."""
+whole-job rate, the algorithmic byte model of the roofline and the serving
+mix's handling of jobs that do not finish."""
 import os
 import sys
+import time
 
 import pytest
 
@@ -31,3 +33,73 @@ def test_byte_model_at_ns():
     assert m["count"] == pytest.approx(8 * 2.4e9 + 12 * 4.36e8)
     assert m["total"] == pytest.approx(m["partition"] + m["expand"] + m["sort"] + m["count"])
     assert bench.algorithmic_bytes(1, 1, 1, 1, 1, 63)["w"] == 16
+
+
+class _Info:
+    def __init__(self, state, n_bases=0, submit_s=0.0, end_s=0.0):
+        self.state, self.status, self.n_bases, self.n_kmers = state, 0 if state == 2 else 3, n_bases, n_bases
+        self.submit_s, self.end_s = submit_s, end_s
+
+
+class _FakeServer:
+    """Stands in for gkc_b200.Server: every job finishes at once except the
+    ids in `never`, which stay running (a worker that does not come back)."""
+
+    def __init__(self, device, max_running=4, never=()):
+        self.jobs, self.never, self.closed, self.next = {}, set(never), False, 1
+
+    def _add(self, n_bases):
+        j = self.next
+        self.next += 1
+        t = time.perf_counter()
+        self.jobs[j] = _Info(1 if j in self.never else 2, n_bases, t, t + 0.001)
+        return j
+
+    def submit(self, reads, offs, prm):
+        return self._add(int(offs[-1]))
+
+    def submit_synth(self, prm, g, seed, n_bases):
+        return self._add(int(n_bases))
+
+    def wait(self, j, timeout=-1.0):
+        if self.jobs[j].state == 1:
+            time.sleep(min(timeout, 0.01) if timeout >= 0 else 0.01)
+        return self.jobs[j]
+
+    def release(self, j):
+        assert self.jobs[j].state != 1
+        del self.jobs[j]
+
+    def close(self):
+        self.closed = True
+
+
+def _fake_module(never):
+    import types
+    import gkc_b200 as G
+    made = []
+
+    def server(device, max_running=4):
+        made.append(_FakeServer(device, max_running, never))
+        return made[-1]
+    return types.SimpleNamespace(Server=server, params=G.params, lib=G.lib), made
+
+
+def test_serving_mix_reports_a_job_that_never_finishes():
+    """A job whose worker never returns is reported as unfinished after the
+    grace period (the mix does not wait for it), and the server is left
+    open for the caller to end the process."""
+    fake, made = _fake_module(never={7})
+    out = bench.serve_mix(fake, 0, 12, (0.8,), 5, calib_jobs=4, host_pool_bases=300_000, grace_s=0.2)
+    l80 = out["loads"]["0.80"]
+    assert out["stuck"] is True and not made[0].closed
+    assert l80["unfinished_count"] == 1 and l80["unfinished"][0]["job"] == 7
+    assert l80["unfinished"][0]["state"] == "running"
+    assert l80["failed"] == 0 and l80["jobs"] == 12
+
+
+def test_serving_mix_closes_the_server_when_every_job_ends():
+    fake, made = _fake_module(never=())
+    out = bench.serve_mix(fake, 0, 12, (0.8,), 5, calib_jobs=4, host_pool_bases=300_000, grace_s=0.2)
+    assert out["stuck"] is False and made[0].closed
+    assert out["loads"]["0.80"]["unfinished_count"] == 0
