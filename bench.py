@@ -82,7 +82,7 @@ def parse():
     ap.add_argument("--serve-jobs", type=int, default=None)
     ap.add_argument("--serve-loads", default="0.5,0.8,0.95",
                     help="loads of the serving mix, as fractions of the measured capacity")
-    ap.add_argument("--serve-timeout", type=float, default=300.0,
+    ap.add_argument("--serve-timeout", type=float, default=240.0,
                     help="seconds the default run gives its serving mix (a child process) before ending it")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-tune", action="store_true",
@@ -404,7 +404,7 @@ def host_read_pool(G, seed, n_bases):
 
 
 def serve_mix(G, device, n_jobs, loads, seed, max_running=4, lo=1e5, hi=1e9, calib_jobs=40, host_frac=0.25,
-              host_pool_bases=200_000_000, grace_s=60.0):
+              host_pool_bases=200_000_000, grace_s=30.0):
     """The serving mix: jobs of log-uniform size in [lo, hi] bases, each from
     the config-2 (short reads of a genome, 30x) or config-3 (long reads, 20x,
     HPC) generator at random, k in {25, 31}, Poisson arrivals at each load
