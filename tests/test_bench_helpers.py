@@ -103,3 +103,30 @@ def test_serving_mix_closes_the_server_when_every_job_ends():
     out = bench.serve_mix(fake, 0, 12, (0.8,), 5, calib_jobs=4, host_pool_bases=300_000, grace_s=0.2)
     assert out["stuck"] is False and made[0].closed
     assert out["loads"]["0.80"]["unfinished_count"] == 0
+
+
+def test_serving_child_results_and_failures(monkeypatch):
+    """The default run's serving leg: the child's serving object, its exit
+    code when it left jobs unfinished, and an error (never a hang) when it
+    times out or prints no line."""
+    import subprocess
+    import types
+    args = types.SimpleNamespace(serve_jobs=None, seed=5, serve_timeout=1.0)
+    line = '{"metric": "m", "serving": {"loads": {}, "stuck": true}}'
+
+    def done(rc, out):
+        return lambda cmd, **kw: subprocess.CompletedProcess(cmd, rc, out, "tail")
+    monkeypatch.setattr(bench.subprocess, "run", done(3, "noise\n" + line + "\n"))
+    res = bench.serve_child(args)
+    assert res["stuck"] is True and res["exit_code"] == 3
+    monkeypatch.setattr(bench.subprocess, "run", done(0, line))
+    assert "exit_code" not in bench.serve_child(args)
+    monkeypatch.setattr(bench.subprocess, "run", done(1, "no json here"))
+    assert "without a result" in bench.serve_child(args)["error"]
+
+    def late(cmd, **kw):
+        assert kw["timeout"] == 1.0 and "--serve" in cmd and "0.8" in cmd
+        raise subprocess.TimeoutExpired(cmd, kw["timeout"], output="", stderr="stuck")
+    monkeypatch.setattr(bench.subprocess, "run", late)
+    res = bench.serve_child(args)
+    assert "did not finish within 1 s" in res["error"] and res["stderr_tail"] == "stuck"
