@@ -380,7 +380,9 @@ def run_reference(args, wl):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * float(np.median(secs)), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": config_dict(args, wl, len(offs) - 1, int(offs[-1])),
+        "config": dict(config_dict(args, wl, len(offs) - 1, int(offs[-1])),
+                       mode="the reference's CPU path: its partition kernels as host C++, SKMStore, "
+                            "Thrust-host sort and run count", parallelism=f"{threads} host threads"),
         "cpu_baseline": {"value": value, "unit": "kmers/s", "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "kmers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
